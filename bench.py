@@ -1,0 +1,358 @@
+"""Benchmark: frames/s of the foam hot path at 10k particles on a 128^3 JFA grid.
+
+Workload (the headline foam): N = 10,000, uniform positions (seed 1),
+lognormal radii (median 0.015, sigma_log 0.25, clipped [0.007, 0.03]), 128^3
+int32 owner grid (8 JFA passes), 8 PBD and 20 Jacobi pressure iterations per
+frame, FSC band [12, 16], JFA every frame for 20 warm-start frames and then
+every 5th frame.  One step = one steady-state cadence cycle of 5 frames
+(1 JFA frame + 4 non-JFA frames) replayed from CUDA graphs; value = frames/s.
+
+Timing: W untimed warm-up steps after the 20 warm-start frames; each of the K
+timed steps is bracketed by CUDA events on the launching stream, with a
+256 MiB L2 flush between steps outside the events; barrier + synchronize
+around the timed region; max over ranks.  e2e repeats the step through the
+public API with host buffers: pinned H2D of pos/rad before and D2H of
+pos/rad/fsc after the 5 frames, inside the timed region.
+
+--impl reference times the CPU restatement of the reference (oracle/, the
+reference itself is Python+Taichi and Taichi is not installable here) with all
+host threads on the same workload and metric.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+sys.path.insert(0, os.path.join(ROOT, "fabric-of-space-taichi-jfa_b200"))
+
+METRIC = "frames/s at 10k particles, 128^3 JFA: plain vs surrogate-FSC (>=99% FSC agree)"
+UNIT = "frames/s"
+FRAMES_PER_STEP = 5
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="fos", choices=["fos", "reference"])
+    ap.add_argument("--cpu-sample-steps", type=int, default=1)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    return ap.parse_args()
+
+
+def dist_env():
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return rank, world, local
+
+
+def workload_config(n_gpus):
+    return {"workload": "headline foam: N=10000, 128^3 int32 owner grid, 8 JFA passes, K=8 PBD, "
+                        "M=20 pressure, band [12,16], JFA every 5th frame after 20 warm-start "
+                        "frames; step = 5-frame cadence cycle",
+            "particles": 10000, "jfa_res": 128, "frames_per_step": FRAMES_PER_STEP,
+            "l2": "flushed between timed steps (256 MiB write outside the events)",
+            "parallelism": f"replicas x{n_gpus} (independent foams, no collective)",
+            "path": "plain exact JFA"}
+
+
+# ----------------------------------------------------------------- clocks
+class Clocks:
+    def __init__(self, index: int):
+        self.index = index
+        self.proc = None
+        self.path = f"/tmp/fos_clocks_{os.getpid()}.csv"
+
+    def start(self):
+        q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.index}", f"--query-gpu={q}", "--format=csv,noheader,nounits",
+                 "-lms", "200"], stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+
+    def stop(self):
+        if self.proc is None:
+            return None
+        time.sleep(0.25)
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        sm, mx, reasons = [], 0.0, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        try:
+            for line in open(self.path):
+                f = [x.strip() for x in line.split(",")]
+                if len(f) < 9:
+                    continue
+                try:
+                    sm.append(float(f[1]))
+                    mx = max(mx, float(f[2]))
+                except ValueError:
+                    continue
+                for k, v in zip(names, f[5:9]):
+                    if v.lower().startswith("active"):
+                        reasons.add(k)
+        except OSError:
+            return None
+        if not sm:
+            return None
+        sm.sort()
+        return {"sm_mhz": sm[len(sm) // 2], "sm_max_mhz": mx, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def measured_peaks():
+    try:
+        return json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
+    except Exception:
+        return None
+
+
+def profile_traffic():
+    """Per-launch DRAM bytes of the JFA pass from the committed ncu summary."""
+    path = os.path.join(ROOT, "profiles", "traffic.json")
+    try:
+        return json.load(open(path))
+    except Exception:
+        return None
+
+
+# ------------------------------------------------------------- CPU arm
+def oracle_sim(foam):
+    from oracle import oracle as O
+    p = O.OracleParams(n=foam.n, L=1.0, R=foam.res, r_max_cell=foam.r_max, f_low=foam.f_low,
+                       f_high=foam.f_high, r_min=foam.r_min, r_max=foam.r_max, brownian=1e-4,
+                       seed=foam.seed, pbd_iters=foam.pbd_iters,
+                       pressure_iters=foam.pressure_iters, jfa_warm=foam.jfa_warm,
+                       jfa_cadence=foam.jfa_cadence)
+    sim = O.OracleSim(p, foam.pos, foam.rad)
+    sim.initialize()
+    sim.frame = foam.jfa_warm  # steady-state cadence: frame 20 is a JFA frame
+    return sim, O
+
+
+def time_cpu(foam, steps, warmup):
+    sim, O = oracle_sim(foam)
+    for _ in range(warmup):
+        for _ in range(FRAMES_PER_STEP):
+            sim.step()
+    t0 = time.perf_counter()
+    for _ in range(steps):
+        for _ in range(FRAMES_PER_STEP):
+            sim.step()
+    dt = time.perf_counter() - t0
+    return FRAMES_PER_STEP * steps / dt, dt, O.num_threads()
+
+
+def run_reference(args):
+    rank, world, _ = dist_env()
+    if rank != 0:
+        return 0
+    from oracle import oracle as O
+    O.build()
+    from fos import inputs
+    foam = inputs.headline()
+    fps, dt, cores = time_cpu(foam, args.steps, args.warmup)
+    line = {
+        "impl": "reference", "metric": METRIC, "value": round(fps, 4), "unit": UNIT,
+        "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": round(1000.0 * dt / args.steps, 3), "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": workload_config(1) | {"path": "CPU restatement of the reference (oracle/)"},
+        "cpu_baseline": {"value": round(fps, 4), "unit": UNIT, "cores": cores, "kind": "port",
+                         "sample": f"{args.steps} steps x 5 frames of the headline workload "
+                                   f"(steady-state cadence from frame 20), after {args.warmup} "
+                                   f"warm-up steps; reference is Taichi (not installable)"},
+        "e2e": {"value": round(fps, 4), "unit": UNIT, "h2d_bytes_per_step": 0,
+                "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+# ------------------------------------------------------------- GPU arm
+def run_fos(args):
+    import numpy as np
+    import torch
+    import torch.distributed as dist
+
+    rank, world, local = dist_env()
+    if world > 1:
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", init_method="env://",
+                                timeout=__import__("datetime").timedelta(seconds=300))
+    else:
+        torch.cuda.set_device(0)
+    dev = torch.cuda.current_device()
+
+    from fos import inputs
+    from fos.context import stream
+    from fos.driver import FoamSim
+    import ctypes as C
+    from fos._lib import FosJfaStats, call
+
+    foam = inputs.headline()
+    sim = FoamSim.from_foam(foam, use_graph=True)
+    sim.initialize()
+    for _ in range(foam.jfa_warm):  # 20 warm-start frames, JFA every frame
+        sim.step()
+    assert sim.frame % foam.jfa_cadence == 0
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
+        torch.cuda.synchronize()
+
+    def one_step():
+        for _ in range(FRAMES_PER_STEP):
+            sim.step()
+
+    for _ in range(args.warmup):
+        one_step()
+    barrier()
+    clocks = Clocks(dev)
+    clocks.start()
+    launches0 = sim.ctx.launch_count()
+    s = torch.cuda.current_stream()
+    times = []
+    barrier()
+    for _ in range(args.steps):
+        flush.fill_(1.0)
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(s)
+        one_step()
+        e1.record(s)
+        times.append((e0, e1))
+    barrier()
+    clk = clocks.stop()
+    launches = sim.ctx.launch_count() - launches0
+    total_ms = sum(a.elapsed_time(b) for a, b in times)
+    t = torch.tensor([total_ms], dtype=torch.float64, device=dev)
+    if world > 1:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    total_ms = float(t.item())
+    value = world * FRAMES_PER_STEP * args.steps / (total_ms / 1000.0)
+
+    # ---- e2e through the public API with host buffers
+    n = foam.n
+    h_pos = torch.empty((n, 3), dtype=torch.float32).pin_memory()
+    h_rad = torch.empty((n,), dtype=torch.float32).pin_memory()
+    h_fsc = torch.empty((n,), dtype=torch.int32).pin_memory()
+    h_pos.copy_(sim.pos.cpu())
+    h_rad.copy_(sim.rad.cpu())
+    barrier()
+    e2e_ms = 0.0
+    for _ in range(args.steps):
+        flush.fill_(1.0)
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(s)
+        sim.pos.copy_(h_pos, non_blocking=True)
+        sim.rad.copy_(h_rad, non_blocking=True)
+        one_step()
+        h_pos.copy_(sim.pos, non_blocking=True)
+        h_rad.copy_(sim.rad, non_blocking=True)
+        h_fsc.copy_(sim.fsc, non_blocking=True)
+        e1.record(s)
+        e1.synchronize()
+        e2e_ms += e0.elapsed_time(e1)
+    t = torch.tensor([e2e_ms], dtype=torch.float64, device=dev)
+    if world > 1:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    e2e_value = world * FRAMES_PER_STEP * args.steps / (float(t.item()) / 1000.0)
+
+    # ---- dominant kernel: the JFA pass, timed live on the launching stream
+    ctx = sim.ctx
+    reps = 10
+    barrier()
+    ctx.jfa_init(sim.pos, sim.rad, n)
+    j0 = torch.cuda.Event(enable_timing=True)
+    j1 = torch.cuda.Event(enable_timing=True)
+    jfa_ms = 0.0
+    for _ in range(reps):
+        flush.fill_(1.0)
+        ctx.jfa_init(sim.pos, sim.rad, n)
+        j0.record(s)
+        ctx.jfa_passes(n)
+        j1.record(s)
+        j1.synchronize()
+        jfa_ms += j0.elapsed_time(j1)
+    passes = ctx.num_passes
+    pass_s = jfa_ms / 1000.0 / (reps * passes)
+    V = foam.res ** 3
+    alg_bytes = 8.0 * V  # int32 label read + write per voxel per pass
+    achieved = alg_bytes / pass_s / 1e9
+    peaks = measured_peaks()
+    peak = peaks["hbm_gbs"] if peaks else 6650.0
+    traffic = profile_traffic()
+    st = FosJfaStats()
+    call("fos_jfa_stats", ctx.h, n, C.c_void_p(sim.rad.data_ptr()), C.byref(st), stream())
+    # FP32 issue bound: ~ 15 non-FMA FP32 ops per evaluated candidate (27 per voxel)
+    fp32_peak_tflops = 148 * 128 * 1.965e9 / 1e12
+
+    if world > 1:
+        dist.barrier()
+    if rank != 0:
+        if world > 1:
+            dist.destroy_process_group()
+        return 0
+
+    cpu = None
+    if not args.no_cpu_baseline:
+        fps, dt, cores = time_cpu(foam, args.cpu_sample_steps, 0)
+        cpu = {"value": round(fps, 4), "unit": UNIT, "cores": cores, "kind": "port",
+               "sample": f"{args.cpu_sample_steps} x 5-frame cadence cycle of the same workload "
+                         f"from a fresh warm-up-PBD foam at frame 20 ({dt:.1f} s, OpenMP oracle)"}
+    line = {
+        "metric": METRIC, "value": round(value, 3), "unit": UNIT, "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": round(total_ms / args.steps, 4), "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": workload_config(world),
+        "e2e": {"value": round(e2e_value, 3), "unit": UNIT, "h2d_bytes_per_step": n * 16,
+                "d2h_bytes_per_step": n * 20},
+        "roofline": {"bound": "hbm", "kernel": "k_jfa_pass (128^3, one pass)",
+                     "achieved": round(achieved, 2), "peak": peak, "unit": "GB/s",
+                     "frac": round(achieved / peak, 4),
+                     "peak_source": "measured (MEASURED_PEAKS.json hbm_gbs)" if peaks else
+                                    "fallback 6650 GB/s",
+                     "traffic": traffic.get("k_jfa_pass") if traffic else None,
+                     "alg_bytes_per_launch": alg_bytes, "pass_us": round(pass_s * 1e6, 3)},
+        "gpu_launches": int(launches),
+        "clocks": clk,
+        "cpu_baseline": cpu,
+        "diagnostics": {"finalize_iterations": st.finalize_iterations,
+                        "face_pairs": st.face_pairs, "mean_fsc": round(st.mean_fsc, 3),
+                        "fp32_peak_tflops_nominal": round(fp32_peak_tflops, 2)},
+    }
+    print(json.dumps(line), flush=True)
+    if world > 1:
+        dist.destroy_process_group()
+    return 0
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        return run_reference(args)
+    return run_fos(args)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

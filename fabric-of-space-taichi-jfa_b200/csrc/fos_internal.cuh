@@ -1,0 +1,237 @@
+// fos_internal.cuh -- context layout, error plumbing and device arithmetic
+// shared by the libfos.so translation units.
+//
+// Every FP32 expression that decides a label, a face or a neighbour is written
+// with explicit round-to-nearest intrinsics (__fadd_rn, __fmul_rn, ...) in the
+// operator order of the reference's Taichi source, so nvcc can never contract
+// it into an FMA; the library is also built with -fmad=false for the rest.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include <string>
+
+#include "fos.h"
+
+#define FOS_S 32          // MAX_NEIGHBORS (jfa.py:74)
+#define FOS_ROWCAP 64     // candidate partners kept per particle before the 32-slot cut
+#define FOS_FIN_MAXIT 4096
+#define FOS_BAR_SPIN_LIMIT (1u << 26)
+
+// ----------------------------------------------------------- device state
+// Small per-context block in device memory: the frame counters the frame
+// graph reads, the JFA early-exit bookkeeping, and error/diagnostic words.
+struct FosDevState {
+    int frame;          // device frame index (pressure hash, Brownian counter, warm gate)
+    int settle;         // settle_frames_left (run.py:744-750, 1231)
+    int error;          // first device-side error code (FOS_E_*), 0 = none
+    int passes_done;    // JFA passes actually run
+    int final_buf;      // 0: labels in buffer A, 1: in buffer B
+    int early_exited;
+    int pair_count;     // distinct {a,b} pairs claimed in the pair table
+    int row_overflow;   // particles with more than FOS_ROWCAP candidate partners
+    int max_rowcnt;
+    int fin_iters;      // fixed-point sweeps of the exact finalize
+    int zero_fsc;       // particles with fsc == 0 after finalize
+    int changed;        // pressure: particles with |dr| > 1e-12 (last sweep)
+    unsigned int maxabs_dr_bits;  // pressure: max |dr| of the last sweep (float bits)
+    unsigned int omax_bits;       // max overlap depth (float bits)
+    unsigned int bar_count;       // grid barrier arrival counter
+    unsigned int bar_gen;         // grid barrier generation
+    unsigned long long changes[FOS_MAX_PASSES];
+};
+
+struct FosGraphKey {
+    FosState st;
+    FosFrameParams fp;
+    int jfa;
+    int res;
+    FosParams p;
+};
+
+struct FosCtx {
+    int device = 0;
+    int max_n = 0, max_res = 0;
+    int num_sms = 0;
+    FosParams p{};
+    // resolution-derived (jfa.py:207-227)
+    int res = 0, passes = 0;
+    float vs = 0.f;
+    // folded constants (Python floats -> f32 as Taichi folds them)
+    float L = 1.f, halfL = 0.5f, invL = 1.f, beta = 1.f;
+    float face_scale = 1.5f, t_add = 0.15f, t_drop = 0.10f, ema_alpha = 0.33f;
+    float gap1 = 1.015f, mdf = 0.2f, dmul = 2.f, eps = 1e-8f, contact_tol = 0.035f;
+    float deadband = 1.f;
+    int G = 3;
+    // JFA fields
+    int32_t *labA = nullptr, *labB = nullptr, *filt = nullptr;
+    unsigned long long* seedslot = nullptr;
+    float4* seeds = nullptr;
+    int32_t *fsc = nullptr, *used = nullptr;
+    float* ema = nullptr;
+    int32_t *face_ids = nullptr, *face_counts = nullptr, *nl = nullptr;
+    float *face_score = nullptr, *prev = nullptr;
+    uint8_t *acc0 = nullptr, *acc1 = nullptr;
+    // pair table
+    size_t H = 0;
+    unsigned long long* hkeys = nullptr;
+    unsigned int *hmin = nullptr, *hcnt = nullptr, *claimed = nullptr;
+    int32_t* rowcnt = nullptr;
+    uint4* rowbuf = nullptr;
+    int32_t *revcnt = nullptr, *revstart = nullptr, *revfill = nullptr, *rev = nullptr;
+    // scratch
+    int32_t* scan_tmp = nullptr;      // block sums for the multi-block scan
+    size_t scan_tmp_n = 0;
+    float* pos_tmp = nullptr;         // [max_n*3]
+    float* rad_tmp = nullptr;         // [max_n]
+    int32_t *cellof = nullptr, *rank = nullptr;   // [max_n]
+    int32_t* cell_tmp = nullptr;      // [G^3]  (scatter's copy of cell_write)
+    size_t cell_tmp_n = 0;
+    float* stats_f = nullptr;         // device stats scratch
+    int32_t* stats_i = nullptr;
+    FosDevState* ds = nullptr;
+    int* fin_changed = nullptr;       // [FOS_FIN_MAXIT] per-sweep change flags of the finalize
+    void* pinned = nullptr;           // small host staging buffer
+    // graphs
+    cudaGraphExec_t gexec[2] = {nullptr, nullptr};
+    FosGraphKey gkey[2];
+    bool gvalid[2] = {false, false};
+    long long glaunch[2] = {0, 0};    // kernels per captured frame graph
+    long long launches = 0;
+};
+
+// ------------------------------------------------------------- host errors
+void fos_set_error(const std::string& msg);
+int fos_fail(int code, const char* what);
+int fos_cuda_fail(cudaError_t e, const char* what, const char* file, int line);
+
+#define FOS_CUDA(call)                                                         \
+    do {                                                                       \
+        cudaError_t e_ = (call);                                               \
+        if (e_ != cudaSuccess) return fos_cuda_fail(e_, #call, __FILE__, __LINE__); \
+    } while (0)
+
+#define FOS_LAUNCHED(ctx)                                                      \
+    do {                                                                       \
+        (ctx)->launches++;                                                     \
+        cudaError_t e_ = cudaPeekAtLastError();                                \
+        if (e_ != cudaSuccess) return fos_cuda_fail(e_, "kernel launch", __FILE__, __LINE__); \
+    } while (0)
+
+#define FOS_REQUIRE(cond, code, msg)                                           \
+    do {                                                                       \
+        if (!(cond)) return fos_fail((code), (msg));                           \
+    } while (0)
+
+inline int fos_blocks(long long work, int threads) {
+    long long b = (work + threads - 1) / threads;
+    return (int)(b < 1 ? 1 : b);
+}
+
+// Exclusive scan of n int32 values (d_in may equal d_out); d_out[n] gets the
+// total when with_total.  Launch-count aware.
+int fos_scan_exclusive(FosCtx* ctx, const int32_t* d_in, int32_t* d_out, int n, bool with_total,
+                       cudaStream_t s);
+
+// ------------------------------------------------------------ device math
+__device__ __forceinline__ float fadd(float a, float b) { return __fadd_rn(a, b); }
+__device__ __forceinline__ float fsub(float a, float b) { return __fsub_rn(a, b); }
+__device__ __forceinline__ float fmul(float a, float b) { return __fmul_rn(a, b); }
+__device__ __forceinline__ float fdiv(float a, float b) { return __fdiv_rn(a, b); }
+
+// jfa.wrapP (jfa.py:290-308): d - L*round(d/L).  With L == 1 the division and
+// multiplication by L are exact identities, so the UNIT_L form is bit-identical.
+template <bool UNIT_L>
+__device__ __forceinline__ float jfa_wrap(float d, float L) {
+    if (UNIT_L) return fsub(d, roundf(d));
+    return fsub(d, fmul(L, roundf(fdiv(d, L))));
+}
+
+// power_distance_sq (jfa.py:450-477) against a seed (x, y, z, (beta*r)^2).
+template <bool UNIT_L>
+__device__ __forceinline__ float power_dist(float vx, float vy, float vz, float4 s, float L) {
+    float dx = jfa_wrap<UNIT_L>(fsub(vx, s.x), L);
+    float dy = jfa_wrap<UNIT_L>(fsub(vy, s.y), L);
+    float dz = jfa_wrap<UNIT_L>(fsub(vz, s.z), L);
+    float d2 = fadd(fadd(fmul(dx, dx), fmul(dy, dy)), fmul(dz, dz));
+    return fsub(d2, s.w);
+}
+
+// voxel_to_world (jfa.py:273-287)
+__device__ __forceinline__ float voxel_centre(int idx, float vs, float halfL) {
+    return fsub(fmul(fadd((float)idx, 0.5f), vs), halfL);
+}
+
+// grid.wrapP (grid.py:30-48): p - L*floor(p*INV_L + 0.5)
+__device__ __forceinline__ float grid_wrap(float p, float L, float invL) {
+    return fsub(p, fmul(L, floorf(fadd(fmul(p, invL), 0.5f))));
+}
+
+__device__ __forceinline__ int wrap_small(int v, int R) {  // |v| < 2R
+    v += (v < 0) ? R : 0;
+    v -= (v >= R) ? R : 0;
+    return v;
+}
+
+__device__ __forceinline__ int wrap_mod(int v, int R) { return ((v % R) + R) % R; }
+
+// Order-preserving map of a float to uint32 (-0 folded onto +0 so that equal
+// floats map to equal keys, matching the reference's strict '<').
+__device__ __forceinline__ unsigned int float_order_key(float f) {
+    f = __fadd_rn(f, 0.0f);  // -0 + +0 = +0 under round-to-nearest
+    unsigned int u = __float_as_uint(f);
+    return (u & 0x80000000u) ? ~u : (u | 0x80000000u);
+}
+
+// Philox-4x32-10 (Salmon, Moraes, Dror, Shaw, SC'11).
+__device__ __forceinline__ uint4 philox4x32_10(uint4 c, uint32_t k0, uint32_t k1) {
+#pragma unroll
+    for (int r = 0; r < 10; ++r) {
+        uint32_t h0 = __umulhi(0xD2511F53u, c.x), l0 = 0xD2511F53u * c.x;
+        uint32_t h1 = __umulhi(0xCD9E8D57u, c.z), l1 = 0xCD9E8D57u * c.z;
+        uint4 n;
+        n.x = h1 ^ c.y ^ k0;
+        n.y = l1;
+        n.z = h0 ^ c.w ^ k1;
+        n.w = l0;
+        c = n;
+        k0 += 0x9E3779B9u;
+        k1 += 0xBB67AE85u;
+    }
+    return c;
+}
+
+// Software grid barrier for kernels launched cooperatively (all blocks
+// co-resident).  Bounded: gives up after FOS_BAR_SPIN_LIMIT polls, records
+// FOS_E_TIMEOUT in ds->error and returns false.
+__device__ __forceinline__ bool grid_barrier(FosDevState* ds) {
+    __syncthreads();
+    bool ok = true;
+    if (threadIdx.x == 0) {
+        volatile unsigned int* genp = &ds->bar_gen;
+        unsigned int gen = *genp;
+        __threadfence();
+        unsigned int arrived = atomicAdd(&ds->bar_count, 1u) + 1u;
+        if (arrived == gridDim.x) {
+            ds->bar_count = 0;
+            __threadfence();
+            atomicAdd(&ds->bar_gen, 1u);
+        } else {
+            unsigned int spins = 0;
+            while (*genp == gen) {
+                if (++spins > FOS_BAR_SPIN_LIMIT) {
+                    atomicCAS(&ds->error, 0, (int)FOS_E_TIMEOUT);
+                    ok = false;
+                    break;
+                }
+                __nanosleep(32);
+            }
+        }
+        __threadfence();
+    }
+    __shared__ int s_ok;
+    if (threadIdx.x == 0) s_ok = ok ? 1 : 0;
+    __syncthreads();
+    return s_ok != 0;
+}

@@ -1,0 +1,89 @@
+"""Headless frame driver: run.py's per-frame order (run.py:699-1261) on one GPU.
+
+``FoamSim`` owns the particle state (pos, rad, rad_target, local_max_depth,
+delta_r, hash-grid arrays) as torch CUDA tensors and a libfos ``Context``
+holding the JFA/FSC fields.  ``step()`` issues one frame through
+``fos_frame_graph``: the frame is captured once per kind (JFA frame /
+non-JFA frame) and replayed as a CUDA graph; the frame index, settle counter
+and warm-start gate live on the device, so no frame synchronises the host.
+"""
+from __future__ import annotations
+
+import ctypes as C
+
+import numpy as np
+import torch
+
+from ._lib import FosState, call
+from .config import FosConfig
+from .context import Context, stream
+
+
+class FoamSim:
+    def __init__(self, cfg: FosConfig, pos: np.ndarray, rad: np.ndarray, use_graph: bool = True,
+                 ctx: Context | None = None, device: int | None = None):
+        n = int(rad.shape[0])
+        self.cfg = cfg
+        self.n = n
+        self.use_graph = use_graph
+        self.ctx = ctx or Context(cfg, max_n=n, max_res=cfg.JFA_RES, device=device)
+        self.ctx.set_resolution(cfg.JFA_RES)
+        dev = torch.device("cuda", self.ctx.device)
+        G3 = cfg.grid_res() ** 3
+        self.pos = torch.as_tensor(np.ascontiguousarray(pos, np.float32).reshape(n, 3)).to(dev)
+        self.rad = torch.as_tensor(np.ascontiguousarray(rad, np.float32)).to(dev)
+        self.rad_target = self.rad.clone()
+        self.local_max_depth = torch.zeros(n, dtype=torch.float32, device=dev)
+        self.delta_r = torch.zeros(n, dtype=torch.float32, device=dev)
+        self.cell_count = torch.zeros(G3, dtype=torch.int32, device=dev)
+        self.cell_start = torch.zeros(G3, dtype=torch.int32, device=dev)
+        self.cell_indices = torch.zeros(n, dtype=torch.int32, device=dev)
+        self.state = FosState(n, self.pos.data_ptr(), self.rad.data_ptr(),
+                              self.rad_target.data_ptr(), self.local_max_depth.data_ptr(),
+                              self.delta_r.data_ptr(), self.cell_count.data_ptr(),
+                              self.cell_start.data_ptr(), self.cell_indices.data_ptr())
+        self.fp = cfg.frame_params()
+        self.frame = 0
+
+    @classmethod
+    def from_foam(cls, foam, use_graph: bool = True, **over) -> "FoamSim":
+        return cls(FosConfig.for_foam(foam, **over), foam.pos, foam.rad, use_graph=use_graph)
+
+    def initialize(self, frame0: int = 0):
+        """initialize_simulation's device part (run.py:320-382)."""
+        call("fos_sim_init", self.ctx.h, C.byref(self.state), C.byref(self.fp), int(frame0),
+             stream())
+        self.frame = int(frame0)
+
+    def step(self):
+        jfa = 1 if self.cfg.is_jfa_frame(self.frame) else 0
+        fn = "fos_frame_graph" if self.use_graph else "fos_frame"
+        call(fn, self.ctx.h, C.byref(self.state), C.byref(self.fp), jfa, stream())
+        self.frame += 1
+        return bool(jfa)
+
+    def run(self, frames: int):
+        for _ in range(frames):
+            self.step()
+
+    def counters(self):
+        f, s = C.c_int(), C.c_int()
+        call("fos_sim_counters", self.ctx.h, C.byref(f), C.byref(s), stream())
+        return f.value, s.value
+
+    # convenience views
+    @property
+    def fsc(self) -> torch.Tensor:
+        return self.ctx.fsc[: self.n]
+
+    @property
+    def fsc_ema(self) -> torch.Tensor:
+        return self.ctx.fsc_ema[: self.n]
+
+    @property
+    def face_ids(self) -> torch.Tensor:
+        return self.ctx.face_ids[: self.n]
+
+    @property
+    def neighbor_list(self) -> torch.Tensor:
+        return self.ctx.neighbor_list[: self.n]

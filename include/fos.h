@@ -1,0 +1,262 @@
+/*
+ * fos.h -- C ABI of the B200 foam hot path (libfos.so).
+ *
+ * Plain pointers and sizes only.  Every pointer argument named pos/rad/... is a
+ * DEVICE pointer (cudaMalloc'd, or a torch CUDA tensor's data_ptr()) unless
+ * its name ends in _host.  Every entry point returns an int status (FOS_OK = 0)
+ * and is asynchronous on the given stream, except where it says it
+ * synchronises (the ones that hand a scalar back to the host, as the
+ * reference's Taichi kernels with a return value do).  A context is not
+ * thread safe; use one per host thread.
+ *
+ * Reference interface each entry replaces (VirtualOrganics/Fabric-of-Space-
+ * Taichi-JFA, file:line) is cited beside it.  Layouts: pos is [n][3] float32,
+ * rad [n] float32, face_ids/face_counts/neighbor_list [n][32] int32, voxel
+ * (x,y,z) at linear index (x*R + y)*R + z.
+ */
+#ifndef FOS_H
+#define FOS_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct CUstream_st* fos_stream_t; /* == cudaStream_t; NULL = legacy default stream */
+
+#define FOS_MAX_NEIGHBORS 32 /* jfa.py:74 MAX_NEIGHBORS */
+#define FOS_MAX_PASSES 64
+
+enum FosStatus {
+    FOS_OK = 0,
+    FOS_E_ARG = 1,           /* bad argument (null pointer, n out of range, ...) */
+    FOS_E_CAPACITY = 2,      /* n or res above the context's capacity, table full */
+    FOS_E_CUDA = 3,          /* a CUDA runtime call failed */
+    FOS_E_TIMEOUT = 4,       /* a bounded device-side wait gave up */
+    FOS_E_DEVICE = 5,        /* a device-side check recorded an error word */
+    FOS_E_STATE = 6          /* call out of order (e.g. no JFA has run yet) */
+};
+
+/* Constants of config.py / jfa.py that the reference bakes into its kernels.
+ * Python-float constants are doubles here and are folded to float32 exactly as
+ * Taichi folds a Python float into a kernel literal. */
+typedef struct FosParams {
+    double domain_size;             /* DOMAIN_SIZE (config.py:21), L */
+    int grid_res;                   /* GRID_RES (config.py:317) */
+    double power_beta;              /* power_beta_current (jfa.py:184) */
+    int early_exit;                 /* JFA_EARLY_EXIT_ENABLED (config.py:208) */
+    int min_jfa_passes;             /* MIN_JFA_PASSES (config.py:210) */
+    double th_pass_delta;           /* TH_PASS_DELTA (config.py:209) */
+    int tie_lower_index;            /* 0: reference scan-order ties; 1: lower seed index wins */
+    double expected_face_scale;     /* EXPECTED_FACE_SCALE (jfa.py:58) */
+    double t_add;                   /* T_ADD (jfa.py:63) */
+    double t_drop;                  /* T_DROP (jfa.py:64) */
+    double ema_alpha;               /* JFA_EMA_ALPHA (config.py:81) */
+    double gap_fraction;            /* GAP_FRACTION (config.py:353) */
+    double max_displacement_frac;   /* MAX_DISPLACEMENT_FRAC (config.py:349) */
+    double displacement_multiplier; /* DISPLACEMENT_MULTIPLIER (config.py:350) */
+    double eps;                     /* EPS (config.py:324) */
+    double contact_tol;             /* CONTACT_TOL (config.py:254) */
+    double fsc_deadband;            /* FSC_DEADBAND (config.py:100) */
+} FosParams;
+
+typedef struct FosCtx FosCtx;
+
+/* Fills *p with the reference defaults (config.py / jfa.py). */
+void fos_params_default(FosParams* p);
+
+/* jfa.init_jfa (jfa.py:120-204): allocates every JFA/FSC field at capacity
+ * (max_n particles, max_res^3 voxels) on `device`.  The only entry point,
+ * with fos_ctx_destroy, that allocates or frees device memory. */
+int fos_ctx_create(const FosParams* p, int max_n, int max_res, int device, FosCtx** out);
+int fos_ctx_destroy(FosCtx* ctx);
+int fos_set_params(FosCtx* ctx, const FosParams* p);
+
+/* jfa.set_resolution (jfa.py:207-227) without the [JFA_RES_MIN, JFA_RES_MAX]
+ * clamp (the caller clamps): sets JFA_RES, VOXEL_SIZE = L/R and
+ * JFA_NUM_PASSES = ceil(log2 R) + 1.  res must be in [2, max_res]. */
+int fos_set_resolution(FosCtx* ctx, int res);
+int fos_get_resolution(FosCtx* ctx, int* res, int* num_passes, float* voxel_size);
+
+/* Device pointers of the context-owned fields (jfa.py module fields).  Any out
+ * pointer may be NULL.  labels is the final JFA owner grid of the last run
+ * (int32, R^3), label_filtered the majority-filtered grid. */
+typedef struct FosJfaFields {
+    int32_t* fsc;                  /* jfa.fsc            [max_n] */
+    float* fsc_ema;                /* jfa.fsc_ema        [max_n] */
+    int32_t* face_ids;             /* jfa.face_ids       [max_n][32] */
+    int32_t* face_counts;          /* jfa.face_counts    [max_n][32] */
+    int32_t* neighbor_list;        /* jfa.neighbor_list  [max_n][32] */
+    int32_t* neighbor_used_count;  /* jfa.neighbor_used_count [max_n] (== neighbor_count) */
+    float* neighbor_prev_scores;   /* jfa.neighbor_prev_scores [max_n][32] */
+    int32_t* labels;               /* final owner labels of the last run, R^3 */
+    int32_t* label_filtered;       /* jfa.label_filtered, R^3 */
+} FosJfaFields;
+int fos_jfa_fields(FosCtx* ctx, FosJfaFields* out);
+
+/* jfa.run_jfa (jfa.py:1056-1197), device part: jfa_init, the pass loop (with
+ * the optional device-side early exit), majority_filter_labels,
+ * accumulate_face_area, finalize_faces_kernel and update_fsc_ema.  Results
+ * land in the context's fields; nothing is copied to the host. */
+int fos_jfa_run(FosCtx* ctx, const float* pos, const float* rad, int n, fos_stream_t s);
+
+/* The stages of fos_jfa_run one by one (for tests and the Python mirror). */
+int fos_jfa_init(FosCtx* ctx, const float* pos, const float* rad, int n, fos_stream_t s); /* jfa.py:484-520 */
+int fos_jfa_passes(FosCtx* ctx, int n, fos_stream_t s);          /* jfa.py:1082-1116 (uses the seed table) */
+int fos_jfa_majority_filter(FosCtx* ctx, fos_stream_t s);        /* jfa.py:639-699 */
+int fos_jfa_accumulate_faces(FosCtx* ctx, int n, fos_stream_t s);/* jfa.py:702-762 */
+int fos_jfa_finalize(FosCtx* ctx, const float* rad, int n, fos_stream_t s); /* jfa.py:788-857 */
+int fos_jfa_update_ema(FosCtx* ctx, int n, fos_stream_t s);      /* jfa.py:765-785 */
+
+/* Load an owner grid (R^3 int32, device) as the "final labels" so the FSC
+ * stages can run on given labels (parity tests of the stages in isolation). */
+int fos_jfa_load_labels(FosCtx* ctx, const int32_t* labels, fos_stream_t s);
+
+/* run_jfa's stats dict (jfa.py:1149-1195) plus build diagnostics.  Synchronises. */
+typedef struct FosJfaStats {
+    int num_passes;
+    int early_exit;
+    long long changes[FOS_MAX_PASSES]; /* label_changes per pass (delta_history * V) */
+    int jfa_res;
+    float voxel_size;
+    float mean_score, std_score;       /* compute_score_stats (jfa.py:1257-1330) */
+    int p_dir, p_und_accepted;         /* compute_pair_symmetry (jfa.py:1204-1220) */
+    int overflow_count;                /* compute_overflow_count (jfa.py:1223-1234) */
+    float overflow_pct;
+    float mean_fsc;                    /* compute_fsc_stats (jfa.py:1237-1254) */
+    int min_fsc, max_fsc;
+    float mean_fsc_ema;
+    int finalize_iterations;           /* fixed-point sweeps the exact finalize took */
+    int face_pairs;                    /* distinct {a,b} pairs found this run */
+    int max_row_candidates;            /* largest per-particle candidate count */
+    int zero_fsc_count;                /* particles with fsc == 0 */
+} FosJfaStats;
+int fos_jfa_stats(FosCtx* ctx, int n, const float* rad, FosJfaStats* out, fos_stream_t s);
+
+/* validate_jfa (jfa.py:1400-1426).  Synchronises. */
+typedef struct FosValidate {
+    int passed, asymmetric_pairs, overflow_count, self_loops;
+} FosValidate;
+int fos_jfa_validate(FosCtx* ctx, int n, FosValidate* out, fos_stream_t s);
+
+/* ------------------------------------------------------------------- grid.py
+ * Cell arrays are [GRID_RES^3] int32, cell_indices [n] int32. */
+int fos_grid_clear(FosCtx* ctx, int32_t* cell_count, fos_stream_t s);                  /* grid.py:145-155 */
+int fos_grid_count(FosCtx* ctx, const float* pos, int32_t* cell_count, int n, fos_stream_t s); /* grid.py:186-222 */
+int fos_grid_prefix_sum(FosCtx* ctx, const int32_t* cell_count, int32_t* cell_start, fos_stream_t s); /* grid.py:229-243 */
+int fos_grid_copy_pointers(FosCtx* ctx, const int32_t* cell_start, int32_t* cell_write, fos_stream_t s); /* grid.py:250-261 */
+/* scatter_particles (grid.py:268-309): wraps pos in place; each cell's slice of
+ * cell_indices is ascending (the serial order), cell_write ends at cell end. */
+int fos_grid_scatter(FosCtx* ctx, float* pos, int32_t* cell_write, int32_t* cell_indices, int n,
+                     fos_stream_t s);
+/* rebuild_grid (run.py:476-504) in one call: clear, count, scan, scatter. */
+int fos_grid_build(FosCtx* ctx, float* pos, int n, int32_t* cell_count, int32_t* cell_start,
+                   int32_t* cell_indices, fos_stream_t s);
+
+/* --------------------------------------------------------------- dynamics.py */
+/* project_overlaps (dynamics.py:77-171) as one Jacobi sweep; pos updated in place. */
+int fos_project_overlaps(FosCtx* ctx, float* pos, const float* rad, const int32_t* cell_start,
+                         const int32_t* cell_count, const int32_t* cell_indices, int n,
+                         fos_stream_t s);
+/* compute_max_overlap (dynamics.py:304-372): fills local_max_depth; the global
+ * max goes to *max_host (synchronises) and/or *max_dev (async); either may be NULL. */
+int fos_compute_max_overlap(FosCtx* ctx, const float* pos, const float* rad,
+                            const int32_t* cell_start, const int32_t* cell_count,
+                            const int32_t* cell_indices, float* local_max_depth, int n,
+                            float* max_dev, float* max_host, fos_stream_t s);
+/* equilibrate_pressure (dynamics.py:1454-1557), `sweeps` Jacobi sweeps with the
+ * same frame.  max_abs_dr_host/changed_host (of the last sweep) synchronise
+ * when non-NULL. */
+int fos_equilibrate_pressure(FosCtx* ctx, int n, int frame, float* rad, float* delta_r,
+                             const int32_t* face_ids, const int32_t* fsc, float k, float p_exp,
+                             float pair_cap, int max_nei, float r_min, float r_max, int sweeps,
+                             float* max_abs_dr_host, int* changed_host, fos_stream_t s);
+/* apply_brownian_motion (dynamics.py:1596-1634) with Philox-4x32-10 keyed by
+ * (seed, frame, particle) in place of ti.random(). */
+int fos_apply_brownian(FosCtx* ctx, float* pos, int n, float strength, float domain_size,
+                       uint64_t seed, uint32_t frame, fos_stream_t s);
+/* set_fsc_targets (dynamics.py:1242-1320) */
+int fos_set_fsc_targets(FosCtx* ctx, const float* rad, float* rad_target, const int32_t* fsc,
+                        const float* fsc_ema, int n, int f_low, int f_high, float growth_pct,
+                        float r_min, float r_max, fos_stream_t s);
+/* nudge_radii_adaptive_ema (dynamics.py:1366-1427); mode 0 off, 1 global, 2 local */
+int fos_nudge_radii(FosCtx* ctx, float* rad, const float* rad_target, const float* local_max_depth,
+                    int n, float alpha, float max_step_pct, float r_min, float r_max,
+                    float back_global, int mode, fos_stream_t s);
+/* compute_controller_stats (dynamics.py:1322-1363).  Synchronises. */
+int fos_controller_stats(FosCtx* ctx, const float* rad, const float* rad_target,
+                         const float* fsc_ema, int n, int f_low, int f_high, int* grow,
+                         int* shrink, int* idle, float* mean_dr, float* max_dr, fos_stream_t s);
+/* compute_pressure_stats (dynamics.py:1560-1589).  Synchronises. */
+int fos_pressure_stats(FosCtx* ctx, int n, const float* rad, float* rmin, float* rmax,
+                       fos_stream_t s);
+
+/* ------------------------------------------------------------ frame driver
+ * One headless frame in run.py's order (run.py:699-1261): grid build; max
+ * overlap; settle nudge while the device settle counter is > 0; `pressure_iters`
+ * pressure sweeps on the last JFA's face_ids/fsc; Brownian jitter; pbd_iters x
+ * {grid build; PBD}; grid build; and on a JFA frame run_jfa, the warm-start
+ * gate (frame < warmstart_frames or zero-FSC fraction > zero_rate_thresh) and
+ * set_fsc_targets + settle = adjustment_frames.  The frame index, settle
+ * counter and gate live on the device, so a frame does no host sync and can be
+ * replayed from a CUDA graph. */
+typedef struct FosFrameParams {
+    int pbd_iters;
+    int pressure_iters;
+    int f_low, f_high;            /* FSC band */
+    double growth_pct;            /* GROWTH_PCT */
+    double max_step_pct;          /* MAX_STEP_PCT */
+    int adjustment_frames;        /* ADJUSTMENT_FRAMES */
+    int bp_mode;                  /* BACKPRESSURE_MODE: 0 off, 1 global, 2 local */
+    int warmstart_frames;         /* WARMSTART_FRAMES */
+    double zero_rate_thresh;      /* FSC_ZERO_RATE_THRESH */
+    double r_min, r_max;          /* R_MIN, R_MAX */
+    double pressure_k, pressure_exp, pressure_pair_cap; /* PRESSURE_K/EXP/PAIR_CAP */
+    int max_eq_nei;               /* MAX_EQ_NEI */
+    double brownian_strength;     /* BROWNIAN_STRENGTH (uniform +-strength per axis) */
+    uint64_t seed;                /* Philox key of the Brownian jitter */
+    int warmup_pbd;               /* PBD_BASE_PASSES used by fos_sim_init */
+} FosFrameParams;
+
+/* Caller-owned per-particle state (run.py's fields). */
+typedef struct FosState {
+    int n;
+    float* pos;                 /* [n][3] */
+    float* rad;                 /* [n] */
+    float* rad_target;          /* [n] */
+    float* local_max_depth;     /* [n] */
+    float* delta_r;             /* [n] */
+    int32_t* cell_count;        /* [GRID_RES^3] */
+    int32_t* cell_start;        /* [GRID_RES^3] */
+    int32_t* cell_indices;      /* [n] */
+} FosState;
+
+void fos_frame_params_default(FosFrameParams* fp);
+/* initialize_simulation's device part (run.py:320-382): wrap positions, run
+ * warmup_pbd passes, zero fsc/fsc_ema/face_ids/prev scores, set rad_target =
+ * rad and reset the device frame index to frame0 and the settle counter. */
+int fos_sim_init(FosCtx* ctx, const FosState* st, const FosFrameParams* fp, int frame0,
+                 fos_stream_t s);
+int fos_frame(FosCtx* ctx, const FosState* st, const FosFrameParams* fp, int jfa_frame,
+              fos_stream_t s);
+/* Same frame replayed from a CUDA graph captured on first use per
+ * (state, params, jfa_frame); recaptured when any of them changes. */
+int fos_frame_graph(FosCtx* ctx, const FosState* st, const FosFrameParams* fp, int jfa_frame,
+                    fos_stream_t s);
+/* Device frame index and settle counter (synchronises). */
+int fos_sim_counters(FosCtx* ctx, int* frame, int* settle, fos_stream_t s);
+
+/* Number of this library's kernel launches issued so far on ctx (host count). */
+long long fos_launch_count(FosCtx* ctx);
+/* Device error word (synchronises) and a static string for a status code. */
+int fos_device_error(FosCtx* ctx, int* word, fos_stream_t s);
+const char* fos_status_string(int status);
+/* Thread-local text of the last error raised by any entry point. */
+const char* fos_last_error(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* FOS_H */

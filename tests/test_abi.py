@@ -1,0 +1,56 @@
+"""The C-ABI library builds, loads and exports every symbol include/fos.h declares."""
+import os
+import re
+import subprocess
+
+import pytest
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+def declared_symbols():
+    src = open(os.path.join(ROOT, "include", "fos.h")).read()
+    src = re.sub(r"/\*.*?\*/", "", src, flags=re.S)
+    return sorted(set(re.findall(r"\b(fos_[a-z0-9_]+)\s*\(", src)))
+
+
+@pytest.fixture(scope="module")
+def lib_path():
+    from fos import build
+    return build.build()
+
+
+def test_header_declares_entry_points():
+    syms = declared_symbols()
+    assert "fos_jfa_run" in syms and "fos_frame_graph" in syms
+    assert len(syms) >= 40
+
+
+def test_library_exports_every_declared_symbol(lib_path):
+    out = subprocess.run(["nm", "-D", "--defined-only", lib_path], capture_output=True, text=True,
+                         check=True).stdout
+    exported = set(re.findall(r"\bT (fos_[a-z0-9_]+)", out))
+    missing = [s for s in declared_symbols() if s not in exported]
+    assert not missing, missing
+
+
+def test_ctypes_binding_covers_header(lib_path):
+    from fos import _lib
+    lib = _lib.load()
+    for s in declared_symbols():
+        assert hasattr(lib, s), s
+        assert s in _lib.SIGNATURES, f"{s} has no ctypes signature"
+
+
+def test_status_strings_without_gpu(lib_path):
+    from fos import _lib
+    lib = _lib.load()
+    assert lib.fos_status_string(0) == b"FOS_OK"
+    assert lib.fos_status_string(2) == b"FOS_E_CAPACITY"
+    import ctypes as C
+    p = _lib.FosParams()
+    lib.fos_params_default(C.byref(p))
+    assert p.t_add == 0.15 and p.t_drop == 0.10 and p.expected_face_scale == 1.5
+    # argument validation needs no device
+    assert lib.fos_ctx_create(None, 10, 64, 0, C.byref(C.c_void_p())) == 1
+    assert lib.fos_set_resolution(None, 64) == 1
