@@ -44,6 +44,10 @@ def parse():
     ap.add_argument("--impl", default="fos", choices=["fos", "reference"])
     ap.add_argument("--cpu-sample-steps", type=int, default=1)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--profile", default=None, choices=["jfa", "frame"],
+                    help="stage-timing mode for profiling (one small JSON line)")
+    ap.add_argument("--reps", type=int, default=5)
+    ap.add_argument("--workload", default="headline", choices=["small", "headline", "stress"])
     return ap.parse_args()
 
 
@@ -228,6 +232,7 @@ def run_fos(args):
     clocks = Clocks(dev)
     clocks.start()
     launches0 = sim.ctx.launch_count()
+    torch_kernels_before = 1 + 8  # flush buffer fill + state tensor fills
     s = torch.cuda.current_stream()
     times = []
     barrier()
@@ -337,7 +342,8 @@ def run_fos(args):
         "gpu_launches": int(launches),
         "clocks": clk,
         "cpu_baseline": cpu,
-        "diagnostics": {"finalize_iterations": st.finalize_iterations,
+        "diagnostics": {"launches_before_timed": int(launches0 + torch_kernels_before),
+                        "finalize_iterations": st.finalize_iterations,
                         "face_pairs": st.face_pairs, "mean_fsc": round(st.mean_fsc, 3),
                         "fp32_peak_tflops_nominal": round(fp32_peak_tflops, 2)},
     }
@@ -347,8 +353,84 @@ def run_fos(args):
     return 0
 
 
+def run_profile(args):
+    """Stage timings of one workload with CUDA events (used under ncu as well)."""
+    import numpy as np
+    import torch
+
+    from fos import inputs
+    from fos.config import FosConfig
+    from fos.context import Context
+    from fos.driver import FoamSim
+
+    torch.cuda.set_device(0)
+    foam = inputs.WORKLOADS[args.workload]()
+    s = torch.cuda.current_stream()
+    out = {"profile": args.profile, "workload": foam.name, "reps": args.reps}
+    if args.profile == "jfa":
+        cfg = FosConfig.for_foam(foam)
+        ctx = Context(cfg, max_n=foam.n, max_res=cfg.JFA_RES)
+        f = np.float32
+        p = foam.pos - np.floor(foam.pos + f(0.5))
+        pos = torch.as_tensor(np.ascontiguousarray(p, np.float32)).cuda()
+        rad = torch.as_tensor(foam.rad).cuda()
+        stages = {"init": lambda: ctx.jfa_init(pos, rad, foam.n),
+                  "passes": lambda: ctx.jfa_passes(foam.n),
+                  "filter": ctx.majority_filter,
+                  "faces": lambda: ctx.accumulate_faces(foam.n),
+                  "finalize": lambda: ctx.finalize(rad, foam.n)}
+        acc = {k: 0.0 for k in stages}
+        for r in range(args.reps + 1):
+            for k, fn in stages.items():
+                a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                a.record(s)
+                fn()
+                b.record(s)
+                b.synchronize()
+                if r > 0:
+                    acc[k] += a.elapsed_time(b)
+        out["ms"] = {k: round(v / args.reps, 4) for k, v in acc.items()}
+        out["passes"] = ctx.num_passes
+        out["stats"] = {k: v for k, v in ctx.jfa_stats(foam.n, rad).items()
+                        if k in ("finalize_iterations", "face_pairs", "mean_fsc",
+                                 "max_row_candidates")}
+    else:
+        sim = FoamSim.from_foam(foam, use_graph=True)
+        sim.initialize()
+        for _ in range(min(foam.jfa_warm, 25)):
+            sim.step()
+        ms = {"jfa_frame": 0.0, "plain_frame": 0.0}
+        cnt = {"jfa_frame": 0, "plain_frame": 0}
+        for r in range(args.reps * 5):
+            a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            a.record(s)
+            jfa = sim.step()
+            b.record(s)
+            b.synchronize()
+            k = "jfa_frame" if jfa else "plain_frame"
+            ms[k] += a.elapsed_time(b)
+            cnt[k] += 1
+        out["ms"] = {k: round(ms[k] / max(1, cnt[k]), 4) for k in ms}
+        out["frames"] = cnt
+        # per-stage breakdown (event after every stage, no graph)
+        stages = {"jfa_frame": {}, "plain_frame": {}}
+        nst = {"jfa_frame": 0, "plain_frame": 0}
+        for r in range(args.reps * 5):
+            d = sim.step_profiled()
+            k = "jfa_frame" if d.pop("jfa") else "plain_frame"
+            nst[k] += 1
+            for st, v in d.items():
+                stages[k][st] = stages[k].get(st, 0.0) + v
+        out["stages_ms"] = {k: {st: round(v / max(1, nst[k]), 4) for st, v in d.items()}
+                            for k, d in stages.items()}
+    print(json.dumps(out), flush=True)
+    return 0
+
+
 def main():
     args = parse()
+    if args.profile:
+        return run_profile(args)
     if args.impl == "reference":
         return run_reference(args)
     return run_fos(args)

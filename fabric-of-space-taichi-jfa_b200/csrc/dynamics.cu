@@ -17,116 +17,170 @@ __device__ __forceinline__ int home_coord(float p, float L, float invL, float ha
     return (int)fmul(q, (float)G);
 }
 
-// project_overlaps (dynamics.py:77-171) as one Jacobi sweep: read pos_in,
-// write pos_out (the reference updates in place with atomics, so its result
-// depends on scheduling; the Jacobi form is the deterministic restatement).
-__global__ void __launch_bounds__(128) k_pbd(const float* __restrict__ pin, float* __restrict__ pout,
-                                             const float* __restrict__ rad, int n, int G, float L,
-                                             float invL, float halfL,
-                                             const int32_t* __restrict__ cs,
-                                             const int32_t* __restrict__ cc,
-                                             const int32_t* __restrict__ ci, float gap1, float mdf,
-                                             float dmul) {
-    int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= n) return;
-    float px = pin[3 * i + 0], py = pin[3 * i + 1], pz = pin[3 * i + 2];
-    float ri = rad[i];
+// ------------------------------------------------------------------
+// Warp-cooperative enumeration of a particle's 27-cell neighbourhood.
+// Lane l < 27 owns cell l of the stencil in the reference's (dx, dy, dz)
+// order (dz fastest); an inclusive warp scan of the cell counts numbers the
+// candidates 0..total-1 in exactly the order of the reference's nested loops
+// (cells in stencil order, particles ascending inside a cell).  Candidate t
+// is located by a binary search over the scanned counts.
+struct Stencil {
+    int st, excl, incl, total;
+};
+
+__device__ __forceinline__ Stencil stencil_ranges(float px, float py, float pz, float L, float invL,
+                                                  float halfL, int G,
+                                                  const int32_t* __restrict__ cs,
+                                                  const int32_t* __restrict__ cc, int lane) {
     int hx = home_coord(px, L, invL, halfL, G);
     int hy = home_coord(py, L, invL, halfL, G);
     int hz = home_coord(pz, L, invL, halfL, G);
-    float cx = 0.f, cy = 0.f, cz = 0.f;
-    float md = fmul(mdf, ri);
-    for (int dx = -1; dx <= 1; ++dx) {
-        int nx = wrap_mod(hx + dx, G);
-        for (int dy = -1; dy <= 1; ++dy) {
-            int ny = wrap_mod(hy + dy, G);
-            for (int dz = -1; dz <= 1; ++dz) {
-                int nz = wrap_mod(hz + dz, G);
-                int cid = (nx * G + ny) * G + nz;
-                int st = cs[cid], ct = cc[cid];
-                for (int k = st; k < st + ct; ++k) {
-                    int j = ci[k];
-                    if (j == i) continue;
-                    float ddx = grid_wrap(fsub(pin[3 * j + 0], px), L, invL);
-                    float ddy = grid_wrap(fsub(pin[3 * j + 1], py), L, invL);
-                    float ddz = grid_wrap(fsub(pin[3 * j + 2], pz), L, invL);
-                    float d2 = fadd(fadd(fadd(fmul(ddx, ddx), fmul(ddy, ddy)), fmul(ddz, ddz)), 1e-12f);
-                    float dist = __fsqrt_rn(d2);
-                    float tsep = fmul(fadd(ri, rad[j]), gap1);
-                    if (dist < tsep) {
-                        float ov = fsub(tsep, dist);
-                        float ux = fdiv(ddx, dist), uy = fdiv(ddy, dist), uz = fdiv(ddz, dist);
-                        float mag = fminf(fmul(ov, 0.5f), md);
-                        float vx = fmul(-ux, mag), vy = fmul(-uy, mag), vz = fmul(-uz, mag);
-                        vx = fmaxf(-md, fminf(md, vx));
-                        vy = fmaxf(-md, fminf(md, vy));
-                        vz = fmaxf(-md, fminf(md, vz));
-                        cx = fadd(cx, vx);
-                        cy = fadd(cy, vy);
-                        cz = fadd(cz, vz);
-                    }
-                }
-            }
-        }
+    int st = 0, ct = 0;
+    if (lane < 27) {
+        int nx = wrap_mod(hx + lane / 9 - 1, G);
+        int ny = wrap_mod(hy + (lane / 3) % 3 - 1, G);
+        int nz = wrap_mod(hz + lane % 3 - 1, G);
+        int cid = (nx * G + ny) * G + nz;
+        st = cs[cid];
+        ct = cc[cid];
     }
-    float mt = fmul(fmul(mdf, ri), dmul);
-    float cm = __fsqrt_rn(fadd(fadd(fmul(cx, cx), fmul(cy, cy)), fmul(cz, cz)));
-    if (cm > mt) {
-        float sc = fdiv(mt, cm);
-        cx = fmul(cx, sc);
-        cy = fmul(cy, sc);
-        cz = fmul(cz, sc);
+    int incl = ct;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        int y = __shfl_up_sync(0xffffffffu, incl, o);
+        if (lane >= o) incl += y;
     }
-    pout[3 * i + 0] = grid_wrap(fadd(px, cx), L, invL);
-    pout[3 * i + 1] = grid_wrap(fadd(py, cy), L, invL);
-    pout[3 * i + 2] = grid_wrap(fadd(pz, cz), L, invL);
+    Stencil r;
+    r.st = st;
+    r.incl = incl;
+    r.excl = incl - ct;
+    r.total = __shfl_sync(0xffffffffu, incl, 31);
+    return r;
 }
 
-// compute_local_max_overlaps + reduce_max_depth (dynamics.py:304-372).
-__global__ void __launch_bounds__(128) k_max_overlap(const float* __restrict__ pos,
-                                                     const float* __restrict__ rad, int n, int G,
-                                                     float L, float invL, float halfL,
-                                                     const int32_t* __restrict__ cs,
-                                                     const int32_t* __restrict__ cc,
-                                                     const int32_t* __restrict__ ci, float eps,
-                                                     float* __restrict__ lmd,
-                                                     unsigned int* gmax_bits) {
-    int i = blockIdx.x * blockDim.x + threadIdx.x;
-    float lm = 0.f;
-    if (i < n) {
-        float px = pos[3 * i + 0], py = pos[3 * i + 1], pz = pos[3 * i + 2];
-        float ri = rad[i];
-        int hx = home_coord(px, L, invL, halfL, G);
-        int hy = home_coord(py, L, invL, halfL, G);
-        int hz = home_coord(pz, L, invL, halfL, G);
-        for (int dx = -1; dx <= 1; ++dx) {
-            int nx = wrap_mod(hx + dx, G);
-            for (int dy = -1; dy <= 1; ++dy) {
-                int ny = wrap_mod(hy + dy, G);
-                for (int dz = -1; dz <= 1; ++dz) {
-                    int nz = wrap_mod(hz + dz, G);
-                    int cid = (nx * G + ny) * G + nz;
-                    int st = cs[cid], ct = cc[cid];
-                    for (int k = st; k < st + ct; ++k) {
-                        int j = ci[k];
-                        if (!(i < j)) continue;
-                        float ddx = grid_wrap(fsub(pos[3 * j + 0], px), L, invL);
-                        float ddy = grid_wrap(fsub(pos[3 * j + 1], py), L, invL);
-                        float ddz = grid_wrap(fsub(pos[3 * j + 2], pz), L, invL);
-                        float dist = __fsqrt_rn(
-                            fadd(fadd(fadd(fmul(ddx, ddx), fmul(ddy, ddy)), fmul(ddz, ddz)), eps));
-                        float td = fadd(ri, rad[j]);
-                        if (dist < td) lm = fmaxf(lm, fsub(td, dist));
-                    }
-                }
+// Sorted-array position of candidate t (t < total).
+__device__ __forceinline__ int stencil_locate(const Stencil& r, int t) {
+    int c = 0;
+#pragma unroll
+    for (int step = 16; step >= 1; step >>= 1) {
+        int v = __shfl_sync(0xffffffffu, r.incl, c + step - 1);
+        if (v <= t) c += step;
+    }
+    int src = c & 31;
+    int st = __shfl_sync(0xffffffffu, r.st, src);
+    int ex = __shfl_sync(0xffffffffu, r.excl, src);
+    return st + (t - ex);
+}
+
+// project_overlaps (dynamics.py:77-171) as one Jacobi sweep: every particle
+// reads the pre-sweep positions (the cell-ordered copy sp, which holds pos and
+// rad) and writes pout (the reference updates in place with atomics, so its
+// result depends on scheduling; the Jacobi form is the deterministic
+// restatement).  One warp per particle: lanes evaluate 32 candidates at a
+// time, and the corrections of overlapping pairs are added in candidate
+// order, so the FP32 sum is the reference loop's sum bit for bit.
+__global__ void __launch_bounds__(256) k_pbd(const float4* __restrict__ sp,
+                                             const int32_t* __restrict__ ci,
+                                             float* __restrict__ pout, int n, int G, float L,
+                                             float invL, float halfL,
+                                             const int32_t* __restrict__ cs,
+                                             const int32_t* __restrict__ cc, float gap1, float mdf,
+                                             float dmul) {
+    int kk = (int)(((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5);
+    int lane = threadIdx.x & 31;
+    if (kk >= n) return;  // warp-uniform
+    float4 me = sp[kk];
+    float px = me.x, py = me.y, pz = me.z, ri = me.w;
+    Stencil r = stencil_ranges(px, py, pz, L, invL, halfL, G, cs, cc, lane);
+    float md = fmul(mdf, ri);
+    float cx = 0.f, cy = 0.f, cz = 0.f;
+    for (int base = 0; base < r.total; base += 32) {
+        int t = base + lane;
+        int k = stencil_locate(r, t < r.total ? t : r.total - 1);
+        bool hit = false;
+        float vx = 0.f, vy = 0.f, vz = 0.f;
+        if (t < r.total && k != kk) {
+            float4 q = sp[k];
+            float ddx = grid_wrap(fsub(q.x, px), L, invL);
+            float ddy = grid_wrap(fsub(q.y, py), L, invL);
+            float ddz = grid_wrap(fsub(q.z, pz), L, invL);
+            float d2 = fadd(fadd(fadd(fmul(ddx, ddx), fmul(ddy, ddy)), fmul(ddz, ddz)), 1e-12f);
+            float dist = __fsqrt_rn(d2);
+            float tsep = fmul(fadd(ri, q.w), gap1);
+            if (dist < tsep) {
+                hit = true;
+                float ov = fsub(tsep, dist);
+                float ux = fdiv(ddx, dist), uy = fdiv(ddy, dist), uz = fdiv(ddz, dist);
+                float mag = fminf(fmul(ov, 0.5f), md);
+                vx = fmaxf(-md, fminf(md, fmul(-ux, mag)));
+                vy = fmaxf(-md, fminf(md, fmul(-uy, mag)));
+                vz = fmaxf(-md, fminf(md, fmul(-uz, mag)));
             }
         }
-        lmd[i] = lm;
+        unsigned int m = __ballot_sync(0xffffffffu, hit);
+        while (m) {
+            int b = __ffs(m) - 1;
+            m &= m - 1;
+            cx = fadd(cx, __shfl_sync(0xffffffffu, vx, b));
+            cy = fadd(cy, __shfl_sync(0xffffffffu, vy, b));
+            cz = fadd(cz, __shfl_sync(0xffffffffu, vz, b));
+        }
     }
-    // warp max, then one atomic per warp (non-negative floats order as uints)
-    unsigned int b = __float_as_uint(lm);
-    b = __reduce_max_sync(0xffffffffu, b);
-    if ((threadIdx.x & 31) == 0 && b) atomicMax(gmax_bits, b);
+    if (lane == 0) {
+        float mt = fmul(fmul(mdf, ri), dmul);
+        float cm = __fsqrt_rn(fadd(fadd(fmul(cx, cx), fmul(cy, cy)), fmul(cz, cz)));
+        if (cm > mt) {
+            float sc = fdiv(mt, cm);
+            cx = fmul(cx, sc);
+            cy = fmul(cy, sc);
+            cz = fmul(cz, sc);
+        }
+        int i = ci[kk];
+        pout[3 * i + 0] = grid_wrap(fadd(px, cx), L, invL);
+        pout[3 * i + 1] = grid_wrap(fadd(py, cy), L, invL);
+        pout[3 * i + 2] = grid_wrap(fadd(pz, cz), L, invL);
+    }
+}
+
+// compute_local_max_overlaps + reduce_max_depth (dynamics.py:304-372), one
+// warp per particle over the same candidate enumeration (pairs i < j only).
+__global__ void __launch_bounds__(256) k_max_overlap(const float4* __restrict__ sp,
+                                                     const int32_t* __restrict__ ci, int n, int G,
+                                                     float L, float invL, float halfL,
+                                                     const int32_t* __restrict__ cs,
+                                                     const int32_t* __restrict__ cc, float eps,
+                                                     float* __restrict__ lmd,
+                                                     unsigned int* gmax_bits) {
+    int kk = (int)(((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5);
+    int lane = threadIdx.x & 31;
+    if (kk >= n) return;  // warp-uniform
+    float4 me = sp[kk];
+    int i = ci[kk];
+    Stencil r = stencil_ranges(me.x, me.y, me.z, L, invL, halfL, G, cs, cc, lane);
+    float lm = 0.f;
+    for (int base = 0; base < r.total; base += 32) {
+        int t = base + lane;
+        int k = stencil_locate(r, t < r.total ? t : r.total - 1);
+        if (t < r.total) {
+            int j = ci[k];
+            if (i < j) {
+                float4 q = sp[k];
+                float ddx = grid_wrap(fsub(q.x, me.x), L, invL);
+                float ddy = grid_wrap(fsub(q.y, me.y), L, invL);
+                float ddz = grid_wrap(fsub(q.z, me.z), L, invL);
+                float dist = __fsqrt_rn(
+                    fadd(fadd(fadd(fmul(ddx, ddx), fmul(ddy, ddy)), fmul(ddz, ddz)), eps));
+                float td = fadd(me.w, q.w);
+                if (dist < td) lm = fmaxf(lm, fsub(td, dist));
+            }
+        }
+    }
+    // max is exact in any order; non-negative floats order as their bits
+    unsigned int b = __reduce_max_sync(0xffffffffu, __float_as_uint(lm));
+    if (lane == 0) {
+        lmd[i] = __uint_as_float(b);
+        if (b) atomicMax(gmax_bits, b);
+    }
 }
 
 // hash_func (dynamics.py:1436-1451) in wrapping int32 arithmetic.
@@ -136,8 +190,12 @@ __device__ __forceinline__ int hash_func(int i, int frame) {
 }
 
 // equilibrate_pressure (dynamics.py:1454-1557), one Jacobi sweep: reads
-// rad_in, writes rad_out and delta_r.  Stats of this sweep go to slot
-// `slot` of pmax/pchanged; the other slot is cleared for the next sweep.
+// rad_in, writes rad_out and delta_r.  GS lanes per particle: lane t handles
+// the t-th budgeted neighbour of the hashed rotation, and the radius deltas
+// are summed in neighbour order (the reference's serial accumulation order).
+// Stats of this sweep go to slot `slot` of pmax/pchanged; the other slot is
+// cleared for the next sweep.
+template <int GS>
 __global__ void __launch_bounds__(256) k_pressure(int n, int frame_arg, const int* frame_ptr,
                                                   const float* __restrict__ rin,
                                                   float* __restrict__ rout,
@@ -147,43 +205,61 @@ __global__ void __launch_bounds__(256) k_pressure(int n, int frame_arg, const in
                                                   float P, float cap, int max_nei, float rmin,
                                                   float rmax, unsigned int* pmax, int* pchanged,
                                                   int slot) {
-    int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i == 0) {
+    long long tid = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (tid == 0) {
         pmax[slot ^ 1] = 0u;
         pchanged[slot ^ 1] = 0;
     }
+    int lane = threadIdx.x & 31;
+    int gl = lane & (GS - 1);
+    unsigned int gmask = GS == 32 ? 0xffffffffu : (0xffffu << (lane & 16));
+    int i = (int)(tid / GS);
+    bool live = i < n;
+    int frame = frame_ptr ? *frame_ptr : frame_arg;
+    float ri = live ? rin[i] : 0.f;
+    int fc = live ? fsc[i] : 0;
     float d = 0.f;
-    if (i < n) {
-        int frame = frame_ptr ? *frame_ptr : frame_arg;
-        float ri = rin[i];
+    if (fc > 0) {
+        int an = fc < max_nei ? fc : max_nei;
+        int st = hash_func(i, frame) % fc;
         float Vi = powf(ri, P);
-        int fc = fsc[i];
-        if (fc > 0) {
-            int an = fc < max_nei ? fc : max_nei;
-            int st = hash_func(i, frame) % fc;
-            float invP = fdiv(1.0f, P);
-            for (int kk = 0; kk < an; ++kk) {
+        float invP = fdiv(1.0f, P);
+        for (int base = 0; base < an; base += GS) {
+            int kk = base + gl;
+            bool hit = false;
+            float term = 0.f;
+            if (kk < an) {
                 int ni = (st + kk) % fc;
                 int j = face_ids[(size_t)i * FOS_S + ni];
-                if (j < 0 || j >= n || j == i) continue;
-                float Vj = powf(rin[j], P);
-                float dvr = fmul(k, fsub(Vi, Vj));
-                float vmin = fminf(Vi, Vj);
-                float dv = fmaxf(fmul(-cap, vmin), fminf(fmul(cap, vmin), dvr));
-                float vn = fsub(Vi, dv);
-                d = fadd(d, fsub(powf(vn, invP), ri));
+                if (!(j < 0 || j >= n || j == i)) {
+                    float Vj = powf(rin[j], P);
+                    float dvr = fmul(k, fsub(Vi, Vj));
+                    float vmin = fminf(Vi, Vj);
+                    float dv = fmaxf(fmul(-cap, vmin), fminf(fmul(cap, vmin), dvr));
+                    term = fsub(powf(fsub(Vi, dv), invP), ri);
+                    hit = true;
+                }
+            }
+            unsigned int m = __ballot_sync(gmask, hit) & gmask;
+            m >>= (GS == 32 ? 0 : (lane & 16));
+            while (m) {
+                int b = __ffs(m) - 1;
+                m &= m - 1;
+                d = fadd(d, __shfl_sync(gmask, term, b, GS));
             }
         }
+    }
+    if (live && gl == 0) {
         delta_r[i] = d;
         rout[i] = fmaxf(rmin, fminf(rmax, fadd(ri, d)));
     }
     float ad = fabsf(d);
-    int ch = (i < n) && ad > 1e-12f;
-    unsigned int m = __ballot_sync(0xffffffffu, ch);
-    unsigned int b = __reduce_max_sync(0xffffffffu, ch ? __float_as_uint(ad) : 0u);
-    if ((threadIdx.x & 31) == 0 && m) {
-        atomicAdd(&pchanged[slot], __popc(m));
-        atomicMax(&pmax[slot], b);
+    int ch = (live && gl == 0) && ad > 1e-12f;
+    unsigned int wm = __ballot_sync(0xffffffffu, ch);
+    unsigned int bm = __reduce_max_sync(0xffffffffu, ch ? __float_as_uint(ad) : 0u);
+    if (lane == 0 && wm) {
+        atomicAdd(&pchanged[slot], __popc(wm));
+        atomicMax(&pmax[slot], bm);
     }
 }
 
@@ -326,22 +402,27 @@ static int check_dyn(FosCtx* c, int n) {
     return FOS_OK;
 }
 
-int fos_launch_pbd(FosCtx* c, const float* pin, float* pout, const float* rad,
-                   const int32_t* cs, const int32_t* cc, const int32_t* ci, int n, cudaStream_t s) {
+int fos_grid_gather_sorted(FosCtx* c, const int32_t* idx, const float* pos, const float* rad,
+                           int n, cudaStream_t s);
+
+// PBD sweep over the cell-ordered copy ctx->sorted (must match cs/cc/ci).
+int fos_launch_pbd(FosCtx* c, float* pout, const int32_t* cs, const int32_t* cc,
+                   const int32_t* ci, int n, cudaStream_t s) {
     if (n == 0) return FOS_OK;
-    k_pbd<<<fos_blocks(n, 128), 128, 0, s>>>(pin, pout, rad, n, c->G, c->L, c->invL, c->halfL, cs,
-                                             cc, ci, c->gap1, c->mdf, c->dmul);
+    k_pbd<<<fos_blocks(32LL * n, 256), 256, 0, s>>>(c->sorted, ci, pout, n, c->G, c->L, c->invL,
+                                                    c->halfL, cs, cc, c->gap1, c->mdf, c->dmul);
     FOS_LAUNCHED(c);
     return FOS_OK;
 }
 
-int fos_launch_max_overlap(FosCtx* c, const float* pos, const float* rad, const int32_t* cs,
-                           const int32_t* cc, const int32_t* ci, float* lmd, int n,
-                           unsigned int* gmax_bits, cudaStream_t s) {
+// Max overlap over the cell-ordered copy ctx->sorted (must match cs/cc/ci).
+int fos_launch_max_overlap(FosCtx* c, const int32_t* cs, const int32_t* cc, const int32_t* ci,
+                           float* lmd, int n, unsigned int* gmax_bits, cudaStream_t s) {
     FOS_CUDA(cudaMemsetAsync(gmax_bits, 0, 4, s));
     if (n == 0) return FOS_OK;
-    k_max_overlap<<<fos_blocks(n, 128), 128, 0, s>>>(pos, rad, n, c->G, c->L, c->invL, c->halfL, cs,
-                                                     cc, ci, c->eps, lmd, gmax_bits);
+    k_max_overlap<<<fos_blocks(32LL * n, 256), 256, 0, s>>>(c->sorted, ci, n, c->G, c->L, c->invL,
+                                                            c->halfL, cs, cc, c->eps, lmd,
+                                                            gmax_bits);
     FOS_LAUNCHED(c);
     return FOS_OK;
 }
@@ -361,9 +442,14 @@ int fos_launch_pressure(FosCtx* c, int n, int frame, const int* frame_ptr, float
     for (int w = 0; w < sweeps; ++w) {
         const float* rin = (w & 1) ? c->rad_tmp : rad;
         float* rout = (w & 1) ? rad : c->rad_tmp;
-        k_pressure<<<fos_blocks(n, 256), 256, 0, s>>>(n, frame, frame_ptr, rin, rout, delta_r,
-                                                      face_ids, fsc, k, P, cap, max_nei, rmin,
-                                                      rmax, sm, sc, w & 1);
+        if (max_nei <= 16)
+            k_pressure<16><<<fos_blocks(16LL * n, 256), 256, 0, s>>>(
+                n, frame, frame_ptr, rin, rout, delta_r, face_ids, fsc, k, P, cap, max_nei, rmin,
+                rmax, sm, sc, w & 1);
+        else
+            k_pressure<32><<<fos_blocks(32LL * n, 256), 256, 0, s>>>(
+                n, frame, frame_ptr, rin, rout, delta_r, face_ids, fsc, k, P, cap, max_nei, rmin,
+                rmax, sm, sc, w & 1);
         FOS_LAUNCHED(c);
     }
     if (sweeps & 1)
@@ -419,7 +505,9 @@ extern "C" int fos_project_overlaps(FosCtx* c, float* pos, const float* rad, con
     if (rc) return rc;
     FOS_REQUIRE(n == 0 || (pos && rad && cs && cc && ci), FOS_E_ARG, "NULL argument");
     if (n == 0) return FOS_OK;
-    rc = fos_launch_pbd(c, pos, c->pos_tmp, rad, cs, cc, ci, n, s);
+    rc = fos_grid_gather_sorted(c, ci, pos, rad, n, s);
+    if (rc) return rc;
+    rc = fos_launch_pbd(c, c->pos_tmp, cs, cc, ci, n, s);
     if (rc) return rc;
     FOS_CUDA(cudaMemcpyAsync(pos, c->pos_tmp, (size_t)n * 12, cudaMemcpyDeviceToDevice, s));
     return FOS_OK;
@@ -433,7 +521,9 @@ extern "C" int fos_compute_max_overlap(FosCtx* c, const float* pos, const float*
     if (rc) return rc;
     FOS_REQUIRE(n == 0 || (pos && rad && cs && cc && ci && lmd), FOS_E_ARG, "NULL argument");
     unsigned int* bits = &c->ds->omax_bits;
-    rc = fos_launch_max_overlap(c, pos, rad, cs, cc, ci, lmd, n, bits, s);
+    rc = fos_grid_gather_sorted(c, ci, pos, rad, n, s);
+    if (rc) return rc;
+    rc = fos_launch_max_overlap(c, cs, cc, ci, lmd, n, bits, s);
     if (rc) return rc;
     if (max_dev) FOS_CUDA(cudaMemcpyAsync(max_dev, bits, 4, cudaMemcpyDeviceToDevice, s));
     if (max_host) {

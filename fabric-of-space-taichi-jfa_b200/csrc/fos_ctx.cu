@@ -175,6 +175,7 @@ extern "C" int fos_ctx_create(const FosParams* p, int max_n, int max_res, int de
     c->scan_tmp_n = 4096;
     ALLOC(c->scan_tmp, c->scan_tmp_n * 4);
     ALLOC(c->pos_tmp, (size_t)max_n * 3 * 4);
+    ALLOC(c->sorted, (size_t)max_n * sizeof(float4));
     ALLOC(c->rad_tmp, (size_t)max_n * 4);
     ALLOC(c->cellof, (size_t)max_n * 4);
     ALLOC(c->rank, (size_t)max_n * 4);
@@ -231,7 +232,7 @@ extern "C" int fos_ctx_destroy(FosCtx* c) {
                     c->hkeys, c->hmin, c->hcnt, c->claimed, c->rowcnt, c->rowbuf, c->revcnt,
                     c->revstart, c->revfill, c->rev, c->scan_tmp, c->pos_tmp, c->rad_tmp,
                     c->cellof, c->rank, c->cell_tmp, c->stats_f, c->stats_i, c->ds,
-                    c->fin_changed};
+                    c->fin_changed, c->sorted};
     for (void* q : ptrs)
         if (q) cudaFree(q);
     if (c->pinned) cudaFreeHost(c->pinned);

@@ -84,6 +84,7 @@ struct FosCtx {
     int32_t* scan_tmp = nullptr;      // block sums for the multi-block scan
     size_t scan_tmp_n = 0;
     float* pos_tmp = nullptr;         // [max_n*3]
+    float4* sorted = nullptr;         // [max_n] (x, y, z, r) in hash-cell order
     float* rad_tmp = nullptr;         // [max_n]
     int32_t *cellof = nullptr, *rank = nullptr;   // [max_n]
     int32_t* cell_tmp = nullptr;      // [G^3]  (scatter's copy of cell_write)
@@ -133,6 +134,7 @@ inline int fos_blocks(long long work, int threads) {
 // total when with_total.  Launch-count aware.
 int fos_scan_exclusive(FosCtx* ctx, const int32_t* d_in, int32_t* d_out, int n, bool with_total,
                        cudaStream_t s);
+int fos_jfa_finalize_ema(FosCtx* c, const float* rad, int n, cudaStream_t s);
 
 // ------------------------------------------------------------ device math
 __device__ __forceinline__ float fadd(float a, float b) { return __fadd_rn(a, b); }
@@ -154,6 +156,21 @@ __device__ __forceinline__ float power_dist(float vx, float vy, float vz, float4
     float dx = jfa_wrap<UNIT_L>(fsub(vx, s.x), L);
     float dy = jfa_wrap<UNIT_L>(fsub(vy, s.y), L);
     float dz = jfa_wrap<UNIT_L>(fsub(vz, s.z), L);
+    float d2 = fadd(fadd(fmul(dx, dx), fmul(dy, dy)), fmul(dz, dz));
+    return fsub(d2, s.w);
+}
+
+// power_distance_sq for L == 1 using rintf (round half to even, one
+// instruction) in place of roundf: the two differ only when d is exactly a
+// half-integer, where d - round(d) is +-0.5 either way, and the distance uses
+// only its square.  So the returned value is bit-identical to power_dist<true>.
+__device__ __forceinline__ float power_dist_unit(float vx, float vy, float vz, float4 s) {
+    float dx = fsub(vx, s.x);
+    float dy = fsub(vy, s.y);
+    float dz = fsub(vz, s.z);
+    dx = fsub(dx, rintf(dx));
+    dy = fsub(dy, rintf(dy));
+    dz = fsub(dz, rintf(dz));
     float d2 = fadd(fadd(fmul(dx, dx), fmul(dy, dy)), fmul(dz, dz));
     return fsub(d2, s.w);
 }

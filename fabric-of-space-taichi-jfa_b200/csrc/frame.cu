@@ -9,12 +9,12 @@
 
 // launchers defined in grid.cu / dynamics.cu
 int fos_grid_build_from(FosCtx* c, const float* src, float* dst, int n, int32_t* cell_count,
-                        int32_t* cell_start, int32_t* cell_indices, cudaStream_t s);
-int fos_launch_pbd(FosCtx* c, const float* pin, float* pout, const float* rad, const int32_t* cs,
-                   const int32_t* cc, const int32_t* ci, int n, cudaStream_t s);
-int fos_launch_max_overlap(FosCtx* c, const float* pos, const float* rad, const int32_t* cs,
-                           const int32_t* cc, const int32_t* ci, float* lmd, int n,
-                           unsigned int* gmax_bits, cudaStream_t s);
+                        int32_t* cell_start, int32_t* cell_indices, const float* rad,
+                        cudaStream_t s);
+int fos_launch_pbd(FosCtx* c, float* pout, const int32_t* cs, const int32_t* cc,
+                   const int32_t* ci, int n, cudaStream_t s);
+int fos_launch_max_overlap(FosCtx* c, const int32_t* cs, const int32_t* cc, const int32_t* ci,
+                           float* lmd, int n, unsigned int* gmax_bits, cudaStream_t s);
 int fos_launch_pressure(FosCtx* c, int n, int frame, const int* frame_ptr, float* rad,
                         float* delta_r, const int32_t* face_ids, const int32_t* fsc, float k,
                         float P, float cap, int max_nei, float rmin, float rmax, int sweeps,
@@ -96,10 +96,9 @@ extern "C" int fos_sim_init(FosCtx* c, const FosState* st, const FosFrameParams*
     if (rc) return rc;
     for (int k = 0; k < fp->warmup_pbd; ++k) {
         rc = fos_grid_build_from(c, st->pos, st->pos, n, st->cell_count, st->cell_start,
-                                 st->cell_indices, s);
+                                 st->cell_indices, st->rad, s);
         if (rc) return rc;
-        rc = fos_launch_pbd(c, st->pos, c->pos_tmp, st->rad, st->cell_start, st->cell_count,
-                            st->cell_indices, n, s);
+        rc = fos_launch_pbd(c, c->pos_tmp, st->cell_start, st->cell_count, st->cell_indices, n, s);
         if (rc) return rc;
         FOS_CUDA(cudaMemcpyAsync(st->pos, c->pos_tmp, (size_t)n * 12, cudaMemcpyDeviceToDevice, s));
     }
@@ -110,54 +109,119 @@ static float alpha_for_frames(int frames) {  // run.py:440-452
     return (float)(1.0 - pow(0.05, 1.0 / (double)(frames > 1 ? frames : 1)));
 }
 
+// Optional per-stage event timing of a frame (fos_frame_profile).
+struct FrameProf {
+    cudaEvent_t ev[64];
+    int stage[64];
+    int k = 0;
+    cudaStream_t s;
+    void mark(int stage_id) {
+        if (k < 64) {
+            cudaEventRecord(ev[k], s);
+            stage[k] = stage_id;
+            ++k;
+        }
+    }
+};
+
+static int frame_impl(FosCtx* c, const FosState* st, const FosFrameParams* fp, int jfa_frame,
+                      cudaStream_t s, FrameProf* prof);
+
 extern "C" int fos_frame(FosCtx* c, const FosState* st, const FosFrameParams* fp, int jfa_frame,
                          fos_stream_t s) {
+    return frame_impl(c, st, fp, jfa_frame, s, nullptr);
+}
+
+extern "C" int fos_frame_profile(FosCtx* c, const FosState* st, const FosFrameParams* fp,
+                                 int jfa_frame, float* stage_ms, fos_stream_t s) {
+    FOS_REQUIRE(stage_ms != nullptr, FOS_E_ARG, "stage_ms is NULL");
+    FrameProf prof;
+    prof.s = s;
+    for (int i = 0; i < 64; ++i) FOS_CUDA(cudaEventCreate(&prof.ev[i]));
+    prof.mark(-1);
+    int rc = frame_impl(c, st, fp, jfa_frame, s, &prof);
+    if (rc == FOS_OK) {
+        FOS_CUDA(cudaStreamSynchronize(s));
+        for (int i = 0; i < FOS_FRAME_STAGES; ++i) stage_ms[i] = 0.f;
+        for (int i = 1; i < prof.k; ++i) {
+            float ms = 0.f;
+            cudaEventElapsedTime(&ms, prof.ev[i - 1], prof.ev[i]);
+            int st_id = prof.stage[i];
+            if (st_id >= 0 && st_id < FOS_FRAME_STAGES) stage_ms[st_id] += ms;
+        }
+    }
+    for (int i = 0; i < 64; ++i) cudaEventDestroy(prof.ev[i]);
+    return rc;
+}
+
+static int frame_impl(FosCtx* c, const FosState* st, const FosFrameParams* fp, int jfa_frame,
+                      cudaStream_t s, FrameProf* prof) {
     int rc = check_state(c, st, fp);
     if (rc) return rc;
     const int n = st->n;
+#define MARK(id) \
+    if (prof) prof->mark(id)
     const int* dframe = &c->ds->frame;
     // (1) rebuild_grid (run.py:704)
     rc = fos_grid_build_from(c, st->pos, st->pos, n, st->cell_count, st->cell_start,
-                             st->cell_indices, s);
+                             st->cell_indices, st->rad, s);
     if (rc) return rc;
+    MARK(0);
     // (2) compute_max_overlap (run.py:709, 737 in the defined argument order)
-    rc = fos_launch_max_overlap(c, st->pos, st->rad, st->cell_start, st->cell_count,
-                                st->cell_indices, st->local_max_depth, n, &c->ds->omax_bits, s);
+    rc = fos_launch_max_overlap(c, st->cell_start, st->cell_count, st->cell_indices,
+                                st->local_max_depth, n, &c->ds->omax_bits, s);
     if (rc) return rc;
+    MARK(1);
     // (3) nudge_radii_adaptive_ema while settle_frames_left > 0 (run.py:744-750)
     rc = fos_launch_nudge(c, st->rad, st->rad_target, st->local_max_depth, n,
                           alpha_for_frames(fp->adjustment_frames), (float)fp->max_step_pct,
                           (float)fp->r_min, (float)fp->r_max, 1.0f, &c->ds->omax_bits, fp->bp_mode,
                           c->ds, s);
     if (rc) return rc;
+    MARK(2);
     // (4) equilibrate_pressure x pressure_iters on the last JFA's face_ids/fsc (run.py:755-771)
     rc = fos_launch_pressure(c, n, 0, dframe, st->rad, st->delta_r, c->face_ids, c->fsc,
                              (float)fp->pressure_k, (float)fp->pressure_exp,
                              (float)fp->pressure_pair_cap, fp->max_eq_nei, (float)fp->r_min,
                              (float)fp->r_max, fp->pressure_iters, s);
     if (rc) return rc;
+    MARK(3);
     // (5) apply_brownian_motion (run.py:807-813); also settle_frames_left -= 1
     rc = fos_launch_brownian(c, st->pos, n, (float)fp->brownian_strength, c->L, fp->seed, 0,
                              dframe, c->ds, s);
     if (rc) return rc;
+    MARK(4);
     // (6) PBD passes, each on a fresh grid (run.py:829-846); (7) final rebuild (run.py:874)
     const float* src = st->pos;
     for (int k = 0; k < fp->pbd_iters; ++k) {
         rc = fos_grid_build_from(c, src, st->pos, n, st->cell_count, st->cell_start,
-                                 st->cell_indices, s);
+                                 st->cell_indices, st->rad, s);
         if (rc) return rc;
-        rc = fos_launch_pbd(c, st->pos, c->pos_tmp, st->rad, st->cell_start, st->cell_count,
-                            st->cell_indices, n, s);
+        MARK(0);
+        rc = fos_launch_pbd(c, c->pos_tmp, st->cell_start, st->cell_count, st->cell_indices, n, s);
         if (rc) return rc;
+        MARK(5);
         src = c->pos_tmp;
     }
     rc = fos_grid_build_from(c, src, st->pos, n, st->cell_count, st->cell_start, st->cell_indices,
-                             s);
+                             nullptr, s);
     if (rc) return rc;
+    MARK(0);
     // (8) measurement frame: run_jfa, warm-start gate, set_fsc_targets, settle reset
     if (jfa_frame) {
-        rc = fos_jfa_run(c, st->pos, st->rad, n, s);
+        rc = fos_jfa_init(c, st->pos, st->rad, n, s);
         if (rc) return rc;
+        rc = fos_jfa_passes(c, n, s);
+        if (rc) return rc;
+        MARK(6);
+        rc = fos_jfa_majority_filter(c, s);
+        if (rc) return rc;
+        rc = fos_jfa_accumulate_faces(c, n, s);
+        if (rc) return rc;
+        MARK(7);
+        rc = fos_jfa_finalize_ema(c, st->rad, n, s);
+        if (rc) return rc;
+        MARK(8);
         rc = fos_launch_set_targets(c, st->rad, st->rad_target, c->fsc, c->ema, n, fp->f_low,
                                     fp->f_high, (float)fp->growth_pct, (float)fp->r_min,
                                     (float)fp->r_max, c->ds, fp->warmstart_frames,
@@ -166,6 +230,8 @@ extern "C" int fos_frame(FosCtx* c, const FosState* st, const FosFrameParams* fp
     }
     k_frame_end<<<1, 1, 0, s>>>(c->ds);
     FOS_LAUNCHED(c);
+    MARK(9);
+#undef MARK
     return FOS_OK;
 }
 

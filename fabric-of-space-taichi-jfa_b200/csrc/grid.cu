@@ -71,10 +71,13 @@ __global__ void k_grid_scatter_atomic(float* pos, int n, int G, float L, float i
 }
 
 // Sorts each cell's slice ascending.  Slice c is [begin[c], begin[c]+count[c])
-// or, with end != NULL, [begin[c], end[c]).
+// or, with end != NULL, [begin[c], end[c]).  With sp != NULL it also writes
+// the cell-ordered copy sp[k] = (pos[idx[k]], rad[idx[k]]) that the
+// neighbour-gather kernels read.
 __global__ void k_grid_sort_cells(int ncells, const int32_t* __restrict__ begin,
                                   const int32_t* __restrict__ count, const int32_t* __restrict__ end,
-                                  int32_t* __restrict__ idx) {
+                                  int32_t* __restrict__ idx, const float* __restrict__ pos,
+                                  const float* __restrict__ rad, float4* __restrict__ sp) {
     int c = blockIdx.x * blockDim.x + threadIdx.x;
     if (c >= ncells) return;
     int b = begin[c];
@@ -88,6 +91,30 @@ __global__ void k_grid_sort_cells(int ncells, const int32_t* __restrict__ begin,
         }
         idx[q + 1] = v;
     }
+    if (sp) {
+        for (int k = b; k < e; ++k) {
+            int j = idx[k];
+            sp[k] = make_float4(pos[3 * j + 0], pos[3 * j + 1], pos[3 * j + 2], rad[j]);
+        }
+    }
+}
+
+// sp[k] = (pos[idx[k]], rad[idx[k]]) for a grid built elsewhere.
+__global__ void k_grid_gather_sorted(int n, const int32_t* __restrict__ idx,
+                                     const float* __restrict__ pos, const float* __restrict__ rad,
+                                     float4* __restrict__ sp) {
+    int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= n) return;
+    int j = idx[k];
+    sp[k] = make_float4(pos[3 * j + 0], pos[3 * j + 1], pos[3 * j + 2], rad[j]);
+}
+
+int fos_grid_gather_sorted(FosCtx* c, const int32_t* idx, const float* pos, const float* rad,
+                           int n, cudaStream_t s) {
+    if (n == 0) return FOS_OK;
+    k_grid_gather_sorted<<<fos_blocks(n, 256), 256, 0, s>>>(n, idx, pos, rad, c->sorted);
+    FOS_LAUNCHED(c);
+    return FOS_OK;
 }
 
 static int check_grid(FosCtx* c, int n) {
@@ -142,15 +169,17 @@ extern "C" int fos_grid_scatter(FosCtx* c, float* pos, int32_t* cell_write, int3
                                                              cell_write, cell_indices);
     FOS_LAUNCHED(c);
     k_grid_sort_cells<<<fos_blocks(G3, 256), 256, 0, s>>>(G3, c->cell_tmp, nullptr, cell_write,
-                                                          cell_indices);
+                                                          cell_indices, nullptr, nullptr, nullptr);
     FOS_LAUNCHED(c);
     return FOS_OK;
 }
 
 // Fused rebuild reading positions from src and writing the wrapped positions
-// to dst (src may equal dst).
+// to dst (src may equal dst).  With rad != NULL the cell-ordered (pos, rad)
+// copy ctx->sorted is refreshed as well.
 int fos_grid_build_from(FosCtx* c, const float* src, float* dst, int n, int32_t* cell_count,
-                        int32_t* cell_start, int32_t* cell_indices, cudaStream_t s) {
+                        int32_t* cell_start, int32_t* cell_indices, const float* rad,
+                        cudaStream_t s) {
     int G3 = c->G * c->G * c->G;
     FOS_CUDA(cudaMemsetAsync(cell_count, 0, (size_t)G3 * 4, s));
     if (n > 0) {
@@ -165,7 +194,8 @@ int fos_grid_build_from(FosCtx* c, const float* src, float* dst, int n, int32_t*
                                                              cell_indices);
     FOS_LAUNCHED(c);
     k_grid_sort_cells<<<fos_blocks(G3, 256), 256, 0, s>>>(G3, cell_start, cell_count, nullptr,
-                                                          cell_indices);
+                                                          cell_indices, dst, rad,
+                                                          rad ? c->sorted : nullptr);
     FOS_LAUNCHED(c);
     return FOS_OK;
 }
@@ -176,5 +206,5 @@ extern "C" int fos_grid_build(FosCtx* c, float* pos, int n, int32_t* cell_count,
     if (rc) return rc;
     FOS_REQUIRE(cell_count && cell_start && cell_indices && (n == 0 || pos), FOS_E_ARG,
                 "NULL argument");
-    return fos_grid_build_from(c, pos, pos, n, cell_count, cell_start, cell_indices, s);
+    return fos_grid_build_from(c, pos, pos, n, cell_count, cell_start, cell_indices, nullptr, s);
 }

@@ -76,10 +76,21 @@ __device__ __forceinline__ bool jfa_exited_before(const FosDevState* ds, int p, 
 // One pass: own label first (1e10 when unassigned), then the 27 offsets in
 // lexicographic (dx, dy, dz) order, dz fastest, each times `step` and wrapped;
 // a candidate replaces the best only on a strictly smaller power distance.
-// Candidates equal to the current best or to the previously evaluated label
-// are skipped: their distance is already known not to win, so the result is
-// unchanged.  One thread per voxel, z fastest, so each of the 27 offset loads
-// of a warp is one coalesced 128-byte row.
+// A candidate whose label equals the voxel's own label or the label of the
+// previous offset in scan order is skipped: that label's distance has already
+// been compared, so it cannot win again and the result is unchanged.
+//
+// One thread per voxel, z fastest, so each of the 27 label loads of a warp is
+// one coalesced 128-byte row.  All 27 labels are loaded up front; the seed
+// gathers are then issued nine at a time (one dx plane) independently of the
+// running minimum, so a voxel waits for three rounds of gather latency rather
+// than one per evaluated candidate.  A plane no lane of the warp needs is
+// skipped with one vote.
+template <bool UNIT_L, bool POW2, bool TIE_LOWER>
+__device__ __forceinline__ float jfa_dist(float vx, float vy, float vz, float4 s, float L) {
+    return UNIT_L ? power_dist_unit(vx, vy, vz, s) : power_dist<false>(vx, vy, vz, s, L);
+}
+
 template <bool UNIT_L, bool POW2, bool TIE_LOWER>
 __global__ void __launch_bounds__(256) k_jfa_pass(const int32_t* __restrict__ in,
                                                   int32_t* __restrict__ out,
@@ -91,57 +102,73 @@ __global__ void __launch_bounds__(256) k_jfa_pass(const int32_t* __restrict__ in
     if (early_exit && jfa_exited_before(ds, pass, (double)V, min_passes, th)) return;
     long long lin = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     bool live = lin < V;
+    long long l = live ? lin : 0;
+    int x, y, z;
+    if (POW2) {
+        z = (int)(l & (R - 1));
+        y = (int)((l >> lgR) & (R - 1));
+        x = (int)(l >> (2 * lgR));
+    } else {
+        z = (int)(l % R);
+        y = (int)((l / R) % R);
+        x = (int)(l / ((long long)R * R));
+    }
+    int xs[3], ys[3], zs[3];
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+        int o = (k - 1) * step;
+        if (POW2) {
+            xs[k] = ((x + o) & (R - 1)) << (2 * lgR);
+            ys[k] = ((y + o) & (R - 1)) << lgR;
+            zs[k] = (z + o) & (R - 1);
+        } else {
+            xs[k] = wrap_small(x + o, R) * R * R;
+            ys[k] = wrap_small(y + o, R) * R;
+            zs[k] = wrap_small(z + o, R);
+        }
+    }
+    int ids[27];
+#pragma unroll
+    for (int a = 0; a < 3; ++a)
+#pragma unroll
+        for (int b = 0; b < 3; ++b)
+#pragma unroll
+            for (int c = 0; c < 3; ++c) ids[a * 9 + b * 3 + c] = in[xs[a] + ys[b] + zs[c]];
+    int own = live ? ids[13] : -1;  // offset (0,0,0) is the voxel itself
+    float vx = voxel_centre(x, vs, halfL), vy = voxel_centre(y, vs, halfL),
+          vz = voxel_centre(z, vs, halfL);
+    int best = own;
+    float bd = 1e10f;
+    if (own >= 0) bd = jfa_dist<UNIT_L, POW2, TIE_LOWER>(vx, vy, vz, __ldg(&seeds[own]), L);
+#pragma unroll
+    for (int g = 0; g < 3; ++g) {
+        bool ok[9];
+        bool any = false;
+#pragma unroll
+        for (int k = 0; k < 9; ++k) {
+            int idx = g * 9 + k;
+            int id = ids[idx];
+            int prv = idx == 0 ? own : ids[idx - 1];
+            ok[k] = live && id >= 0 && id != own && id != prv;
+            any |= ok[k];
+        }
+        if (!__any_sync(0xffffffffu, any)) continue;
+        float4 sv[9];
+#pragma unroll
+        for (int k = 0; k < 9; ++k)
+            sv[k] = ok[k] ? __ldg(&seeds[ids[g * 9 + k]]) : make_float4(0.f, 0.f, 0.f, 0.f);
+#pragma unroll
+        for (int k = 0; k < 9; ++k) {
+            int id = ids[g * 9 + k];
+            float d = jfa_dist<UNIT_L, POW2, TIE_LOWER>(vx, vy, vz, sv[k], L);
+            if (ok[k] && (d < bd || (TIE_LOWER && d == bd && id < best))) {
+                bd = d;
+                best = id;
+            }
+        }
+    }
     int changed = 0;
     if (live) {
-        int x, y, z;
-        if (POW2) {
-            z = (int)(lin & (R - 1));
-            y = (int)((lin >> lgR) & (R - 1));
-            x = (int)(lin >> (2 * lgR));
-        } else {
-            z = (int)(lin % R);
-            y = (int)((lin / R) % R);
-            x = (int)(lin / ((long long)R * R));
-        }
-        float vx = voxel_centre(x, vs, halfL), vy = voxel_centre(y, vs, halfL),
-              vz = voxel_centre(z, vs, halfL);
-        int own = in[lin];
-        int best = own, last = own;
-        float bd = 1e10f;
-        if (own >= 0) bd = power_dist<UNIT_L>(vx, vy, vz, __ldg(&seeds[own]), L);
-        int xs[3], ys[3], zs[3];
-#pragma unroll
-        for (int k = 0; k < 3; ++k) {
-            int o = (k - 1) * step;
-            if (POW2) {
-                xs[k] = ((x + o) & (R - 1)) << (2 * lgR);
-                ys[k] = ((y + o) & (R - 1)) << lgR;
-                zs[k] = (z + o) & (R - 1);
-            } else {
-                xs[k] = wrap_small(x + o, R) * R * R;
-                ys[k] = wrap_small(y + o, R) * R;
-                zs[k] = wrap_small(z + o, R);
-            }
-        }
-        int ids[27];
-#pragma unroll
-        for (int a = 0; a < 3; ++a)
-#pragma unroll
-            for (int b = 0; b < 3; ++b)
-#pragma unroll
-                for (int c = 0; c < 3; ++c) ids[a * 9 + b * 3 + c] = in[xs[a] + ys[b] + zs[c]];
-#pragma unroll
-        for (int k = 0; k < 27; ++k) {
-            int id = ids[k];
-            if (id >= 0 && id != best && id != last) {
-                last = id;
-                float d = power_dist<UNIT_L>(vx, vy, vz, __ldg(&seeds[id]), L);
-                if (d < bd || (TIE_LOWER && d == bd && id < best)) {
-                    bd = d;
-                    best = id;
-                }
-            }
-        }
         out[lin] = best;
         changed = best != own;
     }
@@ -742,6 +769,13 @@ extern "C" int fos_jfa_update_ema(FosCtx* c, int n, fos_stream_t s) {
     k_ema<<<fos_blocks(n, 256), 256, 0, s>>>(n, c->fsc, c->ema, c->ema_alpha);
     FOS_LAUNCHED(c);
     return FOS_OK;
+}
+
+// finalize_faces_kernel + update_fsc_ema, the EMA fused into the
+// materialisation of each particle's new fsc (what run_jfa does).
+int fos_jfa_finalize_ema(FosCtx* c, const float* rad, int n, cudaStream_t s) {
+    if (n == 0) return FOS_OK;
+    return finalize_impl(c, rad, n, true, s);
 }
 
 extern "C" int fos_jfa_run(FosCtx* c, const float* pos, const float* rad, int n, fos_stream_t s) {

@@ -62,6 +62,18 @@ class FoamSim:
         self.frame += 1
         return bool(jfa)
 
+    STAGES = ("grid", "max_overlap", "nudge", "pressure", "brownian", "pbd", "jfa_passes",
+              "filter_faces", "finalize_ema", "targets_end")
+
+    def step_profiled(self) -> dict:
+        """One frame (no graph) with CUDA events between stages -> ms per stage."""
+        jfa = 1 if self.cfg.is_jfa_frame(self.frame) else 0
+        ms = (C.c_float * len(self.STAGES))()
+        call("fos_frame_profile", self.ctx.h, C.byref(self.state), C.byref(self.fp), jfa, ms,
+             stream())
+        self.frame += 1
+        return {k: float(v) for k, v in zip(self.STAGES, ms)} | {"jfa": bool(jfa)}
+
     def run(self, frames: int):
         for _ in range(frames):
             self.step()

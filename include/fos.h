@@ -245,6 +245,14 @@ int fos_frame(FosCtx* ctx, const FosState* st, const FosFrameParams* fp, int jfa
  * (state, params, jfa_frame); recaptured when any of them changes. */
 int fos_frame_graph(FosCtx* ctx, const FosState* st, const FosFrameParams* fp, int jfa_frame,
                     fos_stream_t s);
+/* fos_frame with a CUDA event after every stage (no graph; synchronises).
+ * stage_ms[FOS_FRAME_STAGES] receives milliseconds per stage: 0 hash-grid
+ * builds, 1 max overlap, 2 settle nudge, 3 pressure sweeps, 4 Brownian, 5 PBD
+ * sweeps, 6 JFA init + passes, 7 majority filter + faces, 8 finalize + EMA,
+ * 9 targets + frame end. */
+#define FOS_FRAME_STAGES 10
+int fos_frame_profile(FosCtx* ctx, const FosState* st, const FosFrameParams* fp, int jfa_frame,
+                      float* stage_ms, fos_stream_t s);
 /* Device frame index and settle counter (synchronises). */
 int fos_sim_counters(FosCtx* ctx, int* frame, int* settle, fos_stream_t s);
 

@@ -84,7 +84,7 @@ def test_pressure_sweeps(sweeps):
                                         p.pair_cap, p.max_nei, p.r_min, p.r_max, sweeps=sweeps)
     g = drad.cpu().numpy()
     assert np.max(np.abs(g - r_o) / r_o) <= RTOL
-    assert abs(gmx - mx) <= 1e-6 * max(abs(mx), 1e-12) + 1e-9
+    assert abs(gmx - mx) <= RTOL * abs(mx) + 1e-12
     assert abs(gch - ch) <= max(2, ch // 1000)
     vol_g, vol_o = g.astype(np.float64) ** 3, r_o.astype(np.float64) ** 3
     assert np.max(np.abs(vol_g - vol_o) / vol_o) <= 3 * RTOL

@@ -117,7 +117,10 @@ def test_early_exit_and_tie_rule_flags():
         cfg, ctx = _ctx(foam, JFA_EARLY_EXIT_ENABLED=early, TIE_LOWER_INDEX=tie)
         ctx.jfa_run(_dev(pos), _dev(rad), foam.n)
         st = ctx.jfa_stats(foam.n, _dev(rad))
-        assert st["num_passes"] == done and st["early_exit"] == (done < p.passes)
+        V = float(p.R ** 3)
+        fired = any(q >= p.min_passes - 1 and ch[q] / V < p.th_delta for q in range(done))
+        # run_jfa sets early_exit when the exit test fires, even on the last pass
+        assert st["num_passes"] == done and st["early_exit"] == (early and fired)
         assert np.array_equal(ctx.labels().cpu().numpy().reshape(-1), lab)
 
 
@@ -211,3 +214,21 @@ def test_capacity_errors_are_loud():
         ctx.set_resolution(64)
     with pytest.raises(TypeError):
         ctx.jfa_run(pos.double(), rad, 2)
+
+
+@pytest.mark.parametrize("shift", [0.0, 0.5, 1.75])
+def test_unwrapped_seed_positions(shift):
+    """Seeds given outside [-L/2, L/2) (unwrapped or shifted by whole boxes) use
+    the same jfa.wrapP arithmetic: labels match the oracle bit for bit."""
+    rng = np.random.default_rng(21)
+    n, R = 400, 32
+    pos = (rng.random((n, 3), dtype=np.float32) - np.float32(0.5) + np.float32(shift))
+    rad = rng.uniform(0.02, 0.05, n).astype(np.float32)
+    p = O.OracleParams(n=n, R=R)
+    lab, _, _ = O.jfa_labels(pos, rad, p)
+    cfg = FosConfig(DOMAIN_SIZE=1.0, CELL_SIZE=0.1, JFA_RES=R, JFA_RES_MIN=2, JFA_RES_MAX=R,
+                    JFA_EARLY_EXIT_ENABLED=False, MAX_PARTICLES=n)
+    ctx = Context(cfg, max_n=n, max_res=R)
+    ctx.jfa_run(_dev(pos), _dev(rad), n)
+    torch.cuda.synchronize()
+    assert np.array_equal(ctx.labels().cpu().numpy().reshape(-1), lab)
