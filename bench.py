@@ -399,6 +399,8 @@ def run_profile(args):
         sim.initialize()
         for _ in range(min(foam.jfa_warm, 25)):
             sim.step()
+        for _ in range(foam.jfa_cadence if foam.jfa_cadence > 1 else 2):  # capture both graphs
+            sim.step()
         ms = {"jfa_frame": 0.0, "plain_frame": 0.0}
         cnt = {"jfa_frame": 0, "plain_frame": 0}
         for r in range(args.reps * 5):
@@ -423,6 +425,9 @@ def run_profile(args):
                 stages[k][st] = stages[k].get(st, 0.0) + v
         out["stages_ms"] = {k: {st: round(v / max(1, nst[k]), 4) for st, v in d.items()}
                             for k, d in stages.items()}
+        tr = sim.trace_dynamics()
+        out["coop_phase_us"] = [round(x / 1000.0, 2) for x in tr]
+        out["coop_total_us"] = round(sum(tr) / 1000.0, 2)
     print(json.dumps(out), flush=True)
     return 0
 

@@ -89,9 +89,13 @@ static void fold_params(FosCtx* c) {
 static int alloc_cells(FosCtx* c) {
     size_t need = (size_t)c->G * c->G * c->G;
     if (need <= c->cell_tmp_n) return FOS_OK;
-    if (c->cell_tmp) cudaFree(c->cell_tmp);
-    c->cell_tmp = nullptr;
-    FOS_CUDA(cudaMalloc(&c->cell_tmp, need * sizeof(int32_t)));
+    int32_t** bufs[3] = {&c->cell_tmp, &c->coop_cnt, &c->coop_part};
+    for (int32_t** b : bufs) {
+        if (*b) cudaFree(*b);
+        *b = nullptr;
+    }
+    for (int32_t** b : bufs) FOS_CUDA(cudaMalloc((void**)b, need * sizeof(int32_t)));
+    FOS_CUDA(cudaMemset(c->coop_cnt, 0, need * sizeof(int32_t)));
     c->cell_tmp_n = need;
     return FOS_OK;
 }
@@ -176,6 +180,8 @@ extern "C" int fos_ctx_create(const FosParams* p, int max_n, int max_res, int de
     ALLOC(c->scan_tmp, c->scan_tmp_n * 4);
     ALLOC(c->pos_tmp, (size_t)max_n * 3 * 4);
     ALLOC(c->sorted, (size_t)max_n * sizeof(float4));
+    ALLOC(c->ci_tmp, (size_t)max_n * 4);
+    ALLOC(c->coop_bsum, 1024 * 4);
     ALLOC(c->rad_tmp, (size_t)max_n * 4);
     ALLOC(c->cellof, (size_t)max_n * 4);
     ALLOC(c->rank, (size_t)max_n * 4);
@@ -209,6 +215,7 @@ extern "C" int fos_ctx_create(const FosParams* p, int max_n, int max_res, int de
         return fos_cuda_fail(e, "context init", __FILE__, __LINE__);
     }
     rc = alloc_cells(c);
+    if (rc == FOS_OK) rc = fos_grid_init_attributes();
     if (rc) {
         fos_ctx_destroy(c);
         return rc;
@@ -232,7 +239,8 @@ extern "C" int fos_ctx_destroy(FosCtx* c) {
                     c->hkeys, c->hmin, c->hcnt, c->claimed, c->rowcnt, c->rowbuf, c->revcnt,
                     c->revstart, c->revfill, c->rev, c->scan_tmp, c->pos_tmp, c->rad_tmp,
                     c->cellof, c->rank, c->cell_tmp, c->stats_f, c->stats_i, c->ds,
-                    c->fin_changed, c->sorted};
+                    c->fin_changed, c->sorted, c->ci_tmp, c->coop_bsum, c->coop_cnt,
+                    c->coop_part};
     for (void* q : ptrs)
         if (q) cudaFree(q);
     if (c->pinned) cudaFreeHost(c->pinned);

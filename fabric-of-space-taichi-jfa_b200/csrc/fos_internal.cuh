@@ -17,7 +17,7 @@
 #define FOS_S 32          // MAX_NEIGHBORS (jfa.py:74)
 #define FOS_ROWCAP 64     // candidate partners kept per particle before the 32-slot cut
 #define FOS_FIN_MAXIT 4096
-#define FOS_BAR_SPIN_LIMIT (1u << 26)
+#define FOS_BAR_CYCLE_LIMIT 2000000000LL  // ~1 s at the B200's 1.965 GHz SM clock
 
 // ----------------------------------------------------------- device state
 // Small per-context block in device memory: the frame counters the frame
@@ -88,6 +88,11 @@ struct FosCtx {
     float* rad_tmp = nullptr;         // [max_n]
     int32_t *cellof = nullptr, *rank = nullptr;   // [max_n]
     int32_t* cell_tmp = nullptr;      // [G^3]  (scatter's copy of cell_write)
+    int32_t *coop_cnt = nullptr, *coop_part = nullptr;  // [G^3] cooperative rebuild scratch
+    int32_t* coop_bsum = nullptr;     // [1024]
+    int32_t* ci_tmp = nullptr;        // [max_n]
+    int use_coop = 1;                 // plain-frame dynamics as one cooperative kernel
+    int coop_blocks = -1;             // resident blocks of the cooperative kernel (-1: not queried)
     size_t cell_tmp_n = 0;
     float* stats_f = nullptr;         // device stats scratch
     int32_t* stats_i = nullptr;
@@ -135,6 +140,11 @@ inline int fos_blocks(long long work, int threads) {
 int fos_scan_exclusive(FosCtx* ctx, const int32_t* d_in, int32_t* d_out, int n, bool with_total,
                        cudaStream_t s);
 int fos_jfa_finalize_ema(FosCtx* c, const float* rad, int n, cudaStream_t s);
+int fos_grid_init_attributes();
+bool fos_coop_supported(FosCtx* c);
+int fos_frame_coop_dynamics(FosCtx* c, const FosState* st, const FosFrameParams* fp,
+                            cudaStream_t s, unsigned long long* trace = nullptr,
+                            int trace_cap = 0);
 
 // ------------------------------------------------------------ device math
 __device__ __forceinline__ float fadd(float a, float b) { return __fadd_rn(a, b); }
@@ -220,35 +230,44 @@ __device__ __forceinline__ uint4 philox4x32_10(uint4 c, uint32_t k0, uint32_t k1
 }
 
 // Software grid barrier for kernels launched cooperatively (all blocks
-// co-resident).  Bounded: gives up after FOS_BAR_SPIN_LIMIT polls, records
-// FOS_E_TIMEOUT in ds->error and returns false.
-__device__ __forceinline__ bool grid_barrier(FosDevState* ds) {
-    __syncthreads();
-    bool ok = true;
-    if (threadIdx.x == 0) {
-        volatile unsigned int* genp = &ds->bar_gen;
-        unsigned int gen = *genp;
-        __threadfence();
-        unsigned int arrived = atomicAdd(&ds->bar_count, 1u) + 1u;
-        if (arrived == gridDim.x) {
-            ds->bar_count = 0;
-            __threadfence();
-            atomicAdd(&ds->bar_gen, 1u);
-        } else {
-            unsigned int spins = 0;
-            while (*genp == gen) {
-                if (++spins > FOS_BAR_SPIN_LIMIT) {
-                    atomicCAS(&ds->error, 0, (int)FOS_E_TIMEOUT);
-                    ok = false;
-                    break;
-                }
-                __nanosleep(32);
-            }
-        }
-        __threadfence();
-    }
+// co-resident).  ds->bar_count is reset to 0 before the launch and only grows:
+// the e-th barrier of the launch is complete when bar_count reaches
+// e*gridDim.x.  Thread 0 of each block arrives with a release reduction and
+// polls with acquire loads, then releases its block; `epoch` is the caller's
+// count of barriers passed (a register of thread 0, starting at 0).
+// Bounded: a block that has waited ~1 s (clock64), or that sees the error word
+// set, records FOS_E_TIMEOUT and returns false, so a stuck barrier ends the
+// kernel instead of hanging the GPU.
+__device__ __forceinline__ unsigned int ld_acquire_gpu(const unsigned int* p) {
+    unsigned int v;
+    asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+    return v;
+}
+
+__device__ __forceinline__ void red_release_gpu_add(unsigned int* p, unsigned int v) {
+    asm volatile("red.release.gpu.global.add.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
+}
+
+__device__ __forceinline__ bool grid_barrier(FosDevState* ds, unsigned int& epoch) {
     __shared__ int s_ok;
-    if (threadIdx.x == 0) s_ok = ok ? 1 : 0;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        epoch += 1u;
+        unsigned int target = epoch * gridDim.x;
+        bool ok = true;
+        red_release_gpu_add(&ds->bar_count, 1u);
+        long long t0 = clock64();
+        unsigned int polls = 0;
+        while (ld_acquire_gpu(&ds->bar_count) < target) {
+            if (*((volatile int*)&ds->error) != 0 || clock64() - t0 > FOS_BAR_CYCLE_LIMIT) {
+                atomicCAS(&ds->error, 0, (int)FOS_E_TIMEOUT);
+                ok = false;
+                break;
+            }
+            if (++polls > 2048) __nanosleep(32);
+        }
+        s_ok = ok ? 1 : 0;
+    }
     __syncthreads();
     return s_ok != 0;
 }

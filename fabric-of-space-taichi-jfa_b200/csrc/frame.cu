@@ -162,51 +162,57 @@ static int frame_impl(FosCtx* c, const FosState* st, const FosFrameParams* fp, i
 #define MARK(id) \
     if (prof) prof->mark(id)
     const int* dframe = &c->ds->frame;
-    // (1) rebuild_grid (run.py:704)
-    rc = fos_grid_build_from(c, st->pos, st->pos, n, st->cell_count, st->cell_start,
-                             st->cell_indices, st->rad, s);
-    if (rc) return rc;
-    MARK(0);
-    // (2) compute_max_overlap (run.py:709, 737 in the defined argument order)
-    rc = fos_launch_max_overlap(c, st->cell_start, st->cell_count, st->cell_indices,
-                                st->local_max_depth, n, &c->ds->omax_bits, s);
-    if (rc) return rc;
-    MARK(1);
-    // (3) nudge_radii_adaptive_ema while settle_frames_left > 0 (run.py:744-750)
-    rc = fos_launch_nudge(c, st->rad, st->rad_target, st->local_max_depth, n,
-                          alpha_for_frames(fp->adjustment_frames), (float)fp->max_step_pct,
-                          (float)fp->r_min, (float)fp->r_max, 1.0f, &c->ds->omax_bits, fp->bp_mode,
-                          c->ds, s);
-    if (rc) return rc;
-    MARK(2);
-    // (4) equilibrate_pressure x pressure_iters on the last JFA's face_ids/fsc (run.py:755-771)
-    rc = fos_launch_pressure(c, n, 0, dframe, st->rad, st->delta_r, c->face_ids, c->fsc,
-                             (float)fp->pressure_k, (float)fp->pressure_exp,
-                             (float)fp->pressure_pair_cap, fp->max_eq_nei, (float)fp->r_min,
-                             (float)fp->r_max, fp->pressure_iters, s);
-    if (rc) return rc;
-    MARK(3);
-    // (5) apply_brownian_motion (run.py:807-813); also settle_frames_left -= 1
-    rc = fos_launch_brownian(c, st->pos, n, (float)fp->brownian_strength, c->L, fp->seed, 0,
-                             dframe, c->ds, s);
-    if (rc) return rc;
-    MARK(4);
-    // (6) PBD passes, each on a fresh grid (run.py:829-846); (7) final rebuild (run.py:874)
-    const float* src = st->pos;
-    for (int k = 0; k < fp->pbd_iters; ++k) {
-        rc = fos_grid_build_from(c, src, st->pos, n, st->cell_count, st->cell_start,
+    if (c->use_coop && !prof && fp->max_eq_nei <= 16 && fos_coop_supported(c)) {
+        // (1)-(7) as one persistent cooperative kernel (frame_coop.cu)
+        rc = fos_frame_coop_dynamics(c, st, fp, s);
+        if (rc) return rc;
+    } else {
+        // (1) rebuild_grid (run.py:704)
+        rc = fos_grid_build_from(c, st->pos, st->pos, n, st->cell_count, st->cell_start,
                                  st->cell_indices, st->rad, s);
         if (rc) return rc;
         MARK(0);
-        rc = fos_launch_pbd(c, c->pos_tmp, st->cell_start, st->cell_count, st->cell_indices, n, s);
+        // (2) compute_max_overlap (run.py:709, 737 in the defined argument order)
+        rc = fos_launch_max_overlap(c, st->cell_start, st->cell_count, st->cell_indices,
+                                    st->local_max_depth, n, &c->ds->omax_bits, s);
         if (rc) return rc;
-        MARK(5);
-        src = c->pos_tmp;
-    }
-    rc = fos_grid_build_from(c, src, st->pos, n, st->cell_count, st->cell_start, st->cell_indices,
-                             nullptr, s);
-    if (rc) return rc;
-    MARK(0);
+        MARK(1);
+        // (3) nudge_radii_adaptive_ema while settle_frames_left > 0 (run.py:744-750)
+        rc = fos_launch_nudge(c, st->rad, st->rad_target, st->local_max_depth, n,
+                              alpha_for_frames(fp->adjustment_frames), (float)fp->max_step_pct,
+                              (float)fp->r_min, (float)fp->r_max, 1.0f, &c->ds->omax_bits, fp->bp_mode,
+                              c->ds, s);
+        if (rc) return rc;
+        MARK(2);
+        // (4) equilibrate_pressure x pressure_iters on the last JFA's face_ids/fsc (run.py:755-771)
+        rc = fos_launch_pressure(c, n, 0, dframe, st->rad, st->delta_r, c->face_ids, c->fsc,
+                                 (float)fp->pressure_k, (float)fp->pressure_exp,
+                                 (float)fp->pressure_pair_cap, fp->max_eq_nei, (float)fp->r_min,
+                                 (float)fp->r_max, fp->pressure_iters, s);
+        if (rc) return rc;
+        MARK(3);
+        // (5) apply_brownian_motion (run.py:807-813); also settle_frames_left -= 1
+        rc = fos_launch_brownian(c, st->pos, n, (float)fp->brownian_strength, c->L, fp->seed, 0,
+                                 dframe, c->ds, s);
+        if (rc) return rc;
+        MARK(4);
+        // (6) PBD passes, each on a fresh grid (run.py:829-846); (7) final rebuild (run.py:874)
+        const float* src = st->pos;
+        for (int k = 0; k < fp->pbd_iters; ++k) {
+            rc = fos_grid_build_from(c, src, st->pos, n, st->cell_count, st->cell_start,
+                                     st->cell_indices, st->rad, s);
+            if (rc) return rc;
+            MARK(0);
+            rc = fos_launch_pbd(c, c->pos_tmp, st->cell_start, st->cell_count, st->cell_indices, n, s);
+            if (rc) return rc;
+            MARK(5);
+            src = c->pos_tmp;
+        }
+        rc = fos_grid_build_from(c, src, st->pos, n, st->cell_count, st->cell_start, st->cell_indices,
+                                 nullptr, s);
+        if (rc) return rc;
+        MARK(0);
+}
     // (8) measurement frame: run_jfa, warm-start gate, set_fsc_targets, settle reset
     if (jfa_frame) {
         rc = fos_jfa_init(c, st->pos, st->rad, n, s);

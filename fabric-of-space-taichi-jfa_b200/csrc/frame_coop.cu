@@ -1,0 +1,445 @@
+// frame_coop.cu -- the dynamics part of one frame as ONE persistent
+// cooperative kernel.
+//
+// A plain frame of the reference (run.py:699-874) is a chain of ~70 dependent
+// stages: 10 hash-grid rebuilds, the max-overlap reduction, the settle nudge,
+// M pressure sweeps, Brownian jitter and K PBD sweeps.  At 10k particles
+// each stage is a few microseconds of work, so separate launches are bound by
+// launch latency.  Here every stage is a phase of a single launch whose
+// blocks are all co-resident (cooperative launch), separated by bounded grid
+// barriers; each phase calls the same per-element device functions as the
+// standalone kernels (phases.cuh), so the results are identical.
+//
+// Grid rebuild inside the kernel (grid.py:145-309 / run.py:476-504), four
+// phases: histogram with per-particle arrival rank; per-block scan of its
+// chunk of cells; global offsets + rank scatter into a scratch list; stable
+// placement (each particle's slot = cell start + number of lower-indexed
+// particles in its cell) and the cell-ordered (pos, rad) copy.
+#include <string.h>
+
+#include "phases.cuh"
+
+#define COOP_THREADS 1024
+#define COOP_SMALL_G3 12288  // cell tables up to this size are scanned per block in smem
+
+struct CoopArgs {
+    int n, G3, chunk, pbd_iters, sweeps, bp_mode, small_grid;
+    GridGeom g;
+    float* pos;
+    float* pos_tmp;
+    float* rad;
+    float* rad_tmp;
+    const float* rad_target;
+    float* lmd;
+    float* delta_r;
+    int32_t* cc;
+    int32_t* cs;
+    int32_t* ci;
+    int32_t* cellof;
+    int32_t* rank;
+    int32_t* ci_tmp;
+    int32_t* cnt;
+    int32_t* part;
+    int32_t* bsum;
+    float4* sp;
+    FosDevState* ds;
+    float gap1, mdf, dmul, eps, contact_tol;
+    double contact_tol_d;
+    float alpha, max_step, rmin, rmax;
+    PressureArgs pa;
+    float strength, domain, halfL;
+    uint32_t k0, k1;
+    unsigned long long* trace;  // optional: %globaltimer after every phase (block 0)
+    int trace_cap;
+};
+
+__device__ __forceinline__ unsigned long long global_ns() {
+    unsigned long long t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return t;
+}
+
+// Records a timestamp in trace[k++] from block 0, thread 0 (tracing only).
+__device__ __forceinline__ void trace_mark(const CoopArgs& a, int& k) {
+    if (a.trace && blockIdx.x == 0 && threadIdx.x == 0 && k < a.trace_cap) a.trace[k] = global_ns();
+    ++k;
+}
+
+// Block-wide exclusive scan (one value per thread, blockDim <= 1024).
+__device__ __forceinline__ int coop_block_scan(int v, int* total) {
+    __shared__ int s_w[32];
+    int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    int x = v;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        int y = __shfl_up_sync(0xffffffffu, x, o);
+        if (lane >= o) x += y;
+    }
+    if (lane == 31) s_w[w] = x;
+    __syncthreads();
+    if (w == 0) {
+        int nw = blockDim.x >> 5;
+        int t = lane < nw ? s_w[lane] : 0;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            int y = __shfl_up_sync(0xffffffffu, t, o);
+            if (lane >= o) t += y;
+        }
+        if (lane < nw) s_w[lane] = t;
+    }
+    __syncthreads();
+    int base = w > 0 ? s_w[w - 1] : 0;
+    *total = s_w[(blockDim.x >> 5) - 1];
+    __syncthreads();
+    return base + x - v;
+}
+
+// Rebuild of the hash grid from src into dst (wrapped), with the cell-ordered
+// copy sp[k] = (pos, rad) when rad != NULL.  Ends with a grid barrier unless
+// last.  Returns false if a barrier timed out.
+//
+// Small cell tables (G3 <= COOP_SMALL_G3): three phases -- histogram + ranks;
+// every block scans the whole table into its shared memory (block 0 also
+// writes cell_count/cell_start) and scatters ranks; stable placement from the
+// block's own copy of the starts.  Large tables: the chunked four-phase form.
+__device__ bool coop_grid(const CoopArgs& a, const float* src, float* dst, const float* rad,
+                          bool last, int& tk, unsigned int& ep) {
+    extern __shared__ int s_tab[];  // small form: G3 + 1 exclusive starts
+    const int T = gridDim.x * blockDim.x;
+    const int tid = blockIdx.x * blockDim.x + threadIdx.x;
+    // P1: histogram + arrival rank (cnt is all-zero on entry)
+    for (int i = tid; i < a.n; i += T) {
+        float wx = grid_wrap(__ldcg(&src[3 * i + 0]), a.g.L, a.g.invL);
+        float wy = grid_wrap(__ldcg(&src[3 * i + 1]), a.g.L, a.g.invL);
+        float wz = grid_wrap(__ldcg(&src[3 * i + 2]), a.g.L, a.g.invL);
+        dst[3 * i + 0] = wx;
+        dst[3 * i + 1] = wy;
+        dst[3 * i + 2] = wz;
+        int c = cell_of_wrapped(wx, wy, wz, a.g.invL, a.g.halfL, a.g.G);
+        a.cellof[i] = c;
+        a.rank[i] = atomicAdd(&a.cnt[c], 1);
+    }
+    if (!grid_barrier(a.ds, ep)) return false;
+    trace_mark(a, tk);
+    if (a.small_grid) {
+        // P2: whole-table scan per block, then the rank scatter
+        const int per = (a.G3 + blockDim.x - 1) / blockDim.x;
+        const int b0 = threadIdx.x * per, b1 = min(a.G3, b0 + per);
+        int sum = 0;
+        for (int c = b0; c < b1; ++c) {
+            int v = __ldcg(&a.cnt[c]);
+            s_tab[c] = v;
+            sum += v;
+        }
+        int tot;
+        int run = coop_block_scan(sum, &tot);
+        for (int c = b0; c < b1; ++c) {
+            int v = s_tab[c];
+            s_tab[c] = run;
+            if (blockIdx.x == 0) {
+                a.cc[c] = v;
+                a.cs[c] = run;
+            }
+            run += v;
+        }
+        if (threadIdx.x == 0) s_tab[a.G3] = tot;
+        __syncthreads();
+        for (int i = tid; i < a.n; i += T)
+            a.ci_tmp[s_tab[__ldcg(&a.cellof[i])] + __ldcg(&a.rank[i])] = i;
+        if (!grid_barrier(a.ds, ep)) return false;
+        trace_mark(a, tk);
+        // P3: stable placement from the block's copy of the starts
+        int c0 = blockIdx.x * a.chunk;
+        for (int c = c0 + threadIdx.x; c < c0 + a.chunk && c < a.G3; c += blockDim.x)
+            a.cnt[c] = 0;  // ready for the next rebuild; nobody reads cnt in this phase
+        for (int i = tid; i < a.n; i += T) {
+            int c = __ldcg(&a.cellof[i]);
+            int b = s_tab[c], e = s_tab[c + 1];
+            int r = 0;
+            for (int k = b; k < e; ++k) r += __ldcg(&a.ci_tmp[k]) < i;
+            a.ci[b + r] = i;
+            if (rad)
+                a.sp[b + r] = make_float4(__ldcg(&dst[3 * i + 0]), __ldcg(&dst[3 * i + 1]),
+                                          __ldcg(&dst[3 * i + 2]), __ldcg(&rad[i]));
+        }
+        if (!last && !grid_barrier(a.ds, ep)) return false;
+        trace_mark(a, tk);
+        return true;
+    }
+    // P2: each block scans its chunk of cells (local exclusive offsets + total)
+    {
+        int c0 = blockIdx.x * a.chunk;
+        int carry = 0;
+        for (int base = c0; base < c0 + a.chunk; base += blockDim.x) {
+            int c = base + threadIdx.x;
+            bool in = c < c0 + a.chunk && c < a.G3;
+            int v = in ? __ldcg(&a.cnt[c]) : 0;
+            int tot;
+            int ex = coop_block_scan(v, &tot);
+            if (in) {
+                a.part[c] = carry + ex;
+                a.cc[c] = v;
+            }
+            carry += tot;
+        }
+        if (threadIdx.x == 0) a.bsum[blockIdx.x] = carry;
+    }
+    if (!grid_barrier(a.ds, ep)) return false;
+    trace_mark(a, tk);
+    // P3: block-sum prefix, final cell starts of this block's chunk, rank scatter
+    {
+        __shared__ int s_pre[1024];  // gridDim.x <= 1024 (checked on the host)
+        int v = threadIdx.x < gridDim.x ? __ldcg(&a.bsum[threadIdx.x]) : 0;
+        int tot;
+        int ex = coop_block_scan(v, &tot);
+        s_pre[threadIdx.x] = ex;
+        __syncthreads();
+        int c0 = blockIdx.x * a.chunk;
+        for (int c = c0 + threadIdx.x; c < c0 + a.chunk && c < a.G3; c += blockDim.x) {
+            a.cs[c] = __ldcg(&a.part[c]) + s_pre[blockIdx.x];
+            a.cnt[c] = 0;  // ready for the next rebuild; nobody reads cnt in this phase
+        }
+        for (int i = tid; i < a.n; i += T) {
+            int c = __ldcg(&a.cellof[i]);
+            int slot = __ldcg(&a.part[c]) + s_pre[c / a.chunk] + __ldcg(&a.rank[i]);
+            a.ci_tmp[slot] = i;
+        }
+    }
+    if (!grid_barrier(a.ds, ep)) return false;
+    trace_mark(a, tk);
+    // P4: stable placement: slot = cell start + #(lower-indexed particles in the cell)
+    for (int i = tid; i < a.n; i += T) {
+        int c = __ldcg(&a.cellof[i]);
+        int b = __ldcg(&a.cs[c]), e = b + __ldcg(&a.cc[c]);
+        int r = 0;
+        for (int k = b; k < e; ++k) r += __ldcg(&a.ci_tmp[k]) < i;
+        a.ci[b + r] = i;
+        if (rad) {
+            a.sp[b + r] = make_float4(__ldcg(&dst[3 * i + 0]), __ldcg(&dst[3 * i + 1]),
+                                      __ldcg(&dst[3 * i + 2]), __ldcg(&rad[i]));
+        }
+    }
+    if (!last && !grid_barrier(a.ds, ep)) return false;
+    trace_mark(a, tk);
+    return true;
+}
+
+__global__ void __launch_bounds__(COOP_THREADS) k_frame_coop(CoopArgs a) {
+    const int T = gridDim.x * blockDim.x;
+    const int tid = blockIdx.x * blockDim.x + threadIdx.x;
+    const int lane = threadIdx.x & 31;
+    const int W = T >> 5;
+    const int wid = tid >> 5;
+    // rounds of work with block-uniform trip counts (block reductions inside)
+    const int warp_rounds = (a.n + W - 1) / W;
+    int tk = 0;
+    unsigned int ep = 0;
+    trace_mark(a, tk);
+
+    // (1) rebuild_grid (run.py:704)
+    if (!coop_grid(a, a.pos, a.pos, a.rad, false, tk, ep)) return;
+    // (2) compute_max_overlap (run.py:709)
+    for (int r = 0; r < warp_rounds; ++r) {
+        int kk = r * W + wid;
+        unsigned int b = 0u;
+        if (kk < a.n) b = maxov_warp<LdL2>(kk, lane, a.sp, a.ci, a.g, a.cs, a.cc, a.eps, a.lmd);
+        block_max_atomic(b, &a.ds->omax_bits);
+    }
+    if (!grid_barrier(a.ds, ep)) return;
+    trace_mark(a, tk);
+    // (3) nudge_radii_adaptive_ema while settle_frames_left > 0 (run.py:744-750)
+    if (*((volatile int*)&a.ds->settle) > 0) {
+        float bg = back_global_from_bits(*((volatile unsigned int*)&a.ds->omax_bits),
+                                         a.contact_tol_d);
+        for (int i = tid; i < a.n; i += T)
+            a.rad[i] = nudge_one(__ldcg(&a.rad[i]), __ldcg(&a.rad_target[i]), __ldcg(&a.lmd[i]),
+                                 a.alpha, a.max_step, a.rmin, a.rmax, bg, a.bp_mode,
+                                 a.contact_tol);
+    }
+    if (!grid_barrier(a.ds, ep)) return;
+    trace_mark(a, tk);
+    // (4) pressure sweeps (run.py:755-771); the last sweep reports its stats
+    PressureArgs pa = a.pa;
+    pa.frame = *((volatile int*)&a.ds->frame);
+    const int groups_per_round = T / 16;
+    const int p_rounds = (a.n + groups_per_round - 1) / groups_per_round;
+    for (int w = 0; w < a.sweeps; ++w) {
+        const float* rin = (w & 1) ? a.rad_tmp : a.rad;
+        float* rout = (w & 1) ? a.rad : a.rad_tmp;
+        bool last = (w == a.sweeps - 1);
+        for (int r = 0; r < p_rounds; ++r) {
+            int i = r * groups_per_round + tid / 16;
+            float d = pressure_group<16, LdL2>(i, lane, pa, rin, rout, a.delta_r);
+            if (last) {
+                float ad = fabsf(d);
+                int ch = (i < a.n && (lane & 15) == 0) && ad > 1e-12f;
+                int cnt = __syncthreads_count(ch);
+                unsigned int bm = __reduce_max_sync(0xffffffffu, ch ? __float_as_uint(ad) : 0u);
+                block_max_atomic(bm, &a.ds->maxabs_dr_bits);
+                if (threadIdx.x == 0 && cnt) atomicAdd(&a.ds->changed, cnt);
+            }
+        }
+        if (!grid_barrier(a.ds, ep)) return;
+        trace_mark(a, tk);
+    }
+    // (5) apply_brownian_motion (run.py:807-813); the odd-sweep result is copied
+    // back into rad, and settle_frames_left -= 1 (run.py:750)
+    {
+        unsigned int frame = (unsigned int)pa.frame;
+        for (int i = tid; i < a.n; i += T) {
+            if (a.sweeps & 1) a.rad[i] = __ldcg(&a.rad_tmp[i]);
+            brownian_one<LdL2>(i, a.pos, a.strength, a.domain, a.halfL, a.k0, a.k1, frame);
+        }
+        if (tid == 0 && a.ds->settle > 0) a.ds->settle -= 1;
+    }
+    if (!grid_barrier(a.ds, ep)) return;
+    trace_mark(a, tk);
+    // (6) PBD passes, each on a fresh grid (run.py:829-846); (7) rebuild (run.py:874)
+    const float* src = a.pos;
+    for (int k = 0; k < a.pbd_iters; ++k) {
+        if (!coop_grid(a, src, a.pos, a.rad, false, tk, ep)) return;
+        for (int r = 0; r < warp_rounds; ++r) {
+            int kk = r * W + wid;
+            if (kk < a.n)
+                pbd_warp<LdL2>(kk, lane, a.sp, a.ci, a.pos_tmp, a.g, a.cs, a.cc, a.gap1, a.mdf,
+                               a.dmul);
+        }
+        if (!grid_barrier(a.ds, ep)) return;
+        trace_mark(a, tk);
+        src = a.pos_tmp;
+    }
+    coop_grid(a, src, a.pos, nullptr, true, tk, ep);
+}
+
+__global__ void k_coop_prep(FosDevState* ds) {
+    ds->omax_bits = 0u;
+    ds->maxabs_dr_bits = 0u;
+    ds->changed = 0;
+    ds->bar_count = 0u;
+}
+
+// Host side ---------------------------------------------------------------
+static int coop_grid_size(FosCtx* c) {
+    if (c->coop_blocks >= 0) return c->coop_blocks;
+    int per_sm = 0;
+    if (cudaFuncSetAttribute(k_frame_coop, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (COOP_SMALL_G3 + 1) * 4) != cudaSuccess)
+        return -1;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_frame_coop, COOP_THREADS,
+                                                      (COOP_SMALL_G3 + 1) * 4) != cudaSuccess)
+        return -1;
+    if (per_sm > 1) per_sm = 1;  // one full block per SM: fewest barrier arrivals
+    int blocks = per_sm * c->num_sms;
+    if (blocks > 1024) blocks = 1024;
+    c->coop_blocks = blocks;
+    return blocks;
+}
+
+bool fos_coop_supported(FosCtx* c) {
+    int dev = c->device, ok = 0;
+    cudaDeviceGetAttribute(&ok, cudaDevAttrCooperativeLaunch, dev);
+    return ok && coop_grid_size(c) > 0;
+}
+
+int fos_frame_coop_dynamics(FosCtx* c, const FosState* st, const FosFrameParams* fp,
+                            cudaStream_t s, unsigned long long* trace, int trace_cap) {
+    int blocks = coop_grid_size(c);
+    FOS_REQUIRE(blocks > 0, FOS_E_CUDA, "cooperative frame kernel cannot be resident");
+    const int n = st->n;
+    const int G3 = c->G * c->G * c->G;
+    CoopArgs a;
+    memset(&a, 0, sizeof(a));
+    a.n = n;
+    a.G3 = G3;
+    a.chunk = (G3 + blocks - 1) / blocks;
+    a.small_grid = G3 <= COOP_SMALL_G3 ? 1 : 0;
+    a.pbd_iters = fp->pbd_iters;
+    a.sweeps = fp->pressure_iters;
+    a.bp_mode = fp->bp_mode;
+    a.g = GridGeom{c->G, c->L, c->invL, c->halfL};
+    a.pos = st->pos;
+    a.pos_tmp = c->pos_tmp;
+    a.rad = st->rad;
+    a.rad_tmp = c->rad_tmp;
+    a.rad_target = st->rad_target;
+    a.lmd = st->local_max_depth;
+    a.delta_r = st->delta_r;
+    a.cc = st->cell_count;
+    a.cs = st->cell_start;
+    a.ci = st->cell_indices;
+    a.cellof = c->cellof;
+    a.rank = c->rank;
+    a.ci_tmp = c->ci_tmp;
+    a.cnt = c->coop_cnt;
+    a.part = c->coop_part;
+    a.bsum = c->coop_bsum;
+    a.sp = c->sorted;
+    a.ds = c->ds;
+    a.gap1 = c->gap1;
+    a.mdf = c->mdf;
+    a.dmul = c->dmul;
+    a.eps = c->eps;
+    a.contact_tol = c->contact_tol;
+    a.contact_tol_d = c->p.contact_tol;
+    a.alpha = (float)(1.0 - pow(0.05, 1.0 / (double)(fp->adjustment_frames > 1 ? fp->adjustment_frames : 1)));
+    a.max_step = (float)fp->max_step_pct;
+    a.rmin = (float)fp->r_min;
+    a.rmax = (float)fp->r_max;
+    a.pa = PressureArgs{n,
+                        0,
+                        fp->max_eq_nei,
+                        (float)fp->pressure_k,
+                        (float)fp->pressure_exp,
+                        (float)fp->pressure_pair_cap,
+                        (float)fp->r_min,
+                        (float)fp->r_max,
+                        c->face_ids,
+                        c->fsc};
+    a.strength = (float)fp->brownian_strength;
+    a.domain = c->L;
+    a.halfL = (float)(0.5 * (double)c->L);
+    a.k0 = (uint32_t)fp->seed;
+    a.k1 = (uint32_t)(fp->seed >> 32);
+    a.trace = trace;
+    a.trace_cap = trace_cap;
+
+    FOS_REQUIRE(fp->max_eq_nei <= 16, FOS_E_ARG, "cooperative frame needs max_eq_nei <= 16");
+    k_coop_prep<<<1, 1, 0, s>>>(c->ds);
+    FOS_LAUNCHED(c);
+    FOS_CUDA(cudaMemsetAsync(c->coop_cnt, 0, (size_t)G3 * sizeof(int32_t), s));
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(blocks);
+    cfg.blockDim = dim3(COOP_THREADS);
+    cfg.dynamicSmemBytes = a.small_grid ? (size_t)(G3 + 1) * 4 : 0;
+    cfg.stream = s;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeCooperative;
+    attr[0].val.cooperative = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    FOS_CUDA(cudaLaunchKernelEx(&cfg, k_frame_coop, a));
+    FOS_LAUNCHED(c);
+    return FOS_OK;
+}
+
+// Cooperative dynamics of one frame with %globaltimer stamps after every phase
+// (block 0's view): stamp 0 at kernel entry, then one per grid barrier.
+extern "C" int fos_frame_trace(FosCtx* c, const FosState* st, const FosFrameParams* fp,
+                               long long* ns_host, int cap, int* count, fos_stream_t s) {
+    FOS_REQUIRE(c && st && fp && ns_host && count && cap > 0, FOS_E_ARG, "NULL argument");
+    FOS_REQUIRE(fos_coop_supported(c), FOS_E_STATE, "cooperative launch unsupported");
+    unsigned long long* d = nullptr;
+    FOS_CUDA(cudaMalloc(&d, (size_t)cap * 8));
+    cudaMemsetAsync(d, 0, (size_t)cap * 8, s);
+    int rc = fos_frame_coop_dynamics(c, st, fp, s, d, cap);
+    if (rc == FOS_OK) {
+        cudaError_t e = cudaMemcpyAsync(ns_host, d, (size_t)cap * 8, cudaMemcpyDeviceToHost, s);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+        if (e != cudaSuccess) rc = fos_cuda_fail(e, "trace readback", __FILE__, __LINE__);
+    }
+    cudaFree(d);
+    int k = 0;
+    while (k < cap && ns_host[k] != 0) ++k;
+    *count = k;
+    return rc;
+}

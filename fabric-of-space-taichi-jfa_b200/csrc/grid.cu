@@ -6,20 +6,7 @@
 // order) make each cell's slice of cell_indices ascending, and that is what
 // these kernels produce: histogram with per-particle rank -> exclusive scan ->
 // rank scatter -> per-cell sort of the (short) slices.
-#include "fos_internal.cuh"
-
-// Cell of an already wrapped position (grid.py:204-222):
-// floor(((w + HALF_L) + 1e-7) * INV_L * GRID_RES), wrapped, c0*G*G + c1*G + c2.
-__device__ __forceinline__ int cell_of_wrapped(float wx, float wy, float wz, float invL,
-                                               float halfL, int G) {
-    float q0 = fmul(fadd(fadd(wx, halfL), 1e-7f), invL);
-    float q1 = fmul(fadd(fadd(wy, halfL), 1e-7f), invL);
-    float q2 = fmul(fadd(fadd(wz, halfL), 1e-7f), invL);
-    int c0 = wrap_mod((int)floorf(fmul(q0, (float)G)), G);
-    int c1 = wrap_mod((int)floorf(fmul(q1, (float)G)), G);
-    int c2 = wrap_mod((int)floorf(fmul(q2, (float)G)), G);
-    return (c0 * G + c1) * G + c2;
-}
+#include "phases.cuh"
 
 // count_particles_per_cell (grid.py:186-222).  Optionally also writes the
 // wrapped position to dst (scatter_particles' write-back, grid.py:287-288)
@@ -116,6 +103,8 @@ int fos_grid_gather_sorted(FosCtx* c, const int32_t* idx, const float* pos, cons
     FOS_LAUNCHED(c);
     return FOS_OK;
 }
+
+int fos_grid_init_attributes() { return FOS_OK; }
 
 static int check_grid(FosCtx* c, int n) {
     FOS_REQUIRE(c != nullptr, FOS_E_ARG, "ctx is NULL");

@@ -86,20 +86,19 @@ __device__ __forceinline__ bool jfa_exited_before(const FosDevState* ds, int p, 
 // running minimum, so a voxel waits for three rounds of gather latency rather
 // than one per evaluated candidate.  A plane no lane of the warp needs is
 // skipped with one vote.
-template <bool UNIT_L, bool POW2, bool TIE_LOWER>
+template <bool UNIT_L>
 __device__ __forceinline__ float jfa_dist(float vx, float vy, float vz, float4 s, float L) {
-    return UNIT_L ? power_dist_unit(vx, vy, vz, s) : power_dist<false>(vx, vy, vz, s, L);
+    if (!UNIT_L) return power_dist<false>(vx, vy, vz, s, L);
+    return power_dist_unit(vx, vy, vz, s);
 }
 
 template <bool UNIT_L, bool POW2, bool TIE_LOWER>
-__global__ void __launch_bounds__(256) k_jfa_pass(const int32_t* __restrict__ in,
-                                                  int32_t* __restrict__ out,
-                                                  const float4* __restrict__ seeds, int R, int lgR,
-                                                  float vs, float halfL, float L, int step,
-                                                  FosDevState* ds, int pass, int early_exit,
-                                                  int min_passes, double th) {
+__device__ __forceinline__ void jfa_pass_body(const int32_t* __restrict__ in,
+                                              int32_t* __restrict__ out,
+                                              const float4* __restrict__ seeds, int R, int lgR,
+                                              float vs, float halfL, float L, int step,
+                                              FosDevState* ds, int pass) {
     const long long V = (long long)R * R * R;
-    if (early_exit && jfa_exited_before(ds, pass, (double)V, min_passes, th)) return;
     long long lin = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     bool live = lin < V;
     long long l = live ? lin : 0;
@@ -139,7 +138,7 @@ __global__ void __launch_bounds__(256) k_jfa_pass(const int32_t* __restrict__ in
           vz = voxel_centre(z, vs, halfL);
     int best = own;
     float bd = 1e10f;
-    if (own >= 0) bd = jfa_dist<UNIT_L, POW2, TIE_LOWER>(vx, vy, vz, __ldg(&seeds[own]), L);
+    if (own >= 0) bd = jfa_dist<UNIT_L>(vx, vy, vz, __ldg(&seeds[own]), L);
 #pragma unroll
     for (int g = 0; g < 3; ++g) {
         bool ok[9];
@@ -160,7 +159,7 @@ __global__ void __launch_bounds__(256) k_jfa_pass(const int32_t* __restrict__ in
 #pragma unroll
         for (int k = 0; k < 9; ++k) {
             int id = ids[g * 9 + k];
-            float d = jfa_dist<UNIT_L, POW2, TIE_LOWER>(vx, vy, vz, sv[k], L);
+            float d = jfa_dist<UNIT_L>(vx, vy, vz, sv[k], L);
             if (ok[k] && (d < bd || (TIE_LOWER && d == bd && id < best))) {
                 bd = d;
                 best = id;
@@ -172,8 +171,21 @@ __global__ void __launch_bounds__(256) k_jfa_pass(const int32_t* __restrict__ in
         out[lin] = best;
         changed = best != own;
     }
-    unsigned int m = __ballot_sync(0xffffffffu, changed);
-    if ((threadIdx.x & 31) == 0 && m) atomicAdd(&ds->changes[pass], (unsigned long long)__popc(m));
+    // one atomic per block: same-address atomics from every warp serialise in L2
+    int cnt = __syncthreads_count(changed);
+    if (threadIdx.x == 0 && cnt) atomicAdd(&ds->changes[pass], (unsigned long long)cnt);
+}
+
+template <bool UNIT_L, bool POW2, bool TIE_LOWER>
+__global__ void __launch_bounds__(256) k_jfa_pass(const int32_t* __restrict__ in,
+                                                  int32_t* __restrict__ out,
+                                                  const float4* __restrict__ seeds, int R, int lgR,
+                                                  float vs, float halfL, float L, int step,
+                                                  FosDevState* ds, int pass, int early_exit,
+                                                  int min_passes, double th) {
+    const long long V = (long long)R * R * R;
+    if (early_exit && jfa_exited_before(ds, pass, (double)V, min_passes, th)) return;
+    jfa_pass_body<UNIT_L, POW2, TIE_LOWER>(in, out, seeds, R, lgR, vs, halfL, L, step, ds, pass);
 }
 
 __global__ void k_jfa_finish(FosDevState* ds, int passes, long long V, int early_exit,
@@ -529,12 +541,13 @@ __global__ void __launch_bounds__(256) k_finalize(int n, const int32_t* __restri
     uint8_t* cur = acc0;
     uint8_t* nxt = acc1;
     int it = 0;
+    unsigned int epoch = 0;
     for (;;) {
         int ch = 0;
         for (int i = tid; i < n; i += stride)
             ch |= fin_row(i, revstart, rev, cur, nxt, score, prev, t_add, t_drop);
         if (__syncthreads_or(ch) && threadIdx.x == 0) atomicOr(&fin_changed[it], 1);
-        if (!grid_barrier(ds)) return;
+        if (!grid_barrier(ds, epoch)) return;
         int any = *((volatile int*)&fin_changed[it]);
         uint8_t* t = cur;
         cur = nxt;

@@ -1,0 +1,361 @@
+// phases.cuh -- per-particle / per-warp device functions of the frame's
+// stages.  The standalone kernels (grid.cu, dynamics.cu) and the persistent
+// cooperative frame kernel (frame_coop.cu) both call these, so each stage's
+// arithmetic exists once.
+//
+// Reference: grid.py (cells, wrap), dynamics.py (PBD, max overlap, pressure,
+// Brownian, FSC controller).  FP32 expressions keep the reference's operator
+// order with explicit round-to-nearest intrinsics (no FMA contraction).
+#pragma once
+
+#include "fos_internal.cuh"
+
+// Load policies.  Standalone kernels read data no thread of the same launch
+// writes, through the read-only path (LdRO); the persistent cooperative frame
+// kernel rewrites cells, positions and radii between its phases, and other
+// SMs' L1 lines would go stale, so it reads through L2 (LdL2).
+struct LdRO {
+    template <class T>
+    __device__ __forceinline__ static T ld(const T* p) { return __ldg(p); }
+};
+struct LdL2 {
+    template <class T>
+    __device__ __forceinline__ static T ld(const T* p) { return __ldcg(p); }
+};
+
+// ------------------------------------------------------------------ grid
+// Cell of an already wrapped position (grid.py:204-222):
+// floor(((w + HALF_L) + 1e-7) * INV_L * GRID_RES), wrapped, c0*G*G + c1*G + c2.
+__device__ __forceinline__ int cell_of_wrapped(float wx, float wy, float wz, float invL,
+                                               float halfL, int G) {
+    float q0 = fmul(fadd(fadd(wx, halfL), 1e-7f), invL);
+    float q1 = fmul(fadd(fadd(wy, halfL), 1e-7f), invL);
+    float q2 = fmul(fadd(fadd(wz, halfL), 1e-7f), invL);
+    int c0 = wrap_mod((int)floorf(fmul(q0, (float)G)), G);
+    int c1 = wrap_mod((int)floorf(fmul(q1, (float)G)), G);
+    int c2 = wrap_mod((int)floorf(fmul(q2, (float)G)), G);
+    return (c0 * G + c1) * G + c2;
+}
+
+// Home cell as project_overlaps / compute_local_max_overlaps compute it
+// (dynamics.py:101-103): int(((wrapP(p) + HALF_L) * INV_L) * GRID_RES), no
+// epsilon and no wrap before the +-1 offsets.
+__device__ __forceinline__ int home_coord(float p, float L, float invL, float halfL, int G) {
+    float w = grid_wrap(p, L, invL);
+    float q = fmul(fadd(w, halfL), invL);
+    return (int)fmul(q, (float)G);
+}
+
+// Block-wide max of one value per warp (lane 0's), then a single atomicMax
+// per block: same-address atomics from every warp serialise in L2.  Every
+// warp of the block must call it once.
+__device__ __forceinline__ void block_max_atomic(unsigned int warp_val, unsigned int* target) {
+    __shared__ unsigned int s_max;
+    if (threadIdx.x == 0) s_max = 0u;
+    __syncthreads();
+    if ((threadIdx.x & 31) == 0 && warp_val) atomicMax(&s_max, warp_val);
+    __syncthreads();
+    if (threadIdx.x == 0 && s_max) atomicMax(target, s_max);
+}
+
+// ------------------------------------------------------------------
+// Warp-cooperative enumeration of a particle's 27-cell neighbourhood.
+// Lane l < 27 owns cell l of the stencil in the reference's (dx, dy, dz)
+// order (dz fastest); an inclusive warp scan of the cell counts numbers the
+// candidates 0..total-1 in exactly the order of the reference's nested loops
+// (cells in stencil order, particles ascending inside a cell).  Candidate t
+// is located by a binary search over the scanned counts.
+struct Stencil {
+    int st, excl, incl, total;
+};
+
+template <class LD>
+__device__ __forceinline__ Stencil stencil_ranges(float px, float py, float pz, float L, float invL,
+                                                  float halfL, int G, const int32_t* cs,
+                                                  const int32_t* cc, int lane) {
+    int hx = home_coord(px, L, invL, halfL, G);
+    int hy = home_coord(py, L, invL, halfL, G);
+    int hz = home_coord(pz, L, invL, halfL, G);
+    int st = 0, ct = 0;
+    if (lane < 27) {
+        int nx = wrap_mod(hx + lane / 9 - 1, G);
+        int ny = wrap_mod(hy + (lane / 3) % 3 - 1, G);
+        int nz = wrap_mod(hz + lane % 3 - 1, G);
+        int cid = (nx * G + ny) * G + nz;
+        st = LD::ld(&cs[cid]);
+        ct = LD::ld(&cc[cid]);
+    }
+    int incl = ct;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        int y = __shfl_up_sync(0xffffffffu, incl, o);
+        if (lane >= o) incl += y;
+    }
+    Stencil r;
+    r.st = st;
+    r.incl = incl;
+    r.excl = incl - ct;
+    r.total = __shfl_sync(0xffffffffu, incl, 31);
+    return r;
+}
+
+// Sorted-array position of candidate t (t < total).
+__device__ __forceinline__ int stencil_locate(const Stencil& r, int t) {
+    int c = 0;
+#pragma unroll
+    for (int step = 16; step >= 1; step >>= 1) {
+        int v = __shfl_sync(0xffffffffu, r.incl, c + step - 1);
+        if (v <= t) c += step;
+    }
+    int src = c & 31;
+    int st = __shfl_sync(0xffffffffu, r.st, src);
+    int ex = __shfl_sync(0xffffffffu, r.excl, src);
+    return st + (t - ex);
+}
+
+struct GridGeom {
+    int G;
+    float L, invL, halfL;
+};
+
+// project_overlaps (dynamics.py:77-171) for the particle at sorted position
+// kk, as one Jacobi sweep: reads the pre-sweep positions (the cell-ordered
+// copy sp holds pos and rad) and writes pout[i].  The whole warp cooperates:
+// lanes evaluate 32 candidates at a time and the corrections of overlapping
+// pairs are added in candidate order, so the FP32 sum is the reference loop's
+// sum bit for bit.  Must be called by all 32 lanes.
+template <class LD>
+__device__ __forceinline__ void pbd_warp(int kk, int lane, const float4* sp, const int32_t* ci,
+                                         float* pout, const GridGeom g, const int32_t* cs,
+                                         const int32_t* cc, float gap1, float mdf, float dmul) {
+    float4 me = LD::ld(&sp[kk]);
+    float px = me.x, py = me.y, pz = me.z, ri = me.w;
+    Stencil r = stencil_ranges<LD>(px, py, pz, g.L, g.invL, g.halfL, g.G, cs, cc, lane);
+    float md = fmul(mdf, ri);
+    float cx = 0.f, cy = 0.f, cz = 0.f;
+    for (int base = 0; base < r.total; base += 32) {
+        int t = base + lane;
+        int k = stencil_locate(r, t < r.total ? t : r.total - 1);
+        bool hit = false;
+        float vx = 0.f, vy = 0.f, vz = 0.f;
+        if (t < r.total && k != kk) {
+            float4 q = LD::ld(&sp[k]);
+            float ddx = grid_wrap(fsub(q.x, px), g.L, g.invL);
+            float ddy = grid_wrap(fsub(q.y, py), g.L, g.invL);
+            float ddz = grid_wrap(fsub(q.z, pz), g.L, g.invL);
+            float d2 = fadd(fadd(fadd(fmul(ddx, ddx), fmul(ddy, ddy)), fmul(ddz, ddz)), 1e-12f);
+            float dist = __fsqrt_rn(d2);
+            float tsep = fmul(fadd(ri, q.w), gap1);
+            if (dist < tsep) {
+                hit = true;
+                float ov = fsub(tsep, dist);
+                float ux = fdiv(ddx, dist), uy = fdiv(ddy, dist), uz = fdiv(ddz, dist);
+                float mag = fminf(fmul(ov, 0.5f), md);
+                vx = fmaxf(-md, fminf(md, fmul(-ux, mag)));
+                vy = fmaxf(-md, fminf(md, fmul(-uy, mag)));
+                vz = fmaxf(-md, fminf(md, fmul(-uz, mag)));
+            }
+        }
+        unsigned int m = __ballot_sync(0xffffffffu, hit);
+        while (m) {
+            int b = __ffs(m) - 1;
+            m &= m - 1;
+            cx = fadd(cx, __shfl_sync(0xffffffffu, vx, b));
+            cy = fadd(cy, __shfl_sync(0xffffffffu, vy, b));
+            cz = fadd(cz, __shfl_sync(0xffffffffu, vz, b));
+        }
+    }
+    if (lane == 0) {
+        float mt = fmul(fmul(mdf, ri), dmul);
+        float cm = __fsqrt_rn(fadd(fadd(fmul(cx, cx), fmul(cy, cy)), fmul(cz, cz)));
+        if (cm > mt) {
+            float sc = fdiv(mt, cm);
+            cx = fmul(cx, sc);
+            cy = fmul(cy, sc);
+            cz = fmul(cz, sc);
+        }
+        int i = LD::ld(&ci[kk]);
+        pout[3 * i + 0] = grid_wrap(fadd(px, cx), g.L, g.invL);
+        pout[3 * i + 1] = grid_wrap(fadd(py, cy), g.L, g.invL);
+        pout[3 * i + 2] = grid_wrap(fadd(pz, cz), g.L, g.invL);
+    }
+}
+
+// compute_local_max_overlaps (dynamics.py:304-352) for the particle at
+// sorted position kk (pairs i < j only); writes lmd[i] and returns the depth's
+// float bits (non-negative floats order as their bits).  All 32 lanes.
+template <class LD>
+__device__ __forceinline__ unsigned int maxov_warp(int kk, int lane, const float4* sp,
+                                                   const int32_t* ci, const GridGeom g,
+                                                   const int32_t* cs, const int32_t* cc, float eps,
+                                                   float* lmd) {
+    float4 me = LD::ld(&sp[kk]);
+    int i = LD::ld(&ci[kk]);
+    Stencil r = stencil_ranges<LD>(me.x, me.y, me.z, g.L, g.invL, g.halfL, g.G, cs, cc, lane);
+    float lm = 0.f;
+    for (int base = 0; base < r.total; base += 32) {
+        int t = base + lane;
+        int k = stencil_locate(r, t < r.total ? t : r.total - 1);
+        if (t < r.total) {
+            int j = LD::ld(&ci[k]);
+            if (i < j) {
+                float4 q = LD::ld(&sp[k]);
+                float ddx = grid_wrap(fsub(q.x, me.x), g.L, g.invL);
+                float ddy = grid_wrap(fsub(q.y, me.y), g.L, g.invL);
+                float ddz = grid_wrap(fsub(q.z, me.z), g.L, g.invL);
+                float dist = __fsqrt_rn(
+                    fadd(fadd(fadd(fmul(ddx, ddx), fmul(ddy, ddy)), fmul(ddz, ddz)), eps));
+                float td = fadd(me.w, q.w);
+                if (dist < td) lm = fmaxf(lm, fsub(td, dist));
+            }
+        }
+    }
+    unsigned int b = __reduce_max_sync(0xffffffffu, __float_as_uint(lm));
+    if (lane == 0) lmd[i] = __uint_as_float(b);
+    return b;
+}
+
+// hash_func (dynamics.py:1436-1451) in wrapping int32 arithmetic.
+__device__ __forceinline__ int hash_func(int i, int frame) {
+    unsigned int t = (unsigned int)i + 12345u * (unsigned int)frame;
+    return (int)((1103515245u * t + 12345u) & 0x7fffffffu);
+}
+
+struct PressureArgs {
+    int n, frame, max_nei;
+    float k, P, cap, rmin, rmax;
+    const int32_t* face_ids;
+    const int32_t* fsc;
+};
+
+// equilibrate_pressure (dynamics.py:1454-1557) for particle i, one Jacobi
+// sweep, by a group of GS lanes: lane t handles the t-th budgeted neighbour
+// of the hashed rotation and the radius deltas are summed in neighbour order
+// (the reference's serial accumulation).  Lane 0 of the group writes
+// rout[i] and delta_r[i] and gets d back; all GS lanes of the group call it
+// (i may be >= n: the group then does nothing).
+template <int GS, class LD>
+__device__ __forceinline__ float pressure_group(int i, int lane, const PressureArgs a,
+                                                const float* rin, float* rout, float* delta_r) {
+    int gl = lane & (GS - 1);
+    unsigned int gmask = GS == 32 ? 0xffffffffu : (0xffffu << (lane & 16));
+    bool live = i < a.n;
+    float ri = live ? LD::ld(&rin[i]) : 0.f;
+    int fc = live ? LD::ld(&a.fsc[i]) : 0;
+    float d = 0.f;
+    if (fc > 0) {
+        int an = fc < a.max_nei ? fc : a.max_nei;
+        int st = hash_func(i, a.frame) % fc;
+        float Vi = powf(ri, a.P);
+        float invP = fdiv(1.0f, a.P);
+        for (int base = 0; base < an; base += GS) {
+            int kk = base + gl;
+            bool hit = false;
+            float term = 0.f;
+            if (kk < an) {
+                int ni = (st + kk) % fc;
+                int j = LD::ld(&a.face_ids[(size_t)i * FOS_S + ni]);
+                if (!(j < 0 || j >= a.n || j == i)) {
+                    float Vj = powf(LD::ld(&rin[j]), a.P);
+                    float dvr = fmul(a.k, fsub(Vi, Vj));
+                    float vmin = fminf(Vi, Vj);
+                    float dv = fmaxf(fmul(-a.cap, vmin), fminf(fmul(a.cap, vmin), dvr));
+                    term = fsub(powf(fsub(Vi, dv), invP), ri);
+                    hit = true;
+                }
+            }
+            unsigned int m = __ballot_sync(gmask, hit) & gmask;
+            m >>= (GS == 32 ? 0 : (lane & 16));
+            while (m) {
+                int b = __ffs(m) - 1;
+                m &= m - 1;
+                d = fadd(d, __shfl_sync(gmask, term, b, GS));
+            }
+        }
+    }
+    if (live && gl == 0) {
+        delta_r[i] = d;
+        rout[i] = fmaxf(a.rmin, fminf(a.rmax, fadd(ri, d)));
+    }
+    return d;
+}
+
+// apply_brownian_motion (dynamics.py:1596-1634) for particle i.  ti.random()
+// is replaced by Philox-4x32-10 with counter (i, frame, 'BROW', 0) and key =
+// seed; each axis draws u = (x >> 8) * 2^-24.
+template <class LD>
+__device__ __forceinline__ void brownian_one(int i, float* pos, float strength, float domain,
+                                             float halfL, uint32_t k0, uint32_t k1,
+                                             unsigned int frame) {
+    uint4 r = philox4x32_10(make_uint4((unsigned int)i, frame, 0x42524f57u, 0u), k0, k1);
+    unsigned int rr[3] = {r.x, r.y, r.z};
+#pragma unroll
+    for (int d = 0; d < 3; ++d) {
+        float u = fmul((float)(rr[d] >> 8), 0x1p-24f);
+        float dd = fmul(fmul(fsub(u, 0.5f), 2.0f), strength);
+        float p = fadd(LD::ld(&pos[3 * i + d]), dd);
+        if (p < -halfL) p = fadd(p, domain);
+        else if (p >= halfL) p = fsub(p, domain);
+        pos[3 * i + d] = p;
+    }
+}
+
+// smoothstep (dynamics.py:1226-1240)
+__device__ __forceinline__ float smoothstep(float e0, float e1, float x) {
+    float t = fminf(1.0f, fmaxf(0.0f, fdiv(fsub(x, e0), fsub(e1, e0))));
+    return fmul(fmul(t, t), fsub(3.0f, fmul(2.0f, t)));
+}
+
+// set_fsc_targets (dynamics.py:1242-1320) for particle i.
+__device__ __forceinline__ float target_one(float r0, float e, int f_i, int f_low, int f_high,
+                                            float growth, float rmin, float rmax, float db) {
+    const float hg = 1.0f, idle = 0.003f;
+    float f = e > 0.0f ? e : (float)f_i;
+    float lo = (float)f_low, hi = (float)f_high;
+    float out;
+    if (f < fsub(lo, hg)) {
+        out = fminf(fmul(r0, fadd(1.0f, fmul(growth, 1.0f))), rmax);
+    } else if (f < lo) {
+        float gain = fsub(1.0f, smoothstep(fsub(fsub(lo, hg), db), lo, f));
+        out = fminf(fmul(r0, fadd(1.0f, fmul(growth, gain))), rmax);
+    } else if (f > fadd(hi, hg)) {
+        out = fmaxf(fmul(r0, fsub(1.0f, fmul(growth, 1.0f))), rmin);
+    } else if (f > hi) {
+        float gain = smoothstep(hi, fadd(fadd(hi, hg), db), f);
+        out = fmaxf(fmul(r0, fsub(1.0f, fmul(growth, gain))), rmin);
+    } else {
+        float bc = fmul(0.5f, fadd(lo, hi));
+        if (f < bc) out = fminf(fmul(r0, fadd(1.0f, fmul(growth, idle))), rmax);
+        else out = fmaxf(fmul(r0, fsub(1.0f, fmul(growth, idle))), rmin);
+    }
+    return out;
+}
+
+// nudge_radii_adaptive_ema (dynamics.py:1366-1427) for particle i; b_global
+// is the global backpressure (used in mode 1).
+__device__ __forceinline__ float nudge_one(float r0, float rt_i, float lmd_i, float alpha,
+                                           float max_step, float rmin, float rmax, float b_global,
+                                           int mode, float contact_tol) {
+    float r_t = fminf(rmax, fmaxf(rmin, rt_i));
+    float d = fmul(alpha, fsub(r_t, r0));
+    float b = 1.0f;
+    if (mode == 1) b = b_global;
+    else if (mode == 2) {
+        b = fdiv(fsub(contact_tol, lmd_i), contact_tol);
+        b = fminf(1.0f, fmaxf(0.25f, b));
+    }
+    d = fmul(d, b);
+    float cap = fmul(max_step, r0);
+    if (d > cap) d = cap;
+    if (d < -cap) d = -cap;
+    return fminf(rmax, fmaxf(rmin, fadd(r0, d)));
+}
+
+// backpressure_from_overlap (run.py:454-470), evaluated in double like the
+// reference's host code, from the device max-overlap bits.
+__device__ __forceinline__ float back_global_from_bits(unsigned int bits, double contact_tol) {
+    if (!(contact_tol > 0)) return 1.0f;
+    double om = (double)__uint_as_float(bits);
+    double raw = (contact_tol - om) / contact_tol;
+    return (float)fmax(0.25, fmin(1.0, raw));
+}

@@ -124,6 +124,8 @@ SIGNATURES = {
     "fos_frame_graph": [_P, C.POINTER(FosState), C.POINTER(FosFrameParams), _I, _P],
     "fos_frame_profile": [_P, C.POINTER(FosState), C.POINTER(FosFrameParams), _I,
                           C.POINTER(C.c_float), _P],
+    "fos_frame_trace": [_P, C.POINTER(FosState), C.POINTER(FosFrameParams),
+                        C.POINTER(C.c_longlong), _I, C.POINTER(_I), _P],
     "fos_sim_counters": [_P, C.POINTER(_I), C.POINTER(_I), _P],
     "fos_launch_count": [_P],
     "fos_device_error": [_P, C.POINTER(_I), _P],

@@ -74,6 +74,16 @@ class FoamSim:
         self.frame += 1
         return {k: float(v) for k, v in zip(self.STAGES, ms)} | {"jfa": bool(jfa)}
 
+    def trace_dynamics(self, cap: int = 256) -> list:
+        """ns between the phases of one cooperative plain-frame kernel (block 0's
+        view; the frame counter is not advanced, positions and radii are)."""
+        buf = (C.c_longlong * cap)()
+        cnt = C.c_int()
+        call("fos_frame_trace", self.ctx.h, C.byref(self.state), C.byref(self.fp), buf, cap,
+             C.byref(cnt), stream())
+        t = [buf[i] for i in range(cnt.value)]
+        return [t[i + 1] - t[i] for i in range(len(t) - 1)]
+
     def run(self, frames: int):
         for _ in range(frames):
             self.step()

@@ -253,6 +253,13 @@ int fos_frame_graph(FosCtx* ctx, const FosState* st, const FosFrameParams* fp, i
 #define FOS_FRAME_STAGES 10
 int fos_frame_profile(FosCtx* ctx, const FosState* st, const FosFrameParams* fp, int jfa_frame,
                       float* stage_ms, fos_stream_t s);
+/* Tracing: the dynamics part of a plain frame (the persistent cooperative
+ * kernel) with a %globaltimer stamp, in ns, at kernel entry and after every
+ * grid barrier (block 0's view).  Allocates a scratch buffer and
+ * synchronises; for profiling, not for the frame loop.  *count gets the
+ * number of stamps written (<= cap). */
+int fos_frame_trace(FosCtx* ctx, const FosState* st, const FosFrameParams* fp, long long* ns_host,
+                    int cap, int* count, fos_stream_t s);
 /* Device frame index and settle counter (synchronises). */
 int fos_sim_counters(FosCtx* ctx, int* frame, int* settle, fos_stream_t s);
 

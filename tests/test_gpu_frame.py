@@ -85,3 +85,26 @@ def test_long_run_distributions():
     ks = np.max(np.abs(np.searchsorted(rg, allv, "right") / len(rg)
                        - np.searchsorted(ro, allv, "right") / len(ro)))
     assert ks <= 0.05
+
+
+@pytest.mark.parametrize("name", ["small", "headline"])
+def test_cooperative_frame_matches_stage_kernels(name):
+    """The persistent cooperative frame kernel and the one-kernel-per-stage path
+    (used by the per-stage profiler) give bit-identical frames."""
+    foam = {"small": inputs.small, "headline": inputs.headline}[name]()
+    a = FoamSim.from_foam(foam, use_graph=True)
+    b = FoamSim.from_foam(foam, use_graph=False)
+    a.initialize()
+    b.initialize()
+    for _ in range(6):
+        a.step()
+        b.step_profiled()
+    torch.cuda.synchronize()
+    assert np.array_equal(a.pos.cpu().numpy(), b.pos.cpu().numpy())
+    assert np.array_equal(a.rad.cpu().numpy(), b.rad.cpu().numpy())
+    assert np.array_equal(a.fsc.cpu().numpy(), b.fsc.cpu().numpy())
+    assert np.array_equal(a.cell_indices.cpu().numpy(), b.cell_indices.cpu().numpy())
+    assert np.array_equal(a.cell_start.cpu().numpy(), b.cell_start.cpu().numpy())
+    assert np.array_equal(a.local_max_depth.cpu().numpy(), b.local_max_depth.cpu().numpy())
+    assert a.counters() == b.counters()
+    assert a.ctx.device_error() == 0

@@ -216,10 +216,12 @@ def test_capacity_errors_are_loud():
         ctx.jfa_run(pos.double(), rad, 2)
 
 
-@pytest.mark.parametrize("shift", [0.0, 0.5, 1.75])
+@pytest.mark.parametrize("shift", [0.0, 0.5, 1.75, 3.0e6])
 def test_unwrapped_seed_positions(shift):
     """Seeds given outside [-L/2, L/2) (unwrapped or shifted by whole boxes) use
-    the same jfa.wrapP arithmetic: labels match the oracle bit for bit."""
+    the same jfa.wrapP arithmetic: labels match the oracle bit for bit.  The
+    3e6 shift rounds positions to multiples of 0.25 (many exact distance ties)
+    and takes the conversion-unit rounding path for huge coordinates."""
     rng = np.random.default_rng(21)
     n, R = 400, 32
     pos = (rng.random((n, 3), dtype=np.float32) - np.float32(0.5) + np.float32(shift))
