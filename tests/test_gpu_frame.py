@@ -21,7 +21,7 @@ RTOL = 1e-5
 
 
 def _pair(name, use_graph=True):
-    foam = {"small": inputs.small, "headline": inputs.headline}[name]()
+    foam = {"small": inputs.small, "headline": inputs.headline, "stress": inputs.stress}[name]()
     osim = O.OracleSim(oracle_params(foam), foam.pos, foam.rad)
     osim.initialize()
     gsim = FoamSim.from_foam(foam, use_graph=use_graph)
@@ -35,9 +35,10 @@ def _periodic_maxdiff(a, b):
     return float(np.max(np.abs(d)))
 
 
-@pytest.mark.parametrize("use_graph", [False, True])
-def test_initialisation_and_first_frame_bit_exact(use_graph):
-    foam, osim, gsim = _pair("small", use_graph)
+@pytest.mark.parametrize("name,use_graph", [("small", False), ("small", True),
+                                            ("stress", True)])
+def test_initialisation_and_first_frame_bit_exact(name, use_graph):
+    foam, osim, gsim = _pair(name, use_graph)
     torch.cuda.synchronize()
     assert np.array_equal(gsim.pos.cpu().numpy(), osim.pos)
     osim.step()
@@ -87,11 +88,12 @@ def test_long_run_distributions():
     assert ks <= 0.05
 
 
-@pytest.mark.parametrize("name", ["small", "headline"])
+@pytest.mark.parametrize("name", ["small", "headline", "stress"])
 def test_cooperative_frame_matches_stage_kernels(name):
     """The persistent cooperative frame kernel and the one-kernel-per-stage path
-    (used by the per-stage profiler) give bit-identical frames."""
-    foam = {"small": inputs.small, "headline": inputs.headline}[name]()
+    (used by the per-stage profiler) give bit-identical frames.  The 200k foam
+    (175,616 cells) takes the chunked four-phase grid rebuild."""
+    foam = {"small": inputs.small, "headline": inputs.headline, "stress": inputs.stress}[name]()
     a = FoamSim.from_foam(foam, use_graph=True)
     b = FoamSim.from_foam(foam, use_graph=False)
     a.initialize()

@@ -27,9 +27,9 @@ def _dev(a):
     return torch.as_tensor(np.ascontiguousarray(a)).cuda()
 
 
-@pytest.mark.parametrize("name", ["small", "headline"])
+@pytest.mark.parametrize("name", ["small", "headline", "stress"])
 def test_labels_and_fsc_bit_exact(name):
-    foam = {"small": inputs.small, "headline": inputs.headline}[name]()
+    foam = {"small": inputs.small, "headline": inputs.headline, "stress": inputs.stress}[name]()
     pos = wrapped(foam.pos)
     rad = foam.rad.copy()
     p = oracle_params(foam)
