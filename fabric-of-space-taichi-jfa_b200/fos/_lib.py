@@ -108,6 +108,7 @@ SIGNATURES = {
     "fos_grid_copy_pointers": [_P, _P, _P, _P],
     "fos_grid_scatter": [_P, _P, _P, _P, _I, _P],
     "fos_grid_build": [_P, _P, _I, _P, _P, _P, _P],
+    "fos_grid_build_noalloc": [_P, _I, _I, C.c_double, _P, _P, _P, _P],
     "fos_project_overlaps": [_P, _P, _P, _P, _P, _P, _I, _P],
     "fos_compute_max_overlap": [_P, _P, _P, _P, _P, _P, _P, _I, _P, C.POINTER(_F), _P],
     "fos_equilibrate_pressure": [_P, _I, _I, _P, _P, _P, _P, _F, _F, _F, _I, _F, _F, _I,

@@ -155,6 +155,27 @@ int fos_grid_scatter(FosCtx* ctx, float* pos, int32_t* cell_write, int32_t* cell
 int fos_grid_build(FosCtx* ctx, float* pos, int n, int32_t* cell_count, int32_t* cell_start,
                    int32_t* cell_indices, fos_stream_t s);
 
+/* No counterpart in the reference.  The hash-grid rebuild of fos_grid_build for
+ * callers that cannot allocate device memory at the point where they need the
+ * grid: a host whose own pool or caching allocator owns all device memory, a
+ * frame loop that cannot afford cudaMalloc/cudaFree synchronising the device,
+ * or a C host that holds raw buffers and no context.  It takes no context and
+ * allocates nothing.  The per-particle scratch (cell and arrival rank) lives in
+ * a static device array compiled into the library: 512 KiB on every GPU that
+ * loads it, held until the process exits.  That caps n at
+ * FOS_NOALLOC_MAX_PARTICLES; a larger n returns FOS_E_CAPACITY and launches
+ * nothing.  The first call on each device resolves the array's device address
+ * (cudaGetSymbolAddress), so make that first call before any stream capture.
+ * All calls share the one array: calls that overlap on the GPU (other streams,
+ * other host threads) race and must be serialised.  Outputs equal
+ * fos_grid_build's: cell_count and cell_start [grid_res^3], cell_indices
+ * ascending inside each cell, pos wrapped in place.  grid_res and domain_size
+ * are GRID_RES and DOMAIN_SIZE. */
+#define FOS_NOALLOC_MAX_PARTICLES 65536
+int fos_grid_build_noalloc(float* pos, int n, int grid_res, double domain_size,
+                           int32_t* cell_count, int32_t* cell_start, int32_t* cell_indices,
+                           fos_stream_t s);
+
 /* --------------------------------------------------------------- dynamics.py */
 /* project_overlaps (dynamics.py:77-171) as one Jacobi sweep; pos updated in place. */
 int fos_project_overlaps(FosCtx* ctx, float* pos, const float* rad, const int32_t* cell_start,
