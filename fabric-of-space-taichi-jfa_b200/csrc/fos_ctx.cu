@@ -115,7 +115,7 @@ extern "C" int fos_set_params(FosCtx* c, const FosParams* p) {
     FOS_CUDA(cudaSetDevice(c->device));
     c->p = *p;
     fold_params(c);
-    c->gvalid[0] = c->gvalid[1] = false;
+    for (int k = 0; k < 4; ++k) c->gvalid[k] = false;
     return alloc_cells(c);
 }
 
@@ -232,8 +232,9 @@ extern "C" int fos_ctx_create(const FosParams* p, int max_n, int max_res, int de
 extern "C" int fos_ctx_destroy(FosCtx* c) {
     if (!c) return FOS_OK;
     cudaSetDevice(c->device);
-    for (int k = 0; k < 2; ++k)
+    for (int k = 0; k < 4; ++k)
         if (c->gexec[k]) cudaGraphExecDestroy(c->gexec[k]);
+    fos_sur_free(c);
     void* ptrs[] = {c->labA, c->labB, c->filt, c->seedslot, c->seeds, c->fsc, c->used, c->ema,
                     c->face_ids, c->face_counts, c->nl, c->face_score, c->prev, c->acc0, c->acc1,
                     c->hkeys, c->hmin, c->hcnt, c->claimed, c->rowcnt, c->rowbuf, c->revcnt,
@@ -255,7 +256,7 @@ extern "C" int fos_set_resolution(FosCtx* c, int res) {
     c->vs = (float)(c->p.domain_size / (double)res);      // VOXEL_SIZE = L / JFA_RES
     c->passes = (int)ceil(log2((double)res)) + 1;         // ceil(log2 R) + 1
     if (c->passes > FOS_MAX_PASSES) c->passes = FOS_MAX_PASSES;
-    c->gvalid[0] = c->gvalid[1] = false;
+    for (int k = 0; k < 4; ++k) c->gvalid[k] = false;
     return FOS_OK;
 }
 

@@ -45,10 +45,14 @@ struct FosDevState {
 struct FosGraphKey {
     FosState st;
     FosFrameParams fp;
+    const FosSurrogate* sur;
+    int sur_mode;
     int jfa;
     int res;
     FosParams p;
 };
+
+struct FosSurBufs;  // surrogate.cu
 
 struct FosCtx {
     int device = 0;
@@ -99,11 +103,13 @@ struct FosCtx {
     FosDevState* ds = nullptr;
     int* fin_changed = nullptr;       // [FOS_FIN_MAXIT] per-sweep change flags of the finalize
     void* pinned = nullptr;           // small host staging buffer
-    // graphs
-    cudaGraphExec_t gexec[2] = {nullptr, nullptr};
-    FosGraphKey gkey[2];
-    bool gvalid[2] = {false, false};
-    long long glaunch[2] = {0, 0};    // kernels per captured frame graph
+    FosSurBufs* sur = nullptr;        // FSC surrogate pair/inference buffers (first use)
+    int sur_mode = FOS_SUR_ABSOLUTE;  // how surrogate frames use the model (fos.h)
+    // graphs, indexed by jfa_frame + 2 * (surrogate frame)
+    cudaGraphExec_t gexec[4] = {nullptr, nullptr, nullptr, nullptr};
+    FosGraphKey gkey[4];
+    bool gvalid[4] = {false, false, false, false};
+    long long glaunch[4] = {0, 0, 0, 0};  // kernels per captured frame graph
     long long launches = 0;
 };
 
@@ -142,6 +148,13 @@ int fos_scan_exclusive(FosCtx* ctx, const int32_t* d_in, int32_t* d_out, int n, 
 int fos_jfa_finalize_ema(FosCtx* c, const float* rad, int n, cudaStream_t s);
 int fos_grid_init_attributes();
 bool fos_coop_supported(FosCtx* c);
+void fos_sur_free(FosCtx* c);
+int fos_sur_prepare(FosCtx* c);
+int fos_sur_frame_before_jfa(FosCtx* c, const FosSurrogate* m, const FosState* st,
+                             const FosFrameParams* fp, cudaStream_t s);
+int fos_sur_frame_judge(FosCtx* c, int n, cudaStream_t s);
+int fos_sur_frame_between(FosCtx* c, const FosSurrogate* m, const FosState* st,
+                          const FosFrameParams* fp, cudaStream_t s);
 int fos_frame_coop_dynamics(FosCtx* c, const FosState* st, const FosFrameParams* fp,
                             cudaStream_t s, unsigned long long* trace = nullptr,
                             int trace_cap = 0);

@@ -125,11 +125,19 @@ struct FrameProf {
 };
 
 static int frame_impl(FosCtx* c, const FosState* st, const FosFrameParams* fp, int jfa_frame,
-                      cudaStream_t s, FrameProf* prof);
+                      cudaStream_t s, FrameProf* prof, const FosSurrogate* sur = nullptr);
 
 extern "C" int fos_frame(FosCtx* c, const FosState* st, const FosFrameParams* fp, int jfa_frame,
                          fos_stream_t s) {
     return frame_impl(c, st, fp, jfa_frame, s, nullptr);
+}
+
+extern "C" int fos_frame_surrogate(FosCtx* c, const FosState* st, const FosFrameParams* fp,
+                                   const FosSurrogate* m, int jfa_frame, fos_stream_t s) {
+    FOS_REQUIRE(c != nullptr && m != nullptr, FOS_E_ARG, "ctx or surrogate model is NULL");
+    int rc = fos_sur_prepare(c);
+    if (rc) return rc;
+    return frame_impl(c, st, fp, jfa_frame, s, nullptr, m);
 }
 
 extern "C" int fos_frame_profile(FosCtx* c, const FosState* st, const FosFrameParams* fp,
@@ -155,7 +163,7 @@ extern "C" int fos_frame_profile(FosCtx* c, const FosState* st, const FosFramePa
 }
 
 static int frame_impl(FosCtx* c, const FosState* st, const FosFrameParams* fp, int jfa_frame,
-                      cudaStream_t s, FrameProf* prof) {
+                      cudaStream_t s, FrameProf* prof, const FosSurrogate* sur) {
     int rc = check_state(c, st, fp);
     if (rc) return rc;
     const int n = st->n;
@@ -213,6 +221,16 @@ static int frame_impl(FosCtx* c, const FosState* st, const FosFrameParams* fp, i
         if (rc) return rc;
         MARK(0);
 }
+    // surrogate frames: the learned FSC between JFA runs; on a JFA frame the
+    // surrogate's estimate for the same positions, judged after the JFA
+    if (sur && !jfa_frame) {
+        rc = fos_sur_frame_between(c, sur, st, fp, s);
+        if (rc) return rc;
+    }
+    if (sur && jfa_frame) {
+        rc = fos_sur_frame_before_jfa(c, sur, st, fp, s);
+        if (rc) return rc;
+    }
     // (8) measurement frame: run_jfa, warm-start gate, set_fsc_targets, settle reset
     if (jfa_frame) {
         rc = fos_jfa_init(c, st->pos, st->rad, n, s);
@@ -233,6 +251,10 @@ static int frame_impl(FosCtx* c, const FosState* st, const FosFrameParams* fp, i
                                     (float)fp->r_max, c->ds, fp->warmstart_frames,
                                     fp->zero_rate_thresh, fp->adjustment_frames, s);
         if (rc) return rc;
+        if (sur) {
+            rc = fos_sur_frame_judge(c, n, s);
+            if (rc) return rc;
+        }
     }
     k_frame_end<<<1, 1, 0, s>>>(c->ds);
     FOS_LAUNCHED(c);
@@ -241,15 +263,35 @@ static int frame_impl(FosCtx* c, const FosState* st, const FosFrameParams* fp, i
     return FOS_OK;
 }
 
+static int frame_graph_impl(FosCtx* c, const FosState* st, const FosFrameParams* fp,
+                            const FosSurrogate* sur, int jfa_frame, cudaStream_t s);
+
 extern "C" int fos_frame_graph(FosCtx* c, const FosState* st, const FosFrameParams* fp,
                                int jfa_frame, fos_stream_t s) {
+    return frame_graph_impl(c, st, fp, nullptr, jfa_frame, s);
+}
+
+extern "C" int fos_frame_surrogate_graph(FosCtx* c, const FosState* st, const FosFrameParams* fp,
+                                         const FosSurrogate* m, int jfa_frame, fos_stream_t s) {
+    FOS_REQUIRE(m != nullptr, FOS_E_ARG, "surrogate model is NULL");
+    return frame_graph_impl(c, st, fp, m, jfa_frame, s);
+}
+
+static int frame_graph_impl(FosCtx* c, const FosState* st, const FosFrameParams* fp,
+                            const FosSurrogate* sur, int jfa_frame, cudaStream_t s) {
     int rc = check_state(c, st, fp);
     if (rc) return rc;
-    int g = jfa_frame ? 1 : 0;
+    if (sur) {
+        rc = fos_sur_prepare(c);  // allocation stays outside the capture
+        if (rc) return rc;
+    }
+    int g = (jfa_frame ? 1 : 0) + (sur ? 2 : 0);
     FosGraphKey key;
     memset(&key, 0, sizeof(key));
     key.st = *st;
     key.fp = *fp;
+    key.sur = sur;
+    key.sur_mode = sur ? c->sur_mode : 0;
     key.jfa = g;
     key.res = c->res;
     key.p = c->p;
@@ -266,7 +308,7 @@ extern "C" int fos_frame_graph(FosCtx* c, const FosState* st, const FosFramePara
             cudaStreamDestroy(cap);
             return fos_cuda_fail(e, "cudaStreamBeginCapture", __FILE__, __LINE__);
         }
-        rc = fos_frame(c, st, fp, jfa_frame, cap);
+        rc = frame_impl(c, st, fp, jfa_frame, cap, nullptr, sur);
         cudaGraph_t graph = nullptr;
         e = cudaStreamEndCapture(cap, &graph);
         cudaStreamDestroy(cap);

@@ -79,6 +79,21 @@ class FosState(C.Structure):
         "cell_indices")]
 
 
+class FosSurrogateStats(C.Structure):
+    _fields_ = [("pairs", C.c_int), ("overflow", C.c_int), ("judged", C.c_int),
+                ("exact", C.c_int), ("within1", C.c_int), ("stale_exact", C.c_int),
+                ("stale_within1", C.c_int), ("abs_err", C.c_double),
+                ("stale_abs_err", C.c_double)]
+
+
+SUR_FEATURES = 16
+SUR_HIDDEN = 64
+SUR_BINS = 13
+SUR_PAIR_CAP = 96
+SUR_NPARAM = 64 * 16 + 64 + 64 * 64 + 64 + 64 + 1
+SUR_ABSOLUTE = 0
+SUR_ANCHORED = 1
+
 _P = C.c_void_p
 _I = C.c_int
 _F = C.c_float
@@ -128,6 +143,23 @@ SIGNATURES = {
     "fos_frame_trace": [_P, C.POINTER(FosState), C.POINTER(FosFrameParams),
                         C.POINTER(C.c_longlong), _I, C.POINTER(_I), _P],
     "fos_sim_counters": [_P, C.POINTER(_I), C.POINTER(_I), _P],
+    "fos_surrogate_create": [_I, _F, C.POINTER(_P)],
+    "fos_surrogate_destroy": [_P],
+    "fos_surrogate_set_weights": [_P, _P, _P, _P],
+    "fos_surrogate_get_weights": [_P, _P, _P, _P],
+    "fos_surrogate_cutoff": [_P],
+    "fos_surrogate_train_step": [_P, _P, _P, _P, _I, _F, _P, _P],
+    "fos_surrogate_gradient": [_P, _P, _P, _P, _I, _P, _P, _P],
+    "fos_surrogate_forward": [_P, _P, _I, _P, _P],
+    "fos_surrogate_pairs": [_P, _P, _P, _P, _I, _F, _P, _P, _P, _P],
+    "fos_surrogate_pair_count": [_P, C.POINTER(_I), C.POINTER(_I), _P],
+    "fos_surrogate_export": [_P, _P, _P, _P, _P, _P, _P],
+    "fos_surrogate_predict": [_P, _P, _P, _P, _P, _P, _P],
+    "fos_surrogate_stats": [_P, C.POINTER(FosSurrogateStats), _P],
+    "fos_surrogate_set_mode": [_P, _I],
+    "fos_frame_surrogate": [_P, C.POINTER(FosState), C.POINTER(FosFrameParams), _P, _I, _P],
+    "fos_frame_surrogate_graph": [_P, C.POINTER(FosState), C.POINTER(FosFrameParams), _P, _I,
+                                  _P],
     "fos_launch_count": [_P],
     "fos_device_error": [_P, C.POINTER(_I), _P],
     "fos_status_string": [_I],
@@ -135,7 +167,7 @@ SIGNATURES = {
 }
 _RESTYPES = {"fos_params_default": None, "fos_frame_params_default": None,
              "fos_launch_count": C.c_longlong, "fos_status_string": C.c_char_p,
-             "fos_last_error": C.c_char_p}
+             "fos_last_error": C.c_char_p, "fos_surrogate_cutoff": C.c_float}
 
 _lib = None
 

@@ -21,9 +21,17 @@ from .context import Context, stream
 
 class FoamSim:
     def __init__(self, cfg: FosConfig, pos: np.ndarray, rad: np.ndarray, use_graph: bool = True,
-                 ctx: Context | None = None, device: int | None = None):
+                 ctx: Context | None = None, device: int | None = None, surrogate=None,
+                 policy=None, surrogate_mode: str = "anchored"):
         n = int(rad.shape[0])
         self.cfg = cfg
+        # learned FSC between JFA runs (fos.surrogate); None = the reference's stale reuse
+        self.surrogate = surrogate
+        if surrogate is not None and policy is None:
+            from .surrogate import RefreshPolicy
+            policy = RefreshPolicy(every=2 * cfg.JFA_CADENCE, warm_frames=cfg.JFA_WARM_FRAMES)
+        self.policy = policy
+        self.surrogate_mode = surrogate_mode
         self.n = n
         self.use_graph = use_graph
         self.ctx = ctx or Context(cfg, max_n=n, max_res=cfg.JFA_RES, device=device)
@@ -44,10 +52,15 @@ class FoamSim:
                               self.cell_start.data_ptr(), self.cell_indices.data_ptr())
         self.fp = cfg.frame_params()
         self.frame = 0
+        if surrogate is not None:
+            from .surrogate import set_mode
+            set_mode(self.ctx, surrogate_mode)
 
     @classmethod
-    def from_foam(cls, foam, use_graph: bool = True, **over) -> "FoamSim":
-        return cls(FosConfig.for_foam(foam, **over), foam.pos, foam.rad, use_graph=use_graph)
+    def from_foam(cls, foam, use_graph: bool = True, surrogate=None, policy=None,
+                  surrogate_mode: str = "anchored", **over) -> "FoamSim":
+        return cls(FosConfig.for_foam(foam, **over), foam.pos, foam.rad, use_graph=use_graph,
+                   surrogate=surrogate, policy=policy, surrogate_mode=surrogate_mode)
 
     def initialize(self, frame0: int = 0):
         """initialize_simulation's device part (run.py:320-382)."""
@@ -56,9 +69,35 @@ class FoamSim:
         self.frame = int(frame0)
 
     def step(self):
+        if self.surrogate is not None:
+            return self._step_surrogate()
         jfa = 1 if self.cfg.is_jfa_frame(self.frame) else 0
         fn = "fos_frame_graph" if self.use_graph else "fos_frame"
         call(fn, self.ctx.h, C.byref(self.state), C.byref(self.fp), jfa, stream())
+        self.frame += 1
+        return bool(jfa)
+
+    def _step_surrogate(self):
+        """A frame with the surrogate's FSC between JFA runs.  Every JFA frame
+        (warm start included) also evaluates the surrogate, which sets the
+        anchor of the anchored mode; after the warm start each JFA frame is
+        judged (one host sync to read the counters) and drift forces
+        refreshes.  Non-JFA frames that the policy gives no surrogate update
+        keep the controller's last FSC."""
+        f = self.frame
+        pol = self.policy
+        jfa = pol.is_jfa(f)
+        if jfa or pol.is_surrogate(f):
+            fn = "fos_frame_surrogate_graph" if self.use_graph else "fos_frame_surrogate"
+            call(fn, self.ctx.h, C.byref(self.state), C.byref(self.fp), self.surrogate.h,
+                 int(jfa), stream())
+        else:
+            fn = "fos_frame_graph" if self.use_graph else "fos_frame"
+            call(fn, self.ctx.h, C.byref(self.state), C.byref(self.fp), 0, stream())
+        pol.ran(f, jfa)
+        if jfa and f >= pol.warm_frames:
+            from .surrogate import stats
+            pol.observe(stats(self.ctx) | {"frame": f})
         self.frame += 1
         return bool(jfa)
 

@@ -73,18 +73,18 @@ def stress(seed: int = 2) -> Foam:
 
 
 def surrogate_variant(seed: int = 10, large: bool = False) -> Foam:
-    """Training/eval foams: the small-workload law, or a 50,000-particle variant with
-    radii scaled by (1/5)^(1/3) on a 192^3 grid."""
-    rng = np.random.default_rng(seed)
+    """Foams of the FSC surrogate: the headline workload's law (training uses
+    seeds 10-19), or the 50,000-particle variant whose radii follow the same
+    law scaled by (1/5)^(1/3), on a 192^3 grid."""
     if not large:
-        f = small(seed)
-        return f
+        return headline(seed)
+    rng = np.random.default_rng(seed)
     n = 50000
     s = (1.0 / 5.0) ** (1.0 / 3.0)
     pos = _uniform_pos(rng, n)
-    rad = (rng.uniform(0.025, 0.035, n) * s).astype(np.float32)
-    return Foam("surrogate-50k-192", pos, rad, 192, 0.0125 * s, 0.035 * s, 10, 16, 4, 10,
-                1 << 30, 1, 100, seed)
+    rad = (np.clip(rng.lognormal(np.log(0.015), 0.25, n), 0.007, 0.03) * s).astype(np.float32)
+    return Foam("surrogate-50k-192", pos, rad, 192, 0.007 * s, 0.03 * s, 12, 16, 8, 20, 20, 5,
+                1000, seed)
 
 
 def ensemble(seed: int = 3, count: int = 64) -> list[Foam]:

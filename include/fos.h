@@ -284,6 +284,128 @@ int fos_frame_trace(FosCtx* ctx, const FosState* st, const FosFrameParams* fp, l
 /* Device frame index and settle counter (synchronises). */
 int fos_sim_counters(FosCtx* ctx, int* frame, int* settle, fos_stream_t s);
 
+/* ------------------------------------------------------------ FSC surrogate
+ * No counterpart in the reference: run.py reuses the last JFA's fsc on the
+ * frames between JFA runs (run.py:1230-1261).  A learned per-pair model gives
+ * a fresh FSC estimate on those frames instead.
+ *
+ * Candidate pairs {a, b} have |d| < cutoff * (r_a + r_b) (periodic minimum
+ * image).  Each pair is kept once, by its owner i (the other particle is j):
+ * for a < b the owner is a when a + b is odd and b when it is even, so every
+ * particle owns about half of its pairs whatever its index.  Each pair gets
+ * FOS_SUR_FEATURES FP32 features, with d = x_j - x_i:
+ *   0       |d| / (r_i + r_j)
+ *   1       r_i / r_j
+ *   2       signed offset of the power bisector from the midpoint, over
+ *           r_i + r_j: (r_i^2 - r_j^2) / (2 |d| (r_i + r_j)), evaluated as
+ *           (r_i - r_j) / ((2 * x0) * (r_i + r_j)) (0 when x0 == 0)
+ *   3..15   13-bin histogram (bins of width cutoff/13 in normalised distance)
+ *           of both particles' other candidates, counts summed over i and j.
+ * The model is an MLP 16 -> 64 -> ReLU -> 64 -> ReLU -> 1 -> sigmoid giving
+ * the probability that the pair shares a face.  A particle's FSC estimate is
+ * the sum of its pairs' probabilities.  Inference uses BF16 weights and
+ * activations with FP32 accumulation on the tensor cores; training keeps FP32
+ * master weights and runs Adam.
+ *
+ * FP32 parameter layout (FOS_SUR_NPARAM floats):
+ *   W1[64][16] | b1[64] | W2[64][64] | b2[64] | w3[64] | b3
+ * with W[out][in]. */
+#define FOS_SUR_FEATURES 16
+#define FOS_SUR_HIDDEN 64
+#define FOS_SUR_BINS 13
+#define FOS_SUR_PAIR_CAP 96 /* pairs kept per owner particle */
+#define FOS_SUR_NPARAM (64 * 16 + 64 + 64 * 64 + 64 + 64 + 1)
+
+typedef struct FosSurrogate FosSurrogate;
+
+typedef struct FosSurrogateStats {
+    int pairs;          /* candidate pairs of the last pair build */
+    int overflow;       /* particles that owned more than FOS_SUR_PAIR_CAP pairs */
+    int judged;         /* particles compared on the last judged JFA frame */
+    int exact;          /* ... with rint(surrogate FSC) == JFA fsc */
+    int within1;        /* ... with |rint(surrogate FSC) - JFA fsc| <= 1 */
+    int stale_exact;    /* ... whose previous JFA fsc equals this JFA fsc */
+    int stale_within1;
+    double abs_err;     /* sum over particles of |surrogate FSC - JFA fsc| */
+    double stale_abs_err;
+} FosSurrogateStats;
+
+/* How a surrogate frame turns the model's estimate s_i into the FSC fed to
+ * the controller:
+ *   FOS_SUR_ABSOLUTE  f_i = s_i;
+ *   FOS_SUR_ANCHORED  f_i = max(0, fsc_i(last JFA) + s_i - s_i(last JFA)),
+ *                     the last JFA's exact count moved by the change the
+ *                     model sees since then (its bias cancels).  Until the
+ *                     context has seen one judged JFA frame it behaves as
+ *                     ABSOLUTE. */
+#define FOS_SUR_ABSOLUTE 0
+#define FOS_SUR_ANCHORED 1
+int fos_surrogate_set_mode(FosCtx* ctx, int mode);
+
+/* A model on `device` with candidate cutoff `cutoff` (in units of r_i + r_j).
+ * Weights start at zero; set them with fos_surrogate_set_weights. */
+int fos_surrogate_create(int device, float cutoff, FosSurrogate** out);
+int fos_surrogate_destroy(FosSurrogate* m);
+/* Host arrays: params[FOS_SUR_NPARAM] (layout above), mu/sd[FOS_SUR_FEATURES]
+ * (the features are standardised as (x - mu) / sd before the first layer).
+ * Resets the Adam moments and step. */
+int fos_surrogate_set_weights(FosSurrogate* m, const float* params, const float* mu,
+                              const float* sd);
+int fos_surrogate_get_weights(FosSurrogate* m, float* params, float* mu, float* sd);
+float fos_surrogate_cutoff(const FosSurrogate* m);
+/* One Adam step (beta1 0.9, beta2 0.999, eps 1e-8) on the mean binary cross
+ * entropy of the `batch` rows X[rows[k]] (device arrays: X [*][16] raw
+ * features, y [*] labels in {0,1}, rows [batch], every entry a valid row).
+ * FP32 forward/backward, deterministic.  loss: device float receiving the
+ * batch loss, or NULL. */
+int fos_surrogate_train_step(FosSurrogate* m, const float* X, const float* y, const int32_t* rows,
+                             int batch, float lr, float* loss, fos_stream_t s);
+/* The same forward/backward without the update: grad[FOS_SUR_NPARAM] (device)
+ * receives d(loss)/d(params). */
+int fos_surrogate_gradient(FosSurrogate* m, const float* X, const float* y, const int32_t* rows,
+                           int batch, float* grad, float* loss, fos_stream_t s);
+/* Tensor-core inference on given raw features X [P][16] (device): prob[P]. */
+int fos_surrogate_forward(FosSurrogate* m, const float* X, int P, float* prob, fos_stream_t s);
+
+/* Candidate pairs of the n particles on ctx, found on the hash grid
+ * (cell_start/count/indices of the same positions; the search reach follows
+ * cutoff * (r_i + r_max)).  r_max bounds every radius.  Asynchronous. */
+int fos_surrogate_pairs(FosCtx* ctx, const FosSurrogate* m, const float* pos, const float* rad,
+                        int n, float r_max, const int32_t* cell_start, const int32_t* cell_count,
+                        const int32_t* cell_indices, fos_stream_t s);
+/* Pair count and overflow count of the last pair build (synchronises). */
+int fos_surrogate_pair_count(FosCtx* ctx, int* pairs, int* overflow, fos_stream_t s);
+/* Training export of the last pair build, in pair order (owner i
+ * ascending, then search order): X [P][16] raw features, y [P] = 1 when j is
+ * in i's JFA neighbour list on ctx (the last finalize), pair_i/pair_j [P].
+ * Any output may be NULL.  Asynchronous; size the outputs with
+ * fos_surrogate_pair_count. */
+int fos_surrogate_export(FosCtx* ctx, const float* rad, float* X, float* y, int32_t* pair_i,
+                         int32_t* pair_j, fos_stream_t s);
+/* Inference over the last pair build: fsc_float[n] = sum of pair
+ * probabilities, fsc_int[n] = rint(fsc_float), pair_prob[P] in export order
+ * (each may be NULL).  Without pair_prob: no host sync, graph-capturable. */
+int fos_surrogate_predict(FosCtx* ctx, const FosSurrogate* m, const float* rad, float* fsc_float,
+                          int32_t* fsc_int, float* pair_prob, fos_stream_t s);
+/* Counters of the last pair build and of the last judged JFA frame
+ * (synchronises). */
+int fos_surrogate_stats(FosCtx* ctx, FosSurrogateStats* out, fos_stream_t s);
+/* A frame whose FSC between JFA runs comes from the surrogate.  Plain
+ * dynamics as fos_frame; then
+ *  - non-JFA frame: candidate pairs + inference on the new positions, the
+ *    mode's FSC f (fos_surrogate_set_mode), fsc_ema <- alpha * f +
+ *    (1 - alpha) * fsc_ema (EMA_ALPHA, same first-value rule as
+ *    update_fsc_ema), and set_fsc_targets on rint(f) behind the same
+ *    warm-start gate;
+ *  - JFA frame: the surrogate's f for the same positions, then the exact
+ *    run_jfa + gate + set_fsc_targets, then the judge counters (f vs the JFA
+ *    fsc, and the previous JFA fsc vs this one) and the anchor update.
+ * No host sync; the _graph form replays a captured CUDA graph. */
+int fos_frame_surrogate(FosCtx* ctx, const FosState* st, const FosFrameParams* fp,
+                        const FosSurrogate* m, int jfa_frame, fos_stream_t s);
+int fos_frame_surrogate_graph(FosCtx* ctx, const FosState* st, const FosFrameParams* fp,
+                              const FosSurrogate* m, int jfa_frame, fos_stream_t s);
+
 /* Number of this library's kernel launches issued so far on ctx (host count). */
 long long fos_launch_count(FosCtx* ctx);
 /* Device error word (synchronises) and a static string for a status code. */
