@@ -48,6 +48,9 @@ def parse():
                     help="stage-timing mode for profiling (one small JSON line)")
     ap.add_argument("--reps", type=int, default=5)
     ap.add_argument("--workload", default="headline", choices=["small", "headline", "stress"])
+    ap.add_argument("--no-surrogate", action="store_true",
+                    help="skip the surrogate-FSC arm of the metric")
+    ap.add_argument("--surrogate-mode", default="absolute", choices=["absolute", "anchored"])
     return ap.parse_args()
 
 
@@ -338,6 +341,8 @@ def run_fos(args):
     call("fos_jfa_stats", ctx.h, n, C.c_void_p(sim.rad.data_ptr()), C.byref(st), stream())
     fp32_peak_tflops = 148 * 128 * 1.965e9 / 1e12
 
+    surrogate = None if args.no_surrogate else run_surrogate_arm(args, foam, flush, barrier, world)
+
     if world > 1:
         dist.barrier()
     if rank != 0:
@@ -376,6 +381,7 @@ def run_fos(args):
                               "pass_us": round(pass_s * 1e6, 3),
                               "note": "issue bound (27 candidate evaluations per voxel); "
                                       "labels are L2-resident at 128^3"},
+        "surrogate": surrogate,
         "gpu_launches": int(launches),
         "clocks": clk,
         "cpu_baseline": cpu,
@@ -388,6 +394,81 @@ def run_fos(args):
     if world > 1:
         dist.destroy_process_group()
     return 0
+
+
+def run_surrogate_arm(args, foam, flush, barrier, world):
+    """The metric's second arm: frames/s when the learned FSC surrogate
+    supplies FSC between exact JFA refreshes every 10 frames (the spec's
+    "refresh every 5 or 10 frames"), next to the plain path with JFA every 10
+    frames (the same JFA work with no FSC update between: the surrogate's
+    cost floor).  Both start from the same warm-started foam at frame 20; a
+    step is one 10-frame refresh cycle, L2 flushed between steps; each judged
+    JFA frame reads its counters on the host (one sync per cycle, inside the
+    timed region).  Agreement: per-cell rint(surrogate FSC) == JFA fsc on the
+    refresh frames of the timed region, beside the stale FSC the reference
+    reuses (previous JFA fsc vs this one)."""
+    import time as _time
+    import torch
+    from fos import surrogate as S
+    from fos.driver import FoamSim
+
+    t0 = _time.perf_counter()
+    sur = S.train_default()
+    torch.cuda.synchronize()
+    train_s = _time.perf_counter() - t0
+    cycle = 10
+    s = torch.cuda.current_stream()
+
+    def timed(sim):
+        for _ in range(foam.jfa_warm):
+            sim.step()
+        for _ in range(args.warmup * cycle):
+            sim.step()
+        barrier()
+        if sim.policy is not None:
+            sim.policy.judged.clear()
+        ms = 0.0
+        for _ in range(args.steps):
+            flush.fill_(1.0)
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            e0.record(s)
+            for _ in range(cycle):
+                sim.step()
+            e1.record(s)
+            e1.synchronize()
+            ms += e0.elapsed_time(e1)
+        t = torch.tensor([ms], dtype=torch.float64, device=flush.device)
+        if world > 1:
+            torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+        return world * cycle * args.steps / (float(t.item()) / 1000.0)
+
+    pol = S.RefreshPolicy(every=cycle, warm_frames=foam.jfa_warm)
+    sim = FoamSim.from_foam(foam, surrogate=sur, policy=pol, surrogate_mode=args.surrogate_mode)
+    sim.initialize()
+    fps_sur = timed(sim)
+    judged = list(pol.judged)
+    sim.ctx.close()
+    plain10 = FoamSim.from_foam(foam, JFA_CADENCE=cycle)
+    plain10.initialize()
+    fps_plain10 = timed(plain10)
+    plain10.ctx.close()
+    keys = ("exact_frac", "within1_frac", "mean_abs_err", "stale_exact_frac",
+            "stale_within1_frac", "stale_mean_abs_err")
+    agree = {k: round(sum(d[k] for d in judged) / max(1, len(judged)), 4) for k in keys}
+    return {
+        "value": round(fps_sur, 3), "unit": UNIT,
+        "path": f"surrogate FSC ({args.surrogate_mode}) on every non-JFA frame, exact JFA "
+                f"refresh every {cycle} frames, judged per cell on each refresh",
+        "plain_jfa_every10_value": round(fps_plain10, 3),
+        "judged_frames": len(judged), "agreement": agree,
+        "meets_99pct_agreement": agree["exact_frac"] >= 0.99,
+        "pairs_last": judged[-1]["pairs"] if judged else None,
+        "overflow_last": judged[-1]["overflow"] if judged else None,
+        "train": {"seconds": round(train_s, 2), "foams": "headline law, seeds 10-19",
+                  "frames": "JFA frames 20-200", "rows": "3,000,000 sampled pairs",
+                  "epochs": 30, "lr": 1e-3, "batch": 65536},
+    }
 
 
 def run_profile(args):
