@@ -44,7 +44,7 @@ def parse():
     ap.add_argument("--impl", default="fos", choices=["fos", "reference"])
     ap.add_argument("--cpu-sample-steps", type=int, default=1)
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--profile", default=None, choices=["jfa", "frame"],
+    ap.add_argument("--profile", default=None, choices=["jfa", "frame", "surrogate"],
                     help="stage-timing mode for profiling (one small JSON line)")
     ap.add_argument("--reps", type=int, default=5)
     ap.add_argument("--workload", default="headline", choices=["small", "headline", "stress"])
@@ -512,6 +512,29 @@ def run_profile(args):
         out["stats"] = {k: v for k, v in ctx.jfa_stats(foam.n, rad).items()
                         if k in ("finalize_iterations", "face_pairs", "mean_fsc",
                                  "max_row_candidates")}
+    elif args.profile == "surrogate":
+        # 20 steady-state surrogate frames (2 refresh cycles) between
+        # cudaProfilerStart/Stop, for `ncu --profile-from-start off`
+        from fos import surrogate as S
+        sur = S.train_default(frames=(20, 60, 100), max_rows=1_000_000, epochs=5)
+        sim = FoamSim.from_foam(foam, surrogate=sur, surrogate_mode="absolute",
+                                policy=S.RefreshPolicy(every=10, warm_frames=foam.jfa_warm))
+        sim.initialize()
+        for _ in range(60):
+            sim.step()
+        torch.cuda.synchronize()
+        torch.cuda.cudart().cudaProfilerStart()
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record(s)
+        for _ in range(20):
+            sim.step()
+        b.record(s)
+        b.synchronize()
+        torch.cuda.cudart().cudaProfilerStop()
+        out["ms_per_frame"] = round(a.elapsed_time(b) / 20, 4)
+        out["judged"] = [{k: round(float(d[k]), 4) for k in ("exact_frac", "stale_exact_frac",
+                                                              "pairs")}
+                         for d in sim.policy.judged[-2:]]
     else:
         sim = FoamSim.from_foam(foam, use_graph=True)
         sim.initialize()

@@ -69,7 +69,7 @@ __global__ void k_brownian(float* pos, int n, float strength, float domain, floa
     if (tick && i == 0 && tick->settle > 0) tick->settle -= 1;
     if (i >= n) return;
     unsigned int frame = (unsigned int)(frame_ptr ? *frame_ptr : frame_arg);
-    brownian_one<LdRO>(i, pos, strength, domain, halfL, k0, k1, frame);
+    brownian_one<LdRO>(i, (unsigned int)i, pos, strength, domain, halfL, k0, k1, frame);
 }
 
 // set_fsc_targets (dynamics.py:1242-1320).  With gate != NULL it runs only
@@ -185,7 +185,7 @@ int fos_launch_pressure(FosCtx* c, int n, int frame, const int* frame_ptr, float
         const float* rin = (w & 1) ? c->rad_tmp : rad;
         float* rout = (w & 1) ? rad : c->rad_tmp;
         bool last = (w == sweeps - 1);
-        PressureArgs a{n, frame, max_nei, k, P, cap, rmin, rmax, face_ids, fsc};
+        PressureArgs a{n, frame, max_nei, k, P, cap, rmin, rmax, face_ids, fsc, 0};
         if (max_nei <= 16)
             k_pressure<16><<<fos_blocks(16LL * n, 256), 256, 0, s>>>(
                 a, frame_ptr, rin, rout, delta_r, last ? pmax : nullptr, last ? pch : nullptr);

@@ -1,0 +1,298 @@
+// jfa_body.cuh -- per-voxel / per-slot device bodies of the JFA and FSC
+// stages.  The single-foam kernels (jfa.cu) and the batched-ensemble kernels
+// (ensemble.cu) call the same bodies, so each stage's arithmetic exists once;
+// a body takes its element index instead of reading blockIdx.
+//
+// Reference: jfa.py (VirtualOrganics/Fabric-of-Space-Taichi-JFA).
+#pragma once
+
+#include "fos_internal.cuh"
+
+#define EMPTY_KEY 0xFFFFFFFFFFFFFFFFull
+
+// ---------------------------------------------------------------- jfa_init
+// world_to_voxel (jfa.py:254-270): floor(((p + 0.5L)/L) * R), wrapped.
+__device__ __forceinline__ int world_to_voxel(float p, float halfL, float L, int R) {
+    float nrm = fdiv(fadd(p, halfL), L);
+    int v = (int)floorf(fmul(nrm, (float)R));
+    return wrap_mod(v, R);
+}
+
+// ------------------------------------------------------------ JFA pass
+// True when the reference's early exit (jfa.py:1108-1112) fired after some
+// pass q < p: q >= MIN_JFA_PASSES-1 and changes[q]/V < TH_PASS_DELTA.
+__device__ __forceinline__ bool jfa_exited_before(const FosDevState* ds, int p, double V,
+                                                  int min_passes, double th) {
+    for (int q = min_passes - 1; q < p; ++q)
+        if (q >= 0 && (double)ds->changes[q] / V < th) return true;
+    return false;
+}
+
+// One pass: own label first (1e10 when unassigned), then the 27 offsets in
+// lexicographic (dx, dy, dz) order, dz fastest, each times `step` and wrapped;
+// a candidate replaces the best only on a strictly smaller power distance.
+// A candidate whose label equals the voxel's own label or the label of the
+// previous offset in scan order is skipped: that label's distance has already
+// been compared, so it cannot win again and the result is unchanged.
+//
+// One thread per voxel, z fastest, so each of the 27 label loads of a warp is
+// one coalesced 128-byte row.  All 27 labels are loaded up front; the seed
+// gathers are then issued nine at a time (one dx plane) independently of the
+// running minimum, so a voxel waits for three rounds of gather latency rather
+// than one per evaluated candidate.  A plane no lane of the warp needs is
+// skipped with one vote.
+template <bool UNIT_L>
+__device__ __forceinline__ float jfa_dist(float vx, float vy, float vz, float4 s, float L) {
+    if (!UNIT_L) return power_dist<false>(vx, vy, vz, s, L);
+    return power_dist_unit(vx, vy, vz, s);
+}
+
+template <bool UNIT_L, bool POW2, bool TIE_LOWER>
+__device__ __forceinline__ void jfa_pass_body(const int32_t* __restrict__ in,
+                                              int32_t* __restrict__ out,
+                                              const float4* __restrict__ seeds, int R, int lgR,
+                                              float vs, float halfL, float L, int step,
+                                              unsigned long long* changes, int pass,
+                                              long long lin) {
+    const long long V = (long long)R * R * R;
+    bool live = lin < V;
+    long long l = live ? lin : 0;
+    int x, y, z;
+    if (POW2) {
+        z = (int)(l & (R - 1));
+        y = (int)((l >> lgR) & (R - 1));
+        x = (int)(l >> (2 * lgR));
+    } else {
+        z = (int)(l % R);
+        y = (int)((l / R) % R);
+        x = (int)(l / ((long long)R * R));
+    }
+    int xs[3], ys[3], zs[3];
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+        int o = (k - 1) * step;
+        if (POW2) {
+            xs[k] = ((x + o) & (R - 1)) << (2 * lgR);
+            ys[k] = ((y + o) & (R - 1)) << lgR;
+            zs[k] = (z + o) & (R - 1);
+        } else {
+            xs[k] = wrap_small(x + o, R) * R * R;
+            ys[k] = wrap_small(y + o, R) * R;
+            zs[k] = wrap_small(z + o, R);
+        }
+    }
+    int ids[27];
+#pragma unroll
+    for (int a = 0; a < 3; ++a)
+#pragma unroll
+        for (int b = 0; b < 3; ++b)
+#pragma unroll
+            for (int c = 0; c < 3; ++c) ids[a * 9 + b * 3 + c] = in[xs[a] + ys[b] + zs[c]];
+    int own = live ? ids[13] : -1;  // offset (0,0,0) is the voxel itself
+    float vx = voxel_centre(x, vs, halfL), vy = voxel_centre(y, vs, halfL),
+          vz = voxel_centre(z, vs, halfL);
+    int best = own;
+    float bd = 1e10f;
+    if (own >= 0) bd = jfa_dist<UNIT_L>(vx, vy, vz, __ldg(&seeds[own]), L);
+#pragma unroll
+    for (int g = 0; g < 3; ++g) {
+        bool ok[9];
+        bool any = false;
+#pragma unroll
+        for (int k = 0; k < 9; ++k) {
+            int idx = g * 9 + k;
+            int id = ids[idx];
+            int prv = idx == 0 ? own : ids[idx - 1];
+            ok[k] = live && id >= 0 && id != own && id != prv;
+            any |= ok[k];
+        }
+        if (!__any_sync(0xffffffffu, any)) continue;
+        float4 sv[9];
+#pragma unroll
+        for (int k = 0; k < 9; ++k)
+            sv[k] = ok[k] ? __ldg(&seeds[ids[g * 9 + k]]) : make_float4(0.f, 0.f, 0.f, 0.f);
+#pragma unroll
+        for (int k = 0; k < 9; ++k) {
+            int id = ids[g * 9 + k];
+            float d = jfa_dist<UNIT_L>(vx, vy, vz, sv[k], L);
+            if (ok[k] && (d < bd || (TIE_LOWER && d == bd && id < best))) {
+                bd = d;
+                best = id;
+            }
+        }
+    }
+    int changed = 0;
+    if (live) {
+        out[lin] = best;
+        changed = best != own;
+    }
+    // one atomic per block: same-address atomics from every warp serialise in L2
+    int cnt = __syncthreads_count(changed);
+    if (threadIdx.x == 0 && cnt) atomicAdd(&changes[pass], (unsigned long long)cnt);
+}
+
+// One voxel of the majority filter: lab is the final owner grid of R^3.
+__device__ __forceinline__ void majority_body(const int32_t* __restrict__ lab, int R,
+                                              int32_t* __restrict__ outp, long long lin) {
+    long long V = (long long)R * R * R;
+    if (lin >= V) return;
+    int z = (int)(lin % R), y = (int)((lin / R) % R), x = (int)(lin / ((long long)R * R));
+    int me = lab[lin];
+    if (me < 0) {
+        outp[lin] = -1;
+        return;
+    }
+    int nb[6];
+    nb[0] = lab[((long long)wrap_small(x - 1, R) * R + y) * R + z];
+    nb[1] = lab[((long long)wrap_small(x + 1, R) * R + y) * R + z];
+    nb[2] = lab[((long long)x * R + wrap_small(y - 1, R)) * R + z];
+    nb[3] = lab[((long long)x * R + wrap_small(y + 1, R)) * R + z];
+    nb[4] = lab[((long long)x * R + y) * R + wrap_small(z - 1, R)];
+    nb[5] = lab[((long long)x * R + y) * R + wrap_small(z + 1, R)];
+    int ids[7], cnt[7], nu = 1;
+    ids[0] = me;
+    cnt[0] = 1;
+#pragma unroll
+    for (int k = 0; k < 6; ++k) {
+        int id = nb[k];
+        if (id >= 0) {
+            bool found = false;
+#pragma unroll
+            for (int u = 0; u < 7; ++u)
+                if (!found && u < nu && ids[u] == id) {
+                    cnt[u]++;
+                    found = true;
+                }
+            if (!found) {
+#pragma unroll
+                for (int u = 0; u < 7; ++u)
+                    if (u == nu) {
+                        ids[u] = id;
+                        cnt[u] = 1;
+                    }
+                nu++;
+            }
+        }
+    }
+    int mc = 0, best = me;
+#pragma unroll
+    for (int u = 0; u < 7; ++u)
+        if (u < nu && cnt[u] > mc) {
+            mc = cnt[u];
+            best = ids[u];
+        }
+    outp[lin] = best;
+}
+
+// ------------------------------------------------------------ face pairs
+// murmur3 fmix64 (Austin Appleby, public domain)
+__device__ __forceinline__ unsigned long long fmix64(unsigned long long k) {
+    k ^= k >> 33;
+    k *= 0xff51afd7ed558ccdull;
+    k ^= k >> 33;
+    k *= 0xc4ceb9fe1a85ec53ull;
+    k ^= k >> 33;
+    return k;
+}
+
+__device__ __forceinline__ void pair_insert(unsigned long long pk, unsigned int fk, unsigned int c,
+                                            unsigned long long* keys, unsigned int* hmin,
+                                            unsigned int* hcnt, unsigned int* claimed,
+                                            FosDevState* ds, unsigned long long mask) {
+    unsigned long long h = fmix64(pk) & mask;
+    for (unsigned long long probe = 0; probe <= mask; ++probe) {
+        unsigned long long k = keys[h];
+        bool hit = (k == pk);
+        if (!hit && k == EMPTY_KEY) {
+            unsigned long long prev = atomicCAS(&keys[h], EMPTY_KEY, pk);
+            if (prev == EMPTY_KEY) {
+                int idx = atomicAdd(&ds->pair_count, 1);
+                claimed[idx] = (unsigned int)h;
+                hit = true;
+            } else {
+                hit = (prev == pk);
+            }
+        }
+        if (hit) {
+            atomicMin(&hmin[h], fk);
+            atomicAdd(&hcnt[h], c);
+            return;
+        }
+        h = (h + 1) & mask;
+    }
+    atomicCAS(&ds->error, 0, (int)FOS_E_CAPACITY);
+}
+
+// accumulate_face_area (jfa.py:702-762).  Each geometric voxel face is visited
+// once (the +1 face of every voxel, wrapped).  A face between labels a != b,
+// both in [0, n), belongs to the pair lo = min(a,b), hi = max(a,b); the serial
+// reference visits it from the lower-label voxel, so its first-touch key is
+// (that voxel's linear index)*6 + axis*2 + (dir == +1).  Lanes of a warp that
+// hit the same pair are merged (__match_any_sync) before one atomic update of
+// the pair's count and minimum first-touch key.
+__device__ __forceinline__ void faces_body(const int32_t* __restrict__ filt, int R, int n,
+                                           unsigned long long* keys, unsigned int* hmin,
+                                           unsigned int* hcnt, unsigned int* claimed,
+                                           FosDevState* ds, unsigned long long mask,
+                                           long long lin) {
+    long long V = (long long)R * R * R;
+    bool live = lin < V;
+    int lane = threadIdx.x & 31;
+    int a = live ? filt[lin] : -1;
+    bool va = a >= 0 && a < n;
+    int z = 0, y = 0, x = 0;
+    if (live) {
+        z = (int)(lin % R);
+        y = (int)((lin / R) % R);
+        x = (int)(lin / ((long long)R * R));
+    }
+#pragma unroll
+    for (int ax = 0; ax < 3; ++ax) {
+        long long nlin = 0;
+        if (live) {
+            if (ax == 0) nlin = ((long long)wrap_small(x + 1, R) * R + y) * R + z;
+            else if (ax == 1) nlin = ((long long)x * R + wrap_small(y + 1, R)) * R + z;
+            else nlin = ((long long)x * R + y) * R + wrap_small(z + 1, R);
+        }
+        int b = va ? filt[nlin] : -1;
+        bool valid = va && b >= 0 && b < n && b != a;
+        unsigned long long pk = 0;
+        unsigned int fk = 0;
+        if (valid) {
+            int lo = a < b ? a : b, hi = a < b ? b : a;
+            pk = ((unsigned long long)(unsigned int)lo << 32) | (unsigned int)hi;
+            fk = (a < b) ? (unsigned int)(lin * 6 + ax * 2 + 1) : (unsigned int)(nlin * 6 + ax * 2);
+        }
+        unsigned int m = __ballot_sync(0xffffffffu, valid);
+        if (valid) {
+            unsigned int grp = __match_any_sync(m, pk);
+            unsigned int mn = __reduce_min_sync(grp, fk);
+            if (lane == __ffs(grp) - 1) pair_insert(pk, mn, __popc(grp), keys, hmin, hcnt, claimed, ds, mask);
+        }
+    }
+}
+
+// Per face slot t = a*32 + s: the normalised score of finalize_faces_kernel
+// with expected_area (jfa.py:378-397, 810-830); -1 marks a slot the reference
+// skips (partner outside [0, n), no voxels, or expected <= 0).  Also seeds the
+// acceptance fixed point with "score >= T_ADD" and counts each partner's
+// incoming lower pairs.
+__device__ __forceinline__ void score_slot(long long t, int n, const int32_t* __restrict__ face_ids,
+                                           const int32_t* __restrict__ face_counts,
+                                           const float* __restrict__ rad, float vs, float face_scale,
+                                           float t_add, float* __restrict__ score, uint8_t* acc,
+                                           int32_t* revcnt) {
+    int a = (int)(t >> 5);
+    int j = face_ids[t];
+    int cnt = face_counts[t];
+    float sc = -1.0f;
+    if (j >= 0 && j < n && cnt > 0) {
+        float rm = fmul(0.5f, fadd(rad[a], rad[j]));
+        float q = fdiv(fmul(2.0f, rm), vs);
+        float expected = fmul(face_scale, fmul(q, q));
+        if (expected > 0.0f) sc = fdiv((float)cnt, expected);
+    }
+    score[t] = sc;
+    acc[t] = (sc >= 0.0f && sc >= t_add) ? 1 : 0;
+    if (sc >= 0.0f) atomicAdd(&revcnt[j], 1);
+}

@@ -226,6 +226,7 @@ struct PressureArgs {
     float k, P, cap, rmin, rmax;
     const int32_t* face_ids;
     const int32_t* fsc;
+    int hoff;  // particle i hashes as i - hoff (its index within its own foam)
 };
 
 // equilibrate_pressure (dynamics.py:1454-1557) for particle i, one Jacobi
@@ -245,7 +246,7 @@ __device__ __forceinline__ float pressure_group(int i, int lane, const PressureA
     float d = 0.f;
     if (fc > 0) {
         int an = fc < a.max_nei ? fc : a.max_nei;
-        int st = hash_func(i, a.frame) % fc;
+        int st = hash_func(i - a.hoff, a.frame) % fc;
         float Vi = powf(ri, a.P);
         float invP = fdiv(1.0f, a.P);
         for (int base = 0; base < an; base += GS) {
@@ -281,13 +282,14 @@ __device__ __forceinline__ float pressure_group(int i, int lane, const PressureA
 }
 
 // apply_brownian_motion (dynamics.py:1596-1634) for particle i.  ti.random()
-// is replaced by Philox-4x32-10 with counter (i, frame, 'BROW', 0) and key =
-// seed; each axis draws u = (x >> 8) * 2^-24.
+// is replaced by Philox-4x32-10 with counter (ctr, frame, 'BROW', 0) and key =
+// seed, ctr being i's index within its own foam; each axis draws
+// u = (x >> 8) * 2^-24.
 template <class LD>
-__device__ __forceinline__ void brownian_one(int i, float* pos, float strength, float domain,
-                                             float halfL, uint32_t k0, uint32_t k1,
+__device__ __forceinline__ void brownian_one(int i, unsigned int ctr, float* pos, float strength,
+                                             float domain, float halfL, uint32_t k0, uint32_t k1,
                                              unsigned int frame) {
-    uint4 r = philox4x32_10(make_uint4((unsigned int)i, frame, 0x42524f57u, 0u), k0, k1);
+    uint4 r = philox4x32_10(make_uint4(ctr, frame, 0x42524f57u, 0u), k0, k1);
     unsigned int rr[3] = {r.x, r.y, r.z};
 #pragma unroll
     for (int d = 0; d < 3; ++d) {

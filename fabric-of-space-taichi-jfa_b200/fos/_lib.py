@@ -86,6 +86,23 @@ class FosSurrogateStats(C.Structure):
                 ("stale_abs_err", C.c_double)]
 
 
+class FosEnsembleFoam(C.Structure):
+    _fields_ = [("n", C.c_int), ("jfa_res", C.c_int), ("grid_res", C.c_int), ("f_low", C.c_int),
+                ("f_high", C.c_int), ("r_min", C.c_double), ("r_max", C.c_double),
+                ("seed", C.c_uint64)]
+
+
+class FosEnsembleTuning(C.Structure):
+    _fields_ = [("pass_block", C.c_int), ("voxel_block", C.c_int), ("coop_threads", C.c_int),
+                ("coop_blocks_per_sm", C.c_int)]
+
+
+class FosEnsembleView(C.Structure):
+    _fields_ = [("nfoams", C.c_int), ("n_total", C.c_int)] + [(k, C.c_void_p) for k in (
+        "pos", "rad", "rad_target", "local_max_depth", "delta_r", "fsc", "fsc_ema", "face_ids",
+        "face_counts", "neighbor_list", "labels_a", "labels_b", "foam_of")]
+
+
 SUR_FEATURES = 16
 SUR_HIDDEN = 64
 SUR_BINS = 13
@@ -160,6 +177,19 @@ SIGNATURES = {
     "fos_frame_surrogate": [_P, C.POINTER(FosState), C.POINTER(FosFrameParams), _P, _I, _P],
     "fos_frame_surrogate_graph": [_P, C.POINTER(FosState), C.POINTER(FosFrameParams), _P, _I,
                                   _P],
+    "fos_ensemble_create": [C.POINTER(FosParams), C.POINTER(FosFrameParams),
+                            C.POINTER(FosEnsembleFoam), _I, _I, C.POINTER(_P)],
+    "fos_ensemble_destroy": [_P],
+    "fos_ensemble_view": [_P, C.POINTER(FosEnsembleView)],
+    "fos_ensemble_offsets": [_P, _P, _P, _P],
+    "fos_ensemble_init": [_P, _I, _P],
+    "fos_ensemble_frame": [_P, _I, _P],
+    "fos_ensemble_frame_graph": [_P, _I, _P],
+    "fos_ensemble_set_tuning": [_P, C.POINTER(FosEnsembleTuning)],
+    "fos_ensemble_get_tuning": [_P, C.POINTER(FosEnsembleTuning)],
+    "fos_ensemble_autotune": [_P, _I, C.POINTER(FosEnsembleTuning), _P, _I, _P],
+    "fos_ensemble_frame_index": [_P, C.POINTER(_I), _P],
+    "fos_ensemble_launch_count": [_P],
     "fos_launch_count": [_P],
     "fos_device_error": [_P, C.POINTER(_I), _P],
     "fos_status_string": [_I],
@@ -167,7 +197,8 @@ SIGNATURES = {
 }
 _RESTYPES = {"fos_params_default": None, "fos_frame_params_default": None,
              "fos_launch_count": C.c_longlong, "fos_status_string": C.c_char_p,
-             "fos_last_error": C.c_char_p, "fos_surrogate_cutoff": C.c_float}
+             "fos_last_error": C.c_char_p, "fos_surrogate_cutoff": C.c_float,
+             "fos_ensemble_launch_count": C.c_longlong}
 
 _lib = None
 

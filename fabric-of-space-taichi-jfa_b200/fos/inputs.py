@@ -87,23 +87,35 @@ def surrogate_variant(seed: int = 10, large: bool = False) -> Foam:
                 1000, seed)
 
 
-def ensemble(seed: int = 3, count: int = 64) -> list[Foam]:
-    """64 independent foams, N ~ U{2000..20000}, lognormal r with median
-    0.03*(1000/N)^(1/3) and sigma_log 0.25, R = smallest of {64, 96, 128} with
-    R^3/N >= 100, band low ~ U{10..14}, high = low + 4."""
+ENSEMBLE_RES = (64, 96, 128)
+
+
+def ensemble_member(n: int, seed: int, band_low: int = 12, name: str = "ensemble") -> Foam:
+    """One foam of the batched ensemble: uniform positions, lognormal radii with
+    median 0.03*(1000/N)^(1/3) and sigma_log 0.25 (clipped to [0.4, 2] x median),
+    JFA_RES the smallest of 64/96/128 with R^3/N >= 100, band [low, low + 4],
+    K=8 PBD and M=20 pressure sweeps, 20 warm-start frames then JFA every 5th."""
+    rng = np.random.default_rng(seed)
+    med = 0.03 * (1000.0 / n) ** (1.0 / 3.0)
+    pos = _uniform_pos(rng, n)
+    rad = rng.lognormal(np.log(med), 0.25, n)
+    lo_clip, hi_clip = 0.4 * med, 2.0 * med
+    rad = np.clip(rad, lo_clip, hi_clip).astype(np.float32)
+    res = next((r for r in ENSEMBLE_RES if r ** 3 / n >= 100), ENSEMBLE_RES[-1])
+    return Foam(name, pos, rad, res, lo_clip, hi_clip, band_low, band_low + 4, 8, 20, 20, 5, 500,
+                seed)
+
+
+def ensemble(seed: int = 3, count: int = 64, n_range=(2000, 20000)) -> list[Foam]:
+    """The batched-ensemble workload: `count` independent foams with N drawn
+    uniformly from n_range (seed 3), per-foam band low ~ U{10..14}; each foam
+    is ensemble_member(N, seed * 1000 + k, low)."""
     rng = np.random.default_rng(seed)
     out = []
     for k in range(count):
-        n = int(rng.integers(2000, 20001))
-        med = 0.03 * (1000.0 / n) ** (1.0 / 3.0)
-        pos = _uniform_pos(rng, n)
-        rad = rng.lognormal(np.log(med), 0.25, n)
-        lo_clip, hi_clip = 0.4 * med, 2.0 * med
-        rad = np.clip(rad, lo_clip, hi_clip).astype(np.float32)
-        res = next((r for r in (64, 96, 128) if r ** 3 / n >= 100), 128)
+        n = int(rng.integers(n_range[0], n_range[1] + 1))
         low = int(rng.integers(10, 15))
-        out.append(Foam(f"ensemble-{k}", pos, rad, res, lo_clip, hi_clip, low, low + 4, 8, 20,
-                        20, 5, 500, seed))
+        out.append(ensemble_member(n, seed * 1000 + k, low, name=f"ensemble-{k}"))
     return out
 
 

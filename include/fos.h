@@ -406,6 +406,94 @@ int fos_frame_surrogate(FosCtx* ctx, const FosState* st, const FosFrameParams* f
 int fos_frame_surrogate_graph(FosCtx* ctx, const FosState* st, const FosFrameParams* fp,
                               const FosSurrogate* m, int jfa_frame, fos_stream_t s);
 
+/* ------------------------------------------------------- batched ensembles
+ * No counterpart in the reference, which runs one foam per process.  Many
+ * independent periodic foams, of uneven particle counts, JFA resolutions and
+ * hash grids, advance together.  All foams share one device frame index and
+ * take their JFA frames together, and every stage of a frame is ONE launch
+ * over all foams:
+ *   - the dynamics are one persistent cooperative kernel;
+ *   - the JFA passes, filter and face extraction are one launch per stage;
+ *   - the finalize is one cooperative kernel.
+ * Each foam's result is bit-identical to the same foam run alone through
+ * fos_frame with the same parameters.
+ *
+ * Layout: the foams' particles are packed (foam f owns the global indices
+ * [part_off[f], part_off[f+1]) in the order given).  JFA labels, face_ids and
+ * neighbor_list hold GLOBAL particle indices; subtract part_off[f] for a
+ * foam's own numbering.  Every foam's voxel grid starts at a multiple of 1024
+ * voxels in the packed label arrays, and every foam's hash grid at its own
+ * offset in the packed cell table.
+ *
+ * Limits: one domain_size for all foams; early_exit must be 0 (every foam runs
+ * all its passes); max_eq_nei <= 16. */
+typedef struct FosEnsembleFoam {
+    int n;              /* particles */
+    int jfa_res;        /* JFA_RES of this foam */
+    int grid_res;       /* GRID_RES (hash cells per axis) of this foam */
+    int f_low, f_high;  /* FSC band */
+    double r_min, r_max;
+    uint64_t seed;      /* Philox key of its Brownian jitter */
+} FosEnsembleFoam;
+
+/* Launch shapes the autotuner chooses between (results do not depend on them). */
+typedef struct FosEnsembleTuning {
+    int pass_block;          /* threads per block of the JFA pass: 128, 256 or 512 */
+    int voxel_block;         /* majority filter / face extraction: 128, 256 or 512 */
+    int coop_threads;        /* dynamics kernel threads per block: 512 or 1024 */
+    int coop_blocks_per_sm;  /* dynamics kernel blocks per SM: 1 or 2 (if resident) */
+} FosEnsembleTuning;
+
+/* Device pointers of the packed state (n_total particles). */
+typedef struct FosEnsembleView {
+    int nfoams, n_total;
+    float* pos;                /* [n_total][3] */
+    float* rad;                /* [n_total] */
+    float* rad_target;
+    float* local_max_depth;
+    float* delta_r;
+    int32_t* fsc;              /* [n_total] */
+    float* fsc_ema;            /* [n_total] */
+    int32_t* face_ids;         /* [n_total][32], global indices */
+    int32_t* face_counts;      /* [n_total][32] */
+    int32_t* neighbor_list;    /* [n_total][32], global indices */
+    int32_t* labels_a;         /* packed owner grids (pass buffers A and B) */
+    int32_t* labels_b;
+    const int32_t* foam_of;    /* [n_total] foam of each particle */
+} FosEnsembleView;
+
+typedef struct FosEnsemble FosEnsemble;
+
+/* p and fp hold the parameters all foams share (their per-foam fields --
+ * grid_res, f_low/f_high, r_min/r_max, seed -- are taken from foams[]). */
+int fos_ensemble_create(const FosParams* p, const FosFrameParams* fp,
+                        const FosEnsembleFoam* foams, int nfoams, int device, FosEnsemble** out);
+int fos_ensemble_destroy(FosEnsemble* e);
+int fos_ensemble_view(FosEnsemble* e, FosEnsembleView* out);
+/* Host arrays of nfoams + 1 entries: particle, voxel and hash-cell offsets. */
+int fos_ensemble_offsets(FosEnsemble* e, int* part_off, long long* vox_off, int* cell_off);
+/* fos_sim_init for every foam: zeroed fields, rad_target = rad, positions
+ * wrapped, warmup_pbd PBD passes (one cooperative launch), frame index frame0. */
+int fos_ensemble_init(FosEnsemble* e, int frame0, fos_stream_t s);
+/* One frame of every foam (fos_frame's order); jfa_frame for all foams. */
+int fos_ensemble_frame(FosEnsemble* e, int jfa_frame, fos_stream_t s);
+/* The same frame replayed from a CUDA graph (one per frame kind and tuning). */
+int fos_ensemble_frame_graph(FosEnsemble* e, int jfa_frame, fos_stream_t s);
+int fos_ensemble_set_tuning(FosEnsemble* e, const FosEnsembleTuning* t);
+int fos_ensemble_get_tuning(FosEnsemble* e, FosEnsembleTuning* t);
+/* Times every candidate shape of each tuned stage on the current state (the
+ * JFA stages on this state's positions, the dynamics from a snapshot that is
+ * restored afterwards), keeps the fastest per stage and applies it.
+ * report_ms (optional, report_cap entries) receives, per candidate, the
+ * stage's mean milliseconds in the order: pass_block 128/256/512,
+ * voxel_block 128/256/512, coop (threads, blocks/SM) (512,1) (512,2)
+ * (1024,1) (1024,2), a non-resident shape reporting -1.  Synchronises. */
+int fos_ensemble_autotune(FosEnsemble* e, int reps, FosEnsembleTuning* best, float* report_ms,
+                          int report_cap, fos_stream_t s);
+/* Frame index (synchronises). */
+int fos_ensemble_frame_index(FosEnsemble* e, int* frame, fos_stream_t s);
+long long fos_ensemble_launch_count(FosEnsemble* e);
+
 /* Number of this library's kernel launches issued so far on ctx (host count). */
 long long fos_launch_count(FosCtx* ctx);
 /* Device error word (synchronises) and a static string for a status code. */
