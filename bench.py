@@ -44,13 +44,16 @@ def parse():
     ap.add_argument("--impl", default="fos", choices=["fos", "reference"])
     ap.add_argument("--cpu-sample-steps", type=int, default=1)
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--profile", default=None, choices=["jfa", "frame", "surrogate"],
+    ap.add_argument("--profile", default=None, choices=["jfa", "frame", "surrogate", "ensemble"],
                     help="stage-timing mode for profiling (one small JSON line)")
     ap.add_argument("--reps", type=int, default=5)
     ap.add_argument("--workload", default="headline", choices=["small", "headline", "stress"])
     ap.add_argument("--no-surrogate", action="store_true",
                     help="skip the surrogate-FSC arm of the metric")
     ap.add_argument("--surrogate-mode", default="absolute", choices=["absolute", "anchored"])
+    ap.add_argument("--no-ensemble", action="store_true",
+                    help="skip the batched-ensemble measurement")
+    ap.add_argument("--ensemble-frames", type=int, default=500)
     return ap.parse_args()
 
 
@@ -342,6 +345,7 @@ def run_fos(args):
     fp32_peak_tflops = 148 * 128 * 1.965e9 / 1e12
 
     surrogate = None if args.no_surrogate else run_surrogate_arm(args, foam, flush, barrier, world)
+    ensemble = None if args.no_ensemble else run_ensemble(args, barrier, world, rank)
 
     if world > 1:
         dist.barrier()
@@ -382,12 +386,14 @@ def run_fos(args):
                               "note": "issue bound (27 candidate evaluations per voxel); "
                                       "labels are L2-resident at 128^3"},
         "surrogate": surrogate,
+        "ensemble": ensemble,
         "gpu_launches": int(launches),
         "clocks": clk,
         "cpu_baseline": cpu,
         "diagnostics": {"launches_before_timed": int(launches0 + torch_kernels_before),
                         "finalize_iterations": st.finalize_iterations,
                         "face_pairs": st.face_pairs, "mean_fsc": round(st.mean_fsc, 3),
+                        "voxel_passes_per_s": round(V * passes * value / FRAMES_PER_STEP, 1),
                         "fp32_peak_tflops_nominal": round(fp32_peak_tflops, 2)},
     }
     print(json.dumps(line), flush=True)
@@ -471,6 +477,105 @@ def run_surrogate_arm(args, foam, flush, barrier, world):
     }
 
 
+def run_ensemble(args, barrier, world, rank):
+    """Batched ensemble: the 64 foams of the ensemble workload (N ~ U[2k, 20k],
+    seed 3; 64^3 / 96^3 / 128^3 grids; per-foam bands), split over the ranks by
+    fos.ensemble.partition, advanced --ensemble-frames frames from the end of
+    their 20-frame warm start, once with the fixed launch shapes and once with
+    the autotuned ones (each from the same warm state).  value = foam-frames/s
+    over all ranks (max time over ranks).  Beside it, the same foams run one
+    after another through their single-foam frame graphs for 25 frames."""
+    import time as _time
+    import torch
+    from fos import inputs
+    from fos.driver import FoamSim
+    from fos.ensemble import FIXED, Ensemble, partition
+
+    foams_all = inputs.ensemble()
+    mine = partition(foams_all, world)[rank]
+    foams = [foams_all[k] for k in mine]
+    frames = args.ensemble_frames
+    s = torch.cuda.current_stream()
+    dev = torch.cuda.current_device()
+
+    def max_over_ranks(ms):
+        t = torch.tensor([ms], dtype=torch.float64, device=dev)
+        if world > 1:
+            torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+        return float(t.item())
+
+    def timed_run(ens, n):
+        barrier()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(s)
+        ens.run(n)
+        e1.record(s)
+        e1.synchronize()
+        return max_over_ranks(e0.elapsed_time(e1))
+
+    out = {"foams": len(foams_all), "particles": int(sum(f.n for f in foams_all)),
+           "jfa_res": {str(r): sum(f.res == r for f in foams_all) for r in (64, 96, 128)},
+           "frames": frames, "unit": "foam-frames/s",
+           "split": "foams partitioned over ranks (LPT greedy on N + R^3/450), no collective "
+                    "inside a frame"}
+    t0 = _time.perf_counter()
+    ens = Ensemble(foams)
+    ens.initialize()
+    ens.run(20)
+    torch.cuda.synchronize()
+    out["setup_s"] = round(_time.perf_counter() - t0, 2)
+    l0 = ens.launch_count()
+    ens.run(5)  # one cadence cycle, graphs captured
+    torch.cuda.synchronize()
+    out["launches_per_5_frames"] = ens.launch_count() - l0
+    snap = [t.clone() for t in (ens.pos, ens.rad, ens.rad_target)]
+    frame0 = ens.frame
+    ens.tuning = FIXED
+    ms_fixed = timed_run(ens, frames)
+    # the tuned run starts from a fresh ensemble at the same warm state
+    ens.close()
+    ens = Ensemble(foams)
+    ens.initialize()
+    ens.run(25)
+    torch.cuda.synchronize()
+    same_start = all(torch.equal(a, b) for a, b in zip(snap, (ens.pos, ens.rad, ens.rad_target)))
+    t0 = _time.perf_counter()
+    tuning, report = ens.autotune(reps=3)
+    tune_s = _time.perf_counter() - t0
+    assert ens.frame == frame0
+    ms_tuned = timed_run(ens, frames)
+    ens.close()
+    nfoam = len(foams_all)
+    out["fixed"] = {"tuning": FIXED, "ms_per_frame": round(ms_fixed / frames, 4),
+                    "value": round(nfoam * frames / (ms_fixed / 1000.0), 2)}
+    out["tuned"] = {"tuning": tuning, "ms_per_frame": round(ms_tuned / frames, 4),
+                    "value": round(nfoam * frames / (ms_tuned / 1000.0), 2),
+                    "autotune_s": round(tune_s, 2), "candidates_ms": report}
+    out["same_start_state"] = same_start
+    out["value"] = max(out["fixed"]["value"], out["tuned"]["value"])
+    # unbatched: every foam through its own single-foam frame graph
+    sims = [FoamSim.from_foam(f) for f in foams]
+    for sm in sims:
+        sm.initialize()
+    for _ in range(25):
+        for sm in sims:
+            sm.step()
+    barrier()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(s)
+    for _ in range(25):
+        for sm in sims:
+            sm.step()
+    e1.record(s)
+    e1.synchronize()
+    ms_seq = max_over_ranks(e0.elapsed_time(e1))
+    for sm in sims:
+        sm.ctx.close()
+    out["sequential_single_foam"] = {"frames": 25, "ms_per_frame": round(ms_seq / 25, 4),
+                                     "value": round(nfoam * 25 / (ms_seq / 1000.0), 2)}
+    return out
+
+
 def run_profile(args):
     """Stage timings of one workload with CUDA events (used under ncu as well)."""
     import numpy as np
@@ -512,6 +617,24 @@ def run_profile(args):
         out["stats"] = {k: v for k, v in ctx.jfa_stats(foam.n, rad).items()
                         if k in ("finalize_iterations", "face_pairs", "mean_fsc",
                                  "max_row_candidates")}
+    elif args.profile == "ensemble":
+        # one 5-frame cadence cycle of the 64-foam ensemble between
+        # cudaProfilerStart/Stop, for `ncu --profile-from-start off`
+        from fos.ensemble import Ensemble
+        ens = Ensemble(inputs.ensemble())
+        ens.initialize()
+        ens.run(25)
+        torch.cuda.synchronize()
+        torch.cuda.cudart().cudaProfilerStart()
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record(s)
+        ens.run(5)
+        b.record(s)
+        b.synchronize()
+        torch.cuda.cudart().cudaProfilerStop()
+        out["ms_per_frame"] = round(a.elapsed_time(b) / 5, 4)
+        out["workload"] = "ensemble-64"
+        ens.close()
     elif args.profile == "surrogate":
         # 20 steady-state surrogate frames (2 refresh cycles) between
         # cudaProfilerStart/Stop, for `ncu --profile-from-start off`
