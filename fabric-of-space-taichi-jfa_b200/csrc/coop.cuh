@@ -62,41 +62,150 @@ __device__ __forceinline__ int coop_block_scan(int v, int* total) {
     return base + x - v;
 }
 
-// Rebuild of the hash grid from src into dst (wrapped), with the cell-ordered
-// copy sp[k] = (pos, rad) when rad != NULL.  Ends with a grid barrier unless
-// last.  Returns false if a barrier timed out.
-//
-// Small cell tables (G3 <= COOP_SMALL_G3): three phases -- histogram + ranks;
-// every block scans the whole table into its shared memory (block 0 also
-// writes cell_count/cell_start) and scatters ranks; stable placement from the
-// block's own copy of the starts.  Large tables: the chunked four-phase form.
+#define COOP_CAP 32  // slots per cell of the fixed-capacity rows (one warp sorts a row)
+
+// One rebuild's grid as its consumers (max overlap, PBD) see it.  Both forms
+// hold each cell's particles in ascending index order, so a stencil walk
+// visits candidates in the reference's order either way; slot_of[i] (an
+// argument array) is particle i's slot in whichever form was built.
+struct CoopLayout {
+    const int32_t* ci;  // particle at slot k
+    const float4* sp;   // (pos, rad) at slot k
+    const int32_t* cs;  // CSR form: first slot of each cell
+    const int32_t* cc;  // particles per cell
+    int cap;            // fixed-capacity form (> 0): cell c's slots start at c * cap
+    __device__ __forceinline__ int start(int c) const { return cap ? c * cap : __ldcg(&cs[c]); }
+    __device__ __forceinline__ int count(int c) const { return __ldcg(&cc[c]); }
+};
+
+// P1 of a rebuild for one particle whose source position is v: wrap v into
+// dst[i], find its cell, take an arrival rank in the count buffer `par`
+// (all-zero before the first arrival) and drop the particle into slot rank
+// of the cell's fixed-capacity row (a full row sets overflow bit par, and
+// the rebuild then takes the CSR form).  A phase that produces particle i's
+// new position can run this for the next rebuild right away, so that rebuild
+// needs no P1 phase or barrier of its own.
+template <class Args, class Geo>
+__device__ __forceinline__ void coop_p1_val(const Args& a, const Geo& geo, int i, float3 v,
+                                            float* dst, int par) {
+    float wx = grid_wrap(v.x, geo.L, geo.invL);
+    float wy = grid_wrap(v.y, geo.L, geo.invL);
+    float wz = grid_wrap(v.z, geo.L, geo.invL);
+    dst[3 * i + 0] = wx;
+    dst[3 * i + 1] = wy;
+    dst[3 * i + 2] = wz;
+    int c = geo.cell(i, wx, wy, wz);
+    a.cellof[i] = c;
+    int r = atomicAdd(&(par ? a.cnt2 : a.cnt)[c], 1);
+    a.rank[i] = r;
+    if (a.cfix) {
+        if (r < COOP_CAP) a.cfix[(size_t)c * COOP_CAP + r] = i;
+        else atomicOr(&a.ds->grid_ovf, 1 << par);
+    }
+}
+
+template <class Args, class Geo>
+__device__ __forceinline__ void coop_p1_one(const Args& a, const Geo& geo, int i, const float* src,
+                                            float* dst, int par) {
+    float3 v = make_float3(__ldcg(&src[3 * i + 0]), __ldcg(&src[3 * i + 1]),
+                           __ldcg(&src[3 * i + 2]));
+    coop_p1_val(a, geo, i, v, dst, par);
+}
+
+// Deferred P1 for a warp's PBD results: the warp's q-th particle goes to
+// lane q % 32 by shuffle, and the lanes run coop_p1_val together every 32
+// particles, so the cell atomics of a warp's particles cost one round trip,
+// not one per particle.
+struct P1Defer {
+    int i = -1;
+    float3 v;
+    int q = 0;
+    template <class Args, class Geo>
+    __device__ __forceinline__ void put(const Args& a, const Geo& geo, int lane, int pi, float3 pv,
+                                        float* dst, int par) {
+        const int slot = q & 31;
+        const int si = __shfl_sync(0xffffffffu, pi, 0);
+        const float sx = __shfl_sync(0xffffffffu, pv.x, 0);
+        const float sy = __shfl_sync(0xffffffffu, pv.y, 0);
+        const float sz = __shfl_sync(0xffffffffu, pv.z, 0);
+        if (lane == slot) {
+            i = si;
+            v = make_float3(sx, sy, sz);
+        }
+        ++q;
+        if (slot == 31) flush(a, geo, dst, par);
+    }
+    template <class Args, class Geo>
+    __device__ __forceinline__ void flush(const Args& a, const Geo& geo, float* dst, int par) {
+        if (i >= 0) coop_p1_val(a, geo, i, v, dst, par);
+        i = -1;
+    }
+};
+
+// Rebuild of the hash grid from src into dst (wrapped) with count buffer
+// `par` (rebuilds alternate buffers, so the next rebuild's P1 can run while
+// this grid is still being read).  Ends with a grid barrier unless last;
+// returns false if a barrier timed out; *out receives the layout.
+//   P1        histogram + arrival rank + fixed-capacity row slot (skipped
+//             when p1_done: the previous phase ran coop_p1_* for every
+//             particle with the same src, dst and par);
+//   fixed     when the rows did not overflow, want_csr is false and rad is
+//             given: one phase, one warp per cell sorts its row by particle
+//             index and writes the (pos, rad) copy;
+//   CSR       otherwise (the user-visible final rebuild always): small tables
+//             (G3 <= COOP_SMALL_G3) scan the whole table in every block's
+//             shared memory (block 0 writes cell_count/cell_start) and scatter
+//             ranks, then place stably; large tables use a chunked four-phase
+//             form.  CSR ci/sp/cc/cs are written.
+// The second phase also clears the other count buffer and overflow bit for
+// the rebuild after this one.
 template <class Args, class Geo>
 __device__ bool coop_grid(const Args& a, const Geo& geo, const float* src, float* dst,
-                          const float* rad, bool last, int& tk, unsigned int& ep) {
+                          const float* rad, bool last, int& tk, unsigned int& ep, bool p1_done,
+                          int par, bool want_csr, CoopLayout* out) {
     extern __shared__ int s_tab[];  // small form: G3 + 1 exclusive starts
     const int T = gridDim.x * blockDim.x;
     const int tid = blockIdx.x * blockDim.x + threadIdx.x;
-    // P1: histogram + arrival rank (cnt is all-zero on entry)
-    for (int i = tid; i < a.n; i += T) {
-        float wx = grid_wrap(__ldcg(&src[3 * i + 0]), geo.L, geo.invL);
-        float wy = grid_wrap(__ldcg(&src[3 * i + 1]), geo.L, geo.invL);
-        float wz = grid_wrap(__ldcg(&src[3 * i + 2]), geo.L, geo.invL);
-        dst[3 * i + 0] = wx;
-        dst[3 * i + 1] = wy;
-        dst[3 * i + 2] = wz;
-        int c = geo.cell(i, wx, wy, wz);
-        a.cellof[i] = c;
-        a.rank[i] = atomicAdd(&a.cnt[c], 1);
+    int32_t* cnt = par ? a.cnt2 : a.cnt;
+    int32_t* cnt_next = par ? a.cnt : a.cnt2;
+    if (!p1_done) {
+        for (int i = tid; i < a.n; i += T) coop_p1_one(a, geo, i, src, dst, par);
+        if (!grid_barrier(a.ds, ep)) return false;
+        trace_mark(a, tk);
     }
-    if (!grid_barrier(a.ds, ep)) return false;
-    trace_mark(a, tk);
+    const bool ovf = ((*((volatile int*)&a.ds->grid_ovf)) >> par) & 1;
+    for (int c = tid; c < a.G3; c += T) cnt_next[c] = 0;
+    if (tid == 0) atomicAnd(&a.ds->grid_ovf, ~(1 << (par ^ 1)));
+    if (a.cfix && !want_csr && !ovf && rad) {
+        // fixed-capacity rows: sort each cell's (<= COOP_CAP) arrivals by index
+        const int lane = threadIdx.x & 31, W = T >> 5, wid = tid >> 5;
+        for (int c = wid; c < a.G3; c += W) {
+            const int m = __ldcg(&cnt[c]);  // warp-uniform, <= COOP_CAP
+            if (m == 0) continue;
+            const size_t base = (size_t)c * COOP_CAP;
+            const int id = lane < m ? __ldcg(&a.cfix[base + lane]) : 0x7fffffff;
+            int r = 0;
+            for (int k = 0; k < m; ++k) r += __shfl_sync(0xffffffffu, id, k) < id;
+            if (lane < m) {
+                a.idsort[base + r] = id;
+                a.spfix[base + r] = make_float4(__ldcg(&dst[3 * id + 0]), __ldcg(&dst[3 * id + 1]),
+                                                __ldcg(&dst[3 * id + 2]), __ldcg(&rad[id]));
+                a.slot_of[id] = (int)(base + r);
+            }
+        }
+        if (out) *out = CoopLayout{a.idsort, a.spfix, nullptr, cnt, COOP_CAP};
+        if (!last && !grid_barrier(a.ds, ep)) return false;
+        trace_mark(a, tk);
+        return true;
+    }
+    if (out) *out = CoopLayout{a.ci, a.sp, a.cs, a.cc, 0};
     if (a.small_grid) {
         // P2: whole-table scan per block, then the rank scatter
         const int per = (a.G3 + blockDim.x - 1) / blockDim.x;
         const int b0 = threadIdx.x * per, b1 = min(a.G3, b0 + per);
         int sum = 0;
         for (int c = b0; c < b1; ++c) {
-            int v = __ldcg(&a.cnt[c]);
+            int v = __ldcg(&cnt[c]);
             s_tab[c] = v;
             sum += v;
         }
@@ -118,15 +227,13 @@ __device__ bool coop_grid(const Args& a, const Geo& geo, const float* src, float
         if (!grid_barrier(a.ds, ep)) return false;
         trace_mark(a, tk);
         // P3: stable placement from the block's copy of the starts
-        int c0 = blockIdx.x * a.chunk;
-        for (int c = c0 + threadIdx.x; c < c0 + a.chunk && c < a.G3; c += blockDim.x)
-            a.cnt[c] = 0;  // ready for the next rebuild; nobody reads cnt in this phase
         for (int i = tid; i < a.n; i += T) {
             int c = __ldcg(&a.cellof[i]);
             int b = s_tab[c], e = s_tab[c + 1];
             int r = 0;
             for (int k = b; k < e; ++k) r += __ldcg(&a.ci_tmp[k]) < i;
             a.ci[b + r] = i;
+            a.slot_of[i] = b + r;
             if (rad)
                 a.sp[b + r] = make_float4(__ldcg(&dst[3 * i + 0]), __ldcg(&dst[3 * i + 1]),
                                           __ldcg(&dst[3 * i + 2]), __ldcg(&rad[i]));
@@ -142,7 +249,7 @@ __device__ bool coop_grid(const Args& a, const Geo& geo, const float* src, float
         for (int base = c0; base < c0 + a.chunk; base += blockDim.x) {
             int c = base + threadIdx.x;
             bool in = c < c0 + a.chunk && c < a.G3;
-            int v = in ? __ldcg(&a.cnt[c]) : 0;
+            int v = in ? __ldcg(&cnt[c]) : 0;
             int tot;
             int ex = coop_block_scan(v, &tot);
             if (in) {
@@ -166,7 +273,6 @@ __device__ bool coop_grid(const Args& a, const Geo& geo, const float* src, float
         int c0 = blockIdx.x * a.chunk;
         for (int c = c0 + threadIdx.x; c < c0 + a.chunk && c < a.G3; c += blockDim.x) {
             a.cs[c] = __ldcg(&a.part[c]) + s_pre[blockIdx.x];
-            a.cnt[c] = 0;  // ready for the next rebuild; nobody reads cnt in this phase
         }
         for (int i = tid; i < a.n; i += T) {
             int c = __ldcg(&a.cellof[i]);
@@ -183,6 +289,7 @@ __device__ bool coop_grid(const Args& a, const Geo& geo, const float* src, float
         int r = 0;
         for (int k = b; k < e; ++k) r += __ldcg(&a.ci_tmp[k]) < i;
         a.ci[b + r] = i;
+        a.slot_of[i] = b + r;
         if (rad) {
             a.sp[b + r] = make_float4(__ldcg(&dst[3 * i + 0]), __ldcg(&dst[3 * i + 1]),
                                       __ldcg(&dst[3 * i + 2]), __ldcg(&rad[i]));

@@ -275,6 +275,11 @@ struct EnsArgs {
     int32_t* rank;
     int32_t* ci_tmp;
     int32_t* cnt;
+    int32_t* cnt2;
+    int32_t* cfix;
+    int32_t* idsort;
+    float4* spfix;
+    int32_t* slot_of;
     int32_t* part;
     int32_t* bsum;
     float4* sp;
@@ -300,18 +305,29 @@ struct EnsArgs {
     float strength, domain, L, invL, halfL;
 };
 
-// One PBD sweep over every particle of every foam (sorted positions), into pos_tmp.
-__device__ __forceinline__ void ens_pbd(const EnsArgs& a, int wid, int W_, int lane) {
+// One PBD sweep over every particle of every foam on layout `lay`, into
+// pos_tmp; with p1, each new position also enters the histogram of the next
+// rebuild (count buffer par), wrapped into pos.
+__device__ __forceinline__ void ens_pbd(const EnsArgs& a, const EnsGeo& geo, const CoopLayout& lay,
+                                        int wid, int W_, int lane, bool p1, int par) {
     const int rounds = (a.n + W_ - 1) / W_;
+    P1Defer d1;
+    int kk_next = wid < a.n ? __ldcg(&a.slot_of[wid]) : 0;
     for (int r = 0; r < rounds; ++r) {
-        int kk = r * W_ + wid;
-        if (kk < a.n) {
-            const EnsFoamDev& d = a.F[a.foam_of[__ldcg(&a.ci[kk])]];
+        const int i = r * W_ + wid;
+        const int kk = kk_next;
+        kk_next = i + W_ < a.n ? __ldcg(&a.slot_of[i + W_]) : 0;
+        if (i < a.n) {  // warp-uniform
+            const EnsFoamDev& d = a.F[a.foam_of[i]];
             const GridGeom g{d.G, a.L, a.invL, a.halfL};
-            pbd_warp<LdL2>(kk, lane, a.sp, a.ci, a.pos_tmp, g, a.cs + d.cell_off,
-                           a.cc + d.cell_off, a.gap1, a.mdf, a.dmul);
+            float3 nv = make_float3(0.f, 0.f, 0.f);
+            int pi = pbd_warp<LdL2>(kk, lane, lay.sp, lay.ci, a.pos_tmp, g,
+                                    lay.cs ? lay.cs + d.cell_off : nullptr, lay.cc + d.cell_off,
+                                    a.gap1, a.mdf, a.dmul, &nv, lay.cap, d.cell_off);
+            if (p1) d1.put(a, geo, lane, pi, nv, a.pos, par);
         }
     }
+    if (p1) d1.flush(a, geo, a.pos, par);
 }
 
 template <int THREADS>
@@ -324,11 +340,15 @@ __global__ void __launch_bounds__(THREADS) k_ens_coop(EnsArgs a) {
     const EnsGeo geo{a.F, a.foam_of, a.L, a.invL, a.halfL};
     int tk = 0;
     unsigned int ep = 0;
+    CoopLayout lay;
+    int gk = 0;  // rebuild gk uses count buffer gk & 1
     if (a.mode == 1) {
         // warmup_pbd of initialize_simulation (run.py:293-318): grid + PBD + copy-back
         for (int k = 0; k < a.warmup; ++k) {
-            if (!coop_grid(a, geo, a.pos, a.pos, a.rad, false, tk, ep)) return;
-            ens_pbd(a, wid, W_, lane);
+            if (!coop_grid(a, geo, a.pos, a.pos, a.rad, false, tk, ep, false, gk & 1, false, &lay))
+                return;
+            ++gk;
+            ens_pbd(a, geo, lay, wid, W_, lane, false, 0);
             if (!grid_barrier(a.ds, ep)) return;
             for (int i = tid; i < 3 * a.n; i += T) a.pos[i] = __ldcg(&a.pos_tmp[i]);
             if (!grid_barrier(a.ds, ep)) return;
@@ -336,18 +356,24 @@ __global__ void __launch_bounds__(THREADS) k_ens_coop(EnsArgs a) {
         return;
     }
     // (1) rebuild_grid
-    if (!coop_grid(a, geo, a.pos, a.pos, a.rad, false, tk, ep)) return;
+    if (!coop_grid(a, geo, a.pos, a.pos, a.rad, false, tk, ep, false, gk & 1, false, &lay)) return;
+    ++gk;
     // (2) compute_max_overlap: per-foam maxima
     {
         const int rounds = (a.n + W_ - 1) / W_;
+        int kk_next = wid < a.n ? __ldcg(&a.slot_of[wid]) : 0;
         for (int r = 0; r < rounds; ++r) {
-            int kk = r * W_ + wid;
-            if (kk < a.n) {
-                const int f = a.foam_of[__ldcg(&a.ci[kk])];
+            const int i = r * W_ + wid;
+            const int kk = kk_next;
+            kk_next = i + W_ < a.n ? __ldcg(&a.slot_of[i + W_]) : 0;
+            if (i < a.n) {
+                const int f = a.foam_of[i];
                 const EnsFoamDev& d = a.F[f];
                 const GridGeom g{d.G, a.L, a.invL, a.halfL};
-                unsigned int b = maxov_warp<LdL2>(kk, lane, a.sp, a.ci, g, a.cs + d.cell_off,
-                                                  a.cc + d.cell_off, a.eps, a.lmd);
+                unsigned int b = maxov_warp<LdL2>(kk, lane, lay.sp, lay.ci, g,
+                                                  lay.cs ? lay.cs + d.cell_off : nullptr,
+                                                  lay.cc + d.cell_off, a.eps, a.lmd, lay.cap,
+                                                  d.cell_off);
                 if (lane == 0 && b > __ldcg(&a.W[f].omax_bits)) atomicMax(&a.W[f].omax_bits, b);
             }
         }
@@ -369,13 +395,13 @@ __global__ void __launch_bounds__(THREADS) k_ens_coop(EnsArgs a) {
     // (4) pressure sweeps with each foam's bounds and local hash index
     const int frame = *((volatile int*)&a.ds->frame);
     {
-        const int groups_per_round = T / 16;
+        const int groups_per_round = T / 8;
         const int p_rounds = (a.n + groups_per_round - 1) / groups_per_round;
         for (int w = 0; w < a.sweeps; ++w) {
             const float* rin = (w & 1) ? a.rad_tmp : a.rad;
             float* rout = (w & 1) ? a.rad : a.rad_tmp;
             for (int r = 0; r < p_rounds; ++r) {
-                int i = r * groups_per_round + tid / 16;
+                int i = r * groups_per_round + tid / 8;
                 PressureArgs pa = a.pa;
                 pa.frame = frame;
                 if (i < a.n) {
@@ -384,7 +410,7 @@ __global__ void __launch_bounds__(THREADS) k_ens_coop(EnsArgs a) {
                     pa.rmax = d.r_max;
                     pa.hoff = d.part_off;
                 }
-                pressure_group<16, LdL2>(i, lane, pa, rin, rout, a.delta_r);
+                pressure_group8x2<LdL2>(i, lane, pa, rin, rout, a.delta_r);
             }
             if (!grid_barrier(a.ds, ep)) return;
         }
@@ -395,6 +421,7 @@ __global__ void __launch_bounds__(THREADS) k_ens_coop(EnsArgs a) {
         const EnsFoamDev& d = a.F[a.foam_of[i]];
         brownian_one<LdL2>(i, (unsigned int)(i - d.part_off), a.pos, a.strength, a.domain, a.halfL,
                            d.k0, d.k1, (unsigned int)frame);
+        coop_p1_one(a, geo, i, a.pos, a.pos, gk & 1);
     }
     for (int f = tid; f < a.nf; f += T)
         if (a.W[f].settle > 0) a.W[f].settle -= 1;
@@ -402,18 +429,20 @@ __global__ void __launch_bounds__(THREADS) k_ens_coop(EnsArgs a) {
     // (6) PBD sweeps, each on a fresh grid; (7) final rebuild
     const float* src = a.pos;
     for (int k = 0; k < a.pbd_iters; ++k) {
-        if (!coop_grid(a, geo, src, a.pos, a.rad, false, tk, ep)) return;
-        ens_pbd(a, wid, W_, lane);
+        if (!coop_grid(a, geo, src, a.pos, a.rad, false, tk, ep, true, gk & 1, false, &lay)) return;
+        ++gk;
+        ens_pbd(a, geo, lay, wid, W_, lane, true, gk & 1);
         if (!grid_barrier(a.ds, ep)) return;
         src = a.pos_tmp;
     }
-    coop_grid(a, geo, src, a.pos, nullptr, true, tk, ep);
+    coop_grid(a, geo, src, a.pos, nullptr, true, tk, ep, true, gk & 1, true, nullptr);
 }
 
 __global__ void k_ens_coop_prep(FosDevState* ds, EnsWords* W, int nf) {
     int f = blockIdx.x * blockDim.x + threadIdx.x;
     if (f < nf) W[f].omax_bits = 0u;
     if (f == 0) {
+        ds->grid_ovf = 0;
         ds->bar_count = 0u;
         ds->omax_bits = 0u;
         ds->maxabs_dr_bits = 0u;
@@ -668,6 +697,11 @@ static int ens_coop_launch(FosEnsemble* e, int mode, cudaStream_t s) {
     a.rank = c->rank;
     a.ci_tmp = c->ci_tmp;
     a.cnt = c->coop_cnt;
+    a.cnt2 = c->coop_cnt2;
+    a.cfix = c->coop_fixed ? c->coop_cfix : nullptr;
+    a.idsort = c->coop_idsort;
+    a.spfix = c->coop_spfix;
+    a.slot_of = c->coop_slot;
     a.part = c->coop_part;
     a.bsum = c->coop_bsum;
     a.sp = c->sorted;

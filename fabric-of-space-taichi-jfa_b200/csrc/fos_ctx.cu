@@ -86,16 +86,34 @@ static void fold_params(FosCtx* c) {
     c->G = p.grid_res;
 }
 
+// Fixed-capacity cell rows of the cooperative rebuilds (32 slots a cell) are
+// allocated while they stay below this size; larger grids use the CSR form.
+#define FOS_COOP_FIXED_MAX_BYTES (1ull << 31)
+
 static int alloc_cells(FosCtx* c) {
     size_t need = (size_t)c->G * c->G * c->G;
     if (need <= c->cell_tmp_n) return FOS_OK;
-    int32_t** bufs[3] = {&c->cell_tmp, &c->coop_cnt, &c->coop_part};
+    int32_t** bufs[4] = {&c->cell_tmp, &c->coop_cnt, &c->coop_part, &c->coop_cnt2};
     for (int32_t** b : bufs) {
         if (*b) cudaFree(*b);
         *b = nullptr;
     }
+    void* rows[3] = {c->coop_cfix, c->coop_idsort, c->coop_spfix};
+    for (void* q : rows)
+        if (q) cudaFree(q);
+    c->coop_cfix = c->coop_idsort = nullptr;
+    c->coop_spfix = nullptr;
+    c->coop_fixed = 0;
     for (int32_t** b : bufs) FOS_CUDA(cudaMalloc((void**)b, need * sizeof(int32_t)));
     FOS_CUDA(cudaMemset(c->coop_cnt, 0, need * sizeof(int32_t)));
+    FOS_CUDA(cudaMemset(c->coop_cnt2, 0, need * sizeof(int32_t)));
+    const size_t slots = need * 32;
+    if (slots * (4 + 4 + sizeof(float4)) <= FOS_COOP_FIXED_MAX_BYTES) {
+        FOS_CUDA(cudaMalloc((void**)&c->coop_cfix, slots * 4));
+        FOS_CUDA(cudaMalloc((void**)&c->coop_idsort, slots * 4));
+        FOS_CUDA(cudaMalloc((void**)&c->coop_spfix, slots * sizeof(float4)));
+        c->coop_fixed = 1;
+    }
     c->cell_tmp_n = need;
     return FOS_OK;
 }
@@ -185,6 +203,7 @@ extern "C" int fos_ctx_create(const FosParams* p, int max_n, int max_res, int de
     ALLOC(c->rad_tmp, (size_t)max_n * 4);
     ALLOC(c->cellof, (size_t)max_n * 4);
     ALLOC(c->rank, (size_t)max_n * 4);
+    ALLOC(c->coop_slot, (size_t)max_n * 4);
     ALLOC(c->stats_f, 64 * 4);
     ALLOC(c->stats_i, 64 * 4);
     ALLOC(c->ds, sizeof(FosDevState));
@@ -241,7 +260,8 @@ extern "C" int fos_ctx_destroy(FosCtx* c) {
                     c->revstart, c->revfill, c->rev, c->scan_tmp, c->pos_tmp, c->rad_tmp,
                     c->cellof, c->rank, c->cell_tmp, c->stats_f, c->stats_i, c->ds,
                     c->fin_changed, c->sorted, c->ci_tmp, c->coop_bsum, c->coop_cnt,
-                    c->coop_part};
+                    c->coop_part, c->coop_cnt2, c->coop_cfix, c->coop_idsort, c->coop_spfix,
+                    c->coop_slot};
     for (void* q : ptrs)
         if (q) cudaFree(q);
     if (c->pinned) cudaFreeHost(c->pinned);

@@ -39,6 +39,7 @@ struct FosDevState {
     unsigned int omax_bits;       // max overlap depth (float bits)
     unsigned int bar_count;       // grid barrier arrival counter
     unsigned int bar_gen;         // grid barrier generation
+    int grid_ovf;                 // bit p: a fixed-capacity cell row of count buffer p overflowed
     unsigned long long changes[FOS_MAX_PASSES];
 };
 
@@ -93,6 +94,11 @@ struct FosCtx {
     int32_t *cellof = nullptr, *rank = nullptr;   // [max_n]
     int32_t* cell_tmp = nullptr;      // [G^3]  (scatter's copy of cell_write)
     int32_t *coop_cnt = nullptr, *coop_part = nullptr;  // [G^3] cooperative rebuild scratch
+    int32_t* coop_cnt2 = nullptr;     // [G^3] second count buffer (rebuilds alternate)
+    int32_t *coop_cfix = nullptr, *coop_idsort = nullptr;  // [G^3 * COOP_CAP] cell rows
+    float4* coop_spfix = nullptr;     // [G^3 * COOP_CAP] (pos, rad) by cell row
+    int coop_fixed = 0;               // the fixed-capacity rows are allocated
+    int32_t* coop_slot = nullptr;     // [max_n] slot of each particle in the last rebuild
     int32_t* coop_bsum = nullptr;     // [1024]
     int32_t* ci_tmp = nullptr;        // [max_n]
     int use_coop = 1;                 // plain-frame dynamics as one cooperative kernel
@@ -272,12 +278,16 @@ __device__ __forceinline__ bool grid_barrier(FosDevState* ds, unsigned int& epoc
         long long t0 = clock64();
         unsigned int polls = 0;
         while (ld_acquire_gpu(&ds->bar_count) < target) {
-            if (*((volatile int*)&ds->error) != 0 || clock64() - t0 > FOS_BAR_CYCLE_LIMIT) {
-                atomicCAS(&ds->error, 0, (int)FOS_E_TIMEOUT);
-                ok = false;
-                break;
+            // the error word and the clock are checked every 32 polls, so a
+            // poll is one L2 round trip and the release is seen sooner
+            if ((++polls & 31u) == 0u) {
+                if (*((volatile int*)&ds->error) != 0 || clock64() - t0 > FOS_BAR_CYCLE_LIMIT) {
+                    atomicCAS(&ds->error, 0, (int)FOS_E_TIMEOUT);
+                    ok = false;
+                    break;
+                }
+                if (polls > 2048u) __nanosleep(32);
             }
-            if (++polls > 2048) __nanosleep(32);
         }
         s_ok = ok ? 1 : 0;
     }

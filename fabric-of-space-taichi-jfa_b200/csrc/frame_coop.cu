@@ -10,11 +10,11 @@
 // barriers; each phase calls the same per-element device functions as the
 // standalone kernels (phases.cuh), so the results are identical.
 //
-// Grid rebuild inside the kernel (grid.py:145-309 / run.py:476-504), four
-// phases: histogram with per-particle arrival rank; per-block scan of its
-// chunk of cells; global offsets + rank scatter into a scratch list; stable
-// placement (each particle's slot = cell start + number of lower-indexed
-// particles in its cell) and the cell-ordered (pos, rad) copy.
+// Grid rebuilds inside the kernel (grid.py:145-309 / run.py:476-504): see
+// coop_grid (coop.cuh).  The rebuilds the frame's own stages read use
+// fixed-capacity cell rows (one phase after the histogram, which itself runs
+// inside the phase that produced the positions); the final rebuild, whose
+// cell arrays the caller sees, is the CSR form.
 #include <string.h>
 
 #include "coop.cuh"
@@ -36,6 +36,11 @@ struct CoopArgs {
     int32_t* rank;
     int32_t* ci_tmp;
     int32_t* cnt;
+    int32_t* cnt2;
+    int32_t* cfix;
+    int32_t* idsort;
+    float4* spfix;
+    int32_t* slot_of;
     int32_t* part;
     int32_t* bsum;
     float4* sp;
@@ -62,15 +67,28 @@ __global__ void __launch_bounds__(COOP_THREADS) k_frame_coop(CoopArgs a) {
     unsigned int ep = 0;
     trace_mark(a, tk);
 
-    // (1) rebuild_grid (run.py:704)
+    // (1) rebuild_grid (run.py:704); rebuild gk uses count buffer gk & 1
     const UniGeo geo{a.g.G, a.g.L, a.g.invL, a.g.halfL};
-    if (!coop_grid(a, geo, a.pos, a.pos, a.rad, false, tk, ep)) return;
-    // (2) compute_max_overlap (run.py:709)
-    for (int r = 0; r < warp_rounds; ++r) {
-        int kk = r * W + wid;
-        unsigned int b = 0u;
-        if (kk < a.n) b = maxov_warp<LdL2>(kk, lane, a.sp, a.ci, a.g, a.cs, a.cc, a.eps, a.lmd);
-        block_max_atomic(b, &a.ds->omax_bits);
+    CoopLayout lay;
+    int gk = 0;
+    if (!coop_grid(a, geo, a.pos, a.pos, a.rad, false, tk, ep, false, gk & 1, false, &lay)) return;
+    ++gk;
+    // (2) compute_max_overlap (run.py:709): particle i's slot comes from
+    // slot_of, prefetched one round ahead
+    {
+        unsigned int wmax = 0u;
+        int kk_next = wid < a.n ? __ldcg(&a.slot_of[wid]) : 0;
+        for (int r = 0; r < warp_rounds; ++r) {
+            const int i = r * W + wid;
+            const int kk = kk_next;
+            kk_next = i + W < a.n ? __ldcg(&a.slot_of[i + W]) : 0;
+            if (i < a.n) {
+                unsigned int b = maxov_warp<LdL2>(kk, lane, lay.sp, lay.ci, a.g, lay.cs, lay.cc,
+                                                  a.eps, a.lmd, lay.cap);
+                wmax = b > wmax ? b : wmax;
+            }
+        }
+        block_max_atomic(wmax, &a.ds->omax_bits);
     }
     if (!grid_barrier(a.ds, ep)) return;
     trace_mark(a, tk);
@@ -88,18 +106,24 @@ __global__ void __launch_bounds__(COOP_THREADS) k_frame_coop(CoopArgs a) {
     // (4) pressure sweeps (run.py:755-771); the last sweep reports its stats
     PressureArgs pa = a.pa;
     pa.frame = *((volatile int*)&a.ds->frame);
-    const int groups_per_round = T / 16;
+    // 8-lane groups, two neighbours per lane: every particle in one round
+    const int groups_per_round = T / 8;
     const int p_rounds = (a.n + groups_per_round - 1) / groups_per_round;
+    // with one round (n <= T/8) each lane keeps its neighbours in registers
+    // for all sweeps: a sweep then waits for one round of radius loads
+    const bool keep_nbr = p_rounds == 1;
+    const PressureNbr nb0 = pressure_nbr8x2<LdL2>(tid / 8, lane, pa);
     for (int w = 0; w < a.sweeps; ++w) {
         const float* rin = (w & 1) ? a.rad_tmp : a.rad;
         float* rout = (w & 1) ? a.rad : a.rad_tmp;
         bool last = (w == a.sweeps - 1);
         for (int r = 0; r < p_rounds; ++r) {
-            int i = r * groups_per_round + tid / 16;
-            float d = pressure_group<16, LdL2>(i, lane, pa, rin, rout, a.delta_r);
+            int i = r * groups_per_round + tid / 8;
+            float d = keep_nbr ? pressure_sweep8x2<LdL2>(i, lane, pa, nb0, rin, rout, a.delta_r)
+                               : pressure_group8x2<LdL2>(i, lane, pa, rin, rout, a.delta_r);
             if (last) {
                 float ad = fabsf(d);
-                int ch = (i < a.n && (lane & 15) == 0) && ad > 1e-12f;
+                int ch = (i < a.n && (lane & 7) == 0) && ad > 1e-12f;
                 int cnt = __syncthreads_count(ch);
                 unsigned int bm = __reduce_max_sync(0xffffffffu, ch ? __float_as_uint(ad) : 0u);
                 block_max_atomic(bm, &a.ds->maxabs_dr_bits);
@@ -110,36 +134,51 @@ __global__ void __launch_bounds__(COOP_THREADS) k_frame_coop(CoopArgs a) {
         trace_mark(a, tk);
     }
     // (5) apply_brownian_motion (run.py:807-813); the odd-sweep result is copied
-    // back into rad, and settle_frames_left -= 1 (run.py:750)
+    // back into rad, and settle_frames_left -= 1 (run.py:750).  Each new
+    // position enters the next rebuild's histogram right away (its P1).
     {
         unsigned int frame = (unsigned int)pa.frame;
         for (int i = tid; i < a.n; i += T) {
             if (a.sweeps & 1) a.rad[i] = __ldcg(&a.rad_tmp[i]);
             brownian_one<LdL2>(i, (unsigned int)i, a.pos, a.strength, a.domain, a.halfL, a.k0,
                                a.k1, frame);
+            coop_p1_one(a, geo, i, a.pos, a.pos, gk & 1);
         }
         if (tid == 0 && a.ds->settle > 0) a.ds->settle -= 1;
     }
     if (!grid_barrier(a.ds, ep)) return;
     trace_mark(a, tk);
     // (6) PBD passes, each on a fresh grid (run.py:829-846); (7) rebuild (run.py:874)
+    // Every rebuild here has its P1 done by the phase that produced the
+    // positions (Brownian, then each PBD sweep's lane 0).
     const float* src = a.pos;
     for (int k = 0; k < a.pbd_iters; ++k) {
-        if (!coop_grid(a, geo, src, a.pos, a.rad, false, tk, ep)) return;
+        if (!coop_grid(a, geo, src, a.pos, a.rad, false, tk, ep, true, gk & 1, false, &lay))
+            return;
+        ++gk;
+        P1Defer p1;
+        int kk_next = wid < a.n ? __ldcg(&a.slot_of[wid]) : 0;
         for (int r = 0; r < warp_rounds; ++r) {
-            int kk = r * W + wid;
-            if (kk < a.n)
-                pbd_warp<LdL2>(kk, lane, a.sp, a.ci, a.pos_tmp, a.g, a.cs, a.cc, a.gap1, a.mdf,
-                               a.dmul);
+            const int i = r * W + wid;
+            const int kk = kk_next;
+            kk_next = i + W < a.n ? __ldcg(&a.slot_of[i + W]) : 0;
+            if (i < a.n) {  // warp-uniform
+                float3 nv = make_float3(0.f, 0.f, 0.f);
+                int pi = pbd_warp<LdL2>(kk, lane, lay.sp, lay.ci, a.pos_tmp, a.g, lay.cs, lay.cc,
+                                        a.gap1, a.mdf, a.dmul, &nv, lay.cap);
+                p1.put(a, geo, lane, pi, nv, a.pos, gk & 1);
+            }
         }
+        p1.flush(a, geo, a.pos, gk & 1);
         if (!grid_barrier(a.ds, ep)) return;
         trace_mark(a, tk);
         src = a.pos_tmp;
     }
-    coop_grid(a, geo, src, a.pos, nullptr, true, tk, ep);
+    coop_grid(a, geo, src, a.pos, nullptr, true, tk, ep, true, gk & 1, true, nullptr);
 }
 
 __global__ void k_coop_prep(FosDevState* ds) {
+    ds->grid_ovf = 0;
     ds->omax_bits = 0u;
     ds->maxabs_dr_bits = 0u;
     ds->changed = 0;
@@ -199,6 +238,11 @@ int fos_frame_coop_dynamics(FosCtx* c, const FosState* st, const FosFrameParams*
     a.rank = c->rank;
     a.ci_tmp = c->ci_tmp;
     a.cnt = c->coop_cnt;
+    a.cnt2 = c->coop_cnt2;
+    a.cfix = c->coop_fixed ? c->coop_cfix : nullptr;
+    a.idsort = c->coop_idsort;
+    a.spfix = c->coop_spfix;
+    a.slot_of = c->coop_slot;
     a.part = c->coop_part;
     a.bsum = c->coop_bsum;
     a.sp = c->sorted;

@@ -69,10 +69,13 @@ struct Stencil {
     int st, excl, incl, total;
 };
 
+// cap > 0: fixed-capacity cell rows, cell cid starting at slot
+// (cell_base + cid) * cap (cs unused); otherwise CSR starts cs[cid].
 template <class LD>
 __device__ __forceinline__ Stencil stencil_ranges(float px, float py, float pz, float L, float invL,
                                                   float halfL, int G, const int32_t* cs,
-                                                  const int32_t* cc, int lane) {
+                                                  const int32_t* cc, int lane, int cap = 0,
+                                                  int cell_base = 0) {
     int hx = home_coord(px, L, invL, halfL, G);
     int hy = home_coord(py, L, invL, halfL, G);
     int hz = home_coord(pz, L, invL, halfL, G);
@@ -82,7 +85,7 @@ __device__ __forceinline__ Stencil stencil_ranges(float px, float py, float pz, 
         int ny = wrap_mod(hy + (lane / 3) % 3 - 1, G);
         int nz = wrap_mod(hz + lane % 3 - 1, G);
         int cid = (nx * G + ny) * G + nz;
-        st = LD::ld(&cs[cid]);
+        st = cap ? (cell_base + cid) * cap : LD::ld(&cs[cid]);
         ct = LD::ld(&cc[cid]);
     }
     int incl = ct;
@@ -124,13 +127,18 @@ struct GridGeom {
 // lanes evaluate 32 candidates at a time and the corrections of overlapping
 // pairs are added in candidate order, so the FP32 sum is the reference loop's
 // sum bit for bit.  Must be called by all 32 lanes.
+// Returns particle i to lane 0 (-1 to the other lanes); with np != NULL,
+// lane 0 also gets the new (wrapped) position in *np.  cap / cell_base as in
+// stencil_ranges.
 template <class LD>
-__device__ __forceinline__ void pbd_warp(int kk, int lane, const float4* sp, const int32_t* ci,
-                                         float* pout, const GridGeom g, const int32_t* cs,
-                                         const int32_t* cc, float gap1, float mdf, float dmul) {
+__device__ __forceinline__ int pbd_warp(int kk, int lane, const float4* sp, const int32_t* ci,
+                                        float* pout, const GridGeom g, const int32_t* cs,
+                                        const int32_t* cc, float gap1, float mdf, float dmul,
+                                        float3* np = nullptr, int cap = 0, int cell_base = 0) {
     float4 me = LD::ld(&sp[kk]);
     float px = me.x, py = me.y, pz = me.z, ri = me.w;
-    Stencil r = stencil_ranges<LD>(px, py, pz, g.L, g.invL, g.halfL, g.G, cs, cc, lane);
+    Stencil r = stencil_ranges<LD>(px, py, pz, g.L, g.invL, g.halfL, g.G, cs, cc, lane, cap,
+                                   cell_base);
     float md = fmul(mdf, ri);
     float cx = 0.f, cy = 0.f, cz = 0.f;
     for (int base = 0; base < r.total; base += 32) {
@@ -175,10 +183,16 @@ __device__ __forceinline__ void pbd_warp(int kk, int lane, const float4* sp, con
             cz = fmul(cz, sc);
         }
         int i = LD::ld(&ci[kk]);
-        pout[3 * i + 0] = grid_wrap(fadd(px, cx), g.L, g.invL);
-        pout[3 * i + 1] = grid_wrap(fadd(py, cy), g.L, g.invL);
-        pout[3 * i + 2] = grid_wrap(fadd(pz, cz), g.L, g.invL);
+        const float nx = grid_wrap(fadd(px, cx), g.L, g.invL);
+        const float ny = grid_wrap(fadd(py, cy), g.L, g.invL);
+        const float nz = grid_wrap(fadd(pz, cz), g.L, g.invL);
+        pout[3 * i + 0] = nx;
+        pout[3 * i + 1] = ny;
+        pout[3 * i + 2] = nz;
+        if (np) *np = make_float3(nx, ny, nz);
+        return i;
     }
+    return -1;
 }
 
 // compute_local_max_overlaps (dynamics.py:304-352) for the particle at
@@ -188,10 +202,11 @@ template <class LD>
 __device__ __forceinline__ unsigned int maxov_warp(int kk, int lane, const float4* sp,
                                                    const int32_t* ci, const GridGeom g,
                                                    const int32_t* cs, const int32_t* cc, float eps,
-                                                   float* lmd) {
+                                                   float* lmd, int cap = 0, int cell_base = 0) {
     float4 me = LD::ld(&sp[kk]);
     int i = LD::ld(&ci[kk]);
-    Stencil r = stencil_ranges<LD>(me.x, me.y, me.z, g.L, g.invL, g.halfL, g.G, cs, cc, lane);
+    Stencil r = stencil_ranges<LD>(me.x, me.y, me.z, g.L, g.invL, g.halfL, g.G, cs, cc, lane, cap,
+                                   cell_base);
     float lm = 0.f;
     for (int base = 0; base < r.total; base += 32) {
         int t = base + lane;
@@ -279,6 +294,92 @@ __device__ __forceinline__ float pressure_group(int i, int lane, const PressureA
         rout[i] = fmaxf(a.rmin, fminf(a.rmax, fadd(ri, d)));
     }
     return d;
+}
+
+// pressure_group for max_nei <= 16 with a group of 8 lanes: lane t handles
+// the budgeted neighbours t and t + 8 at once (independent loads and powf),
+// and the terms are summed in neighbour order 0..an-1 as in pressure_group,
+// so the result is bit-identical.  The neighbour choice (fsc, face_ids, the
+// hashed rotation) does not change within a frame, so it is split out
+// (PressureNbr) and a caller may keep it in registers across the sweeps.
+struct PressureNbr {
+    int fc;       // fsc[i] (0: no neighbours, or i >= n)
+    int j[2];     // neighbours t and t + 8 of this lane
+    bool ok[2];   // whether each takes part (in budget, valid, not i)
+};
+
+template <class LD>
+__device__ __forceinline__ PressureNbr pressure_nbr8x2(int i, int lane, const PressureArgs a) {
+    PressureNbr nb;
+    const int gl = lane & 7;
+    nb.fc = i < a.n ? LD::ld(&a.fsc[i]) : 0;
+    nb.j[0] = nb.j[1] = 0;
+    nb.ok[0] = nb.ok[1] = false;
+    if (nb.fc > 0) {
+        const int an = nb.fc < a.max_nei ? nb.fc : a.max_nei;
+        const int st = hash_func(i - a.hoff, a.frame) % nb.fc;
+#pragma unroll
+        for (int h = 0; h < 2; ++h) {
+            const int kk = gl + 8 * h;
+            if (kk < an) {
+                const int ni = (st + kk) % nb.fc;
+                const int j = LD::ld(&a.face_ids[(size_t)i * FOS_S + ni]);
+                nb.j[h] = j;
+                nb.ok[h] = !(j < 0 || j >= a.n || j == i);
+            }
+        }
+    }
+    return nb;
+}
+
+template <class LD>
+__device__ __forceinline__ float pressure_sweep8x2(int i, int lane, const PressureArgs a,
+                                                   const PressureNbr& nb, const float* rin,
+                                                   float* rout, float* delta_r) {
+    const int gl = lane & 7;
+    const int base_lane = lane & 24;
+    const unsigned int gmask = 0xffu << base_lane;
+    const bool live = i < a.n;
+    const float ri = live ? LD::ld(&rin[i]) : 0.f;
+    float d = 0.f;
+    if (nb.fc > 0) {
+        const float rj0 = nb.ok[0] ? LD::ld(&rin[nb.j[0]]) : 0.f;
+        const float rj1 = nb.ok[1] ? LD::ld(&rin[nb.j[1]]) : 0.f;
+        const float Vi = powf(ri, a.P);
+        const float invP = fdiv(1.0f, a.P);
+        float term[2] = {0.f, 0.f};
+#pragma unroll
+        for (int h = 0; h < 2; ++h) {
+            if (nb.ok[h]) {
+                const float Vj = powf(h == 0 ? rj0 : rj1, a.P);
+                const float dvr = fmul(a.k, fsub(Vi, Vj));
+                const float vmin = fminf(Vi, Vj);
+                const float dv = fmaxf(fmul(-a.cap, vmin), fminf(fmul(a.cap, vmin), dvr));
+                term[h] = fsub(powf(fsub(Vi, dv), invP), ri);
+            }
+        }
+#pragma unroll
+        for (int h = 0; h < 2; ++h) {
+            unsigned int m = (__ballot_sync(gmask, nb.ok[h]) & gmask) >> base_lane;
+            while (m) {
+                const int b = __ffs(m) - 1;
+                m &= m - 1;
+                d = fadd(d, __shfl_sync(gmask, term[h], b, 8));
+            }
+        }
+    }
+    if (live && gl == 0) {
+        delta_r[i] = d;
+        rout[i] = fmaxf(a.rmin, fminf(a.rmax, fadd(ri, d)));
+    }
+    return d;
+}
+
+template <class LD>
+__device__ __forceinline__ float pressure_group8x2(int i, int lane, const PressureArgs a,
+                                                   const float* rin, float* rout, float* delta_r) {
+    const PressureNbr nb = pressure_nbr8x2<LD>(i, lane, a);
+    return pressure_sweep8x2<LD>(i, lane, a, nb, rin, rout, delta_r);
 }
 
 // apply_brownian_motion (dynamics.py:1596-1634) for particle i.  ti.random()
