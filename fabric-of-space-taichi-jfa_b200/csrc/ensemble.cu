@@ -862,7 +862,8 @@ static int ens_finalize_targets(FosEnsemble* e, cudaStream_t s) {
     FosCtx* c = e->c;
     const int n = e->ntot;
     const int nb = fos_blocks(n, 256);
-    k_rows<<<nb, 256, 0, s>>>(n, c->rowcnt, c->rowbuf, c->face_ids, c->face_counts, c->ds);
+    k_rows<<<fos_blocks(32LL * n, 256), 256, 0, s>>>(n, c->rowcnt, c->rowbuf, c->face_ids,
+                                                     c->face_counts, c->ds);
     FOS_LAUNCHED(c);
     k_fin_reset<<<nb, 256, 0, s>>>(c->ds, c->fin_changed, c->revcnt, c->revfill, n);
     FOS_LAUNCHED(c);
@@ -875,7 +876,7 @@ static int ens_finalize_targets(FosEnsemble* e, cudaStream_t s) {
     k_rev_fill<<<fos_blocks((long long)n * FOS_S, 256), 256, 0, s>>>(n, c->face_ids, c->face_score,
                                                                      c->revstart, c->revfill, c->rev);
     FOS_LAUNCHED(c);
-    k_rev_sort<<<nb, 256, 0, s>>>(n, c->revstart, c->rev);
+    k_rev_sort<<<fos_blocks(32LL * n, 256), 256, 0, s>>>(n, c->revstart, c->rev);
     FOS_LAUNCHED(c);
     int per_sm = 0;
     FOS_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_finalize, 256, 0));

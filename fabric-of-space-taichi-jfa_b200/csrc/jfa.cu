@@ -159,28 +159,47 @@ __global__ void k_compact(unsigned long long* keys, unsigned int* hmin, unsigned
 
 // Slot order of face_ids[a] = ascending first-touch key; the first 32 partners
 // get slots, later ones are dropped as the reference's slot search drops them.
-__global__ void k_rows(int n, const int32_t* __restrict__ rowcnt, const uint4* __restrict__ rowbuf,
-                       int32_t* __restrict__ face_ids, int32_t* __restrict__ face_counts,
-                       FosDevState* ds) {
-    int a = blockIdx.x * blockDim.x + threadIdx.x;
-    if (a >= n) return;
+// One warp per particle a: the row's (<= 64) candidates sit in registers,
+// two per lane; each one's rank (stable, by first-touch key) comes from
+// shuffles, and ranks below 32 are the slots.
+__global__ void __launch_bounds__(256) k_rows(int n, const int32_t* __restrict__ rowcnt,
+                                              const uint4* __restrict__ rowbuf,
+                                              int32_t* __restrict__ face_ids,
+                                              int32_t* __restrict__ face_counts, FosDevState* ds) {
+    const int a = (int)(((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5);
+    const int lane = threadIdx.x & 31;
+    if (a >= n) return;  // warp-uniform
     int m = rowcnt[a];
-    if (m > 0) atomicMax(&ds->max_rowcnt, m);
+    if (lane == 0 && m > 0) atomicMax(&ds->max_rowcnt, m);
     if (m > FOS_ROWCAP) m = FOS_ROWCAP;
-    uint4 e[FOS_ROWCAP];
-    for (int k = 0; k < m; ++k) {
-        uint4 v = rowbuf[(size_t)a * FOS_ROWCAP + k];
-        int j = k - 1;
-        while (j >= 0 && e[j].x > v.x) {
-            e[j + 1] = e[j];
-            --j;
-        }
-        e[j + 1] = v;
+    const uint4 none = make_uint4(0xFFFFFFFFu, 0u, 0u, 0u);
+    const size_t rb = (size_t)a * FOS_ROWCAP;
+    const uint4 e0 = lane < m ? rowbuf[rb + lane] : none;
+    const uint4 e1 = lane + 32 < m ? rowbuf[rb + lane + 32] : none;
+    int r0 = 0, r1 = 0;
+    const int m0 = m < 32 ? m : 32;
+    for (int k = 0; k < m0; ++k) {
+        const unsigned int kx = __shfl_sync(0xffffffffu, e0.x, k);
+        r0 += (kx < e0.x) || (kx == e0.x && k < lane);
+        r1 += (kx < e1.x) || (kx == e1.x);
     }
-    for (int s = 0; s < FOS_S; ++s) {
-        size_t o = (size_t)a * FOS_S + s;
-        face_ids[o] = s < m ? (int)e[s].y : -1;
-        face_counts[o] = s < m ? (int)e[s].z : 0;
+    for (int k = 32; k < m; ++k) {
+        const unsigned int kx = __shfl_sync(0xffffffffu, e1.x, k - 32);
+        r0 += kx < e0.x;
+        r1 += (kx < e1.x) || (kx == e1.x && k < lane + 32);
+    }
+    const size_t o = (size_t)a * FOS_S;
+    if (lane < m && r0 < FOS_S) {
+        face_ids[o + r0] = (int)e0.y;
+        face_counts[o + r0] = (int)e0.z;
+    }
+    if (lane + 32 < m && r1 < FOS_S) {
+        face_ids[o + r1] = (int)e1.y;
+        face_counts[o + r1] = (int)e1.z;
+    }
+    if (lane >= m) {
+        face_ids[o + lane] = -1;
+        face_counts[o + lane] = 0;
     }
 }
 
@@ -205,10 +224,37 @@ __global__ void k_rev_fill(int n, const int32_t* __restrict__ face_ids,
     rev[revstart[j] + p] = (int)t;  // encodes (a, s) as a*32 + s
 }
 
-__global__ void k_rev_sort(int n, const int32_t* __restrict__ revstart, int32_t* __restrict__ rev) {
-    int j = blockIdx.x * blockDim.x + threadIdx.x;
-    if (j >= n) return;
-    int b = revstart[j], e = revstart[j + 1];
+// One warp per particle j sorts its reverse list ascending (values are
+// distinct): up to 64 entries by shuffle ranks in registers, longer lists by
+// lane 0's insertion sort.
+__global__ void __launch_bounds__(256) k_rev_sort(int n, const int32_t* __restrict__ revstart,
+                                                  int32_t* __restrict__ rev) {
+    const int j = (int)(((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5);
+    const int lane = threadIdx.x & 31;
+    if (j >= n) return;  // warp-uniform
+    const int b = revstart[j], e = revstart[j + 1], len = e - b;
+    if (len <= 1) return;
+    if (len <= 64) {
+        const int v0 = lane < len ? rev[b + lane] : 0x7fffffff;
+        const int v1 = lane + 32 < len ? rev[b + lane + 32] : 0x7fffffff;
+        int r0 = 0, r1 = 0;
+        const int l0 = len < 32 ? len : 32;
+        for (int k = 0; k < l0; ++k) {
+            const int kv = __shfl_sync(0xffffffffu, v0, k);
+            r0 += kv < v0;
+            r1 += kv < v1;
+        }
+        for (int k = 32; k < len; ++k) {
+            const int kv = __shfl_sync(0xffffffffu, v1, k - 32);
+            r0 += kv < v0;
+            r1 += kv < v1;
+        }
+        __syncwarp();
+        if (lane < len) rev[b + r0] = v0;
+        if (lane + 32 < len) rev[b + r1] = v1;
+        return;
+    }
+    if (lane != 0) return;
     for (int k = b + 1; k < e; ++k) {
         int v = rev[k];
         int q = k - 1;
@@ -454,7 +500,8 @@ extern "C" int fos_jfa_accumulate_faces(FosCtx* c, int n, fos_stream_t s) {
     k_compact<<<c->num_sms * 4, 256, 0, s>>>(c->hkeys, c->hmin, c->hcnt, c->claimed, c->ds,
                                              c->rowcnt, c->rowbuf);
     FOS_LAUNCHED(c);
-    k_rows<<<fos_blocks(n, 256), 256, 0, s>>>(n, c->rowcnt, c->rowbuf, c->face_ids, c->face_counts,
+    k_rows<<<fos_blocks(32LL * n, 256), 256, 0, s>>>(n, c->rowcnt, c->rowbuf, c->face_ids,
+                                                     c->face_counts,
                                               c->ds);
     FOS_LAUNCHED(c);
     return FOS_OK;
@@ -473,7 +520,7 @@ static int finalize_impl(FosCtx* c, const float* rad, int n, bool apply_ema, cud
     k_rev_fill<<<fos_blocks((long long)n * FOS_S, 256), 256, 0, s>>>(n, c->face_ids, c->face_score,
                                                                      c->revstart, c->revfill, c->rev);
     FOS_LAUNCHED(c);
-    k_rev_sort<<<nb, 256, 0, s>>>(n, c->revstart, c->rev);
+    k_rev_sort<<<fos_blocks(32LL * n, 256), 256, 0, s>>>(n, c->revstart, c->rev);
     FOS_LAUNCHED(c);
     int per_sm = 0;
     FOS_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_finalize, 256, 0));
