@@ -116,13 +116,25 @@ __device__ __forceinline__ void coop_p1_one(const Args& a, const Geo& geo, int i
 // lane q % 32 by shuffle, and the lanes run coop_p1_val together every 32
 // particles, so the cell atomics of a warp's particles cost one round trip,
 // not one per particle.
+// With ou != NULL each deferred particle first takes the frame's OU jitter
+// step (apply_brownian + integrate_jitter, run.py:855-867) at its new
+// position, which is what the rebuild after the last PBD sweep then sees.
+struct OuStep {
+    float* vjit;
+    const float* rad;
+    OuParams o;
+    float kick;           // sigma * sqrt(dt)
+    unsigned int frame;
+    int ctr_base;         // Philox counter = i - ctr_base (index within the foam)
+};
+
 struct P1Defer {
     int i = -1;
     float3 v;
     int q = 0;
     template <class Args, class Geo>
     __device__ __forceinline__ void put(const Args& a, const Geo& geo, int lane, int pi, float3 pv,
-                                        float* dst, int par) {
+                                        float* dst, int par, const OuStep* ou = nullptr) {
         const int slot = q & 31;
         const int si = __shfl_sync(0xffffffffu, pi, 0);
         const float sx = __shfl_sync(0xffffffffu, pv.x, 0);
@@ -133,11 +145,17 @@ struct P1Defer {
             v = make_float3(sx, sy, sz);
         }
         ++q;
-        if (slot == 31) flush(a, geo, dst, par);
+        if (slot == 31) flush(a, geo, dst, par, ou);
     }
     template <class Args, class Geo>
-    __device__ __forceinline__ void flush(const Args& a, const Geo& geo, float* dst, int par) {
-        if (i >= 0) coop_p1_val(a, geo, i, v, dst, par);
+    __device__ __forceinline__ void flush(const Args& a, const Geo& geo, float* dst, int par,
+                                          const OuStep* ou = nullptr) {
+        if (i >= 0) {
+            if (ou)
+                v = ou_one(i, (unsigned int)(i - ou->ctr_base), v, ou->vjit, __ldcg(&ou->rad[i]),
+                           ou->kick, ou->o, ou->frame);
+            coop_p1_val(a, geo, i, v, dst, par);
+        }
         i = -1;
     }
 };

@@ -72,6 +72,63 @@ __global__ void k_brownian(float* pos, int n, float strength, float domain, floa
     brownian_one<LdRO>(i, (unsigned int)i, pos, strength, domain, halfL, k0, k1, frame);
 }
 
+// Sum of the radii as 2^-40 fixed-point integers (compute_mean_radius,
+// dynamics.py:675-689): warp sums, one 64-bit atomic per warp.
+__global__ void __launch_bounds__(256) k_rad_sum(const float* __restrict__ rad, int n,
+                                                 unsigned long long* sum) {
+    long long q = 0;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+        q += rad_fixed(__ldg(&rad[i]));
+#pragma unroll
+    for (int o = 16; o >= 1; o >>= 1) q += __shfl_xor_sync(0xffffffffu, q, o);
+    if ((threadIdx.x & 31) == 0 && q) atomicAdd(sum, (unsigned long long)q);
+}
+
+__global__ void k_mean_from_sum(const unsigned long long* sum, int n, float* mean) {
+    *mean = mean_from_fixed(*sum, n);
+}
+
+// apply_brownian (dynamics.py:607-646), mean radius from a device float.
+__global__ void k_ou_velocity(float* vjit, const float* __restrict__ rad, const float* mean, int n,
+                              OuParams o, unsigned int frame) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const float kick = ou_kick(o, *mean);
+    float3 v = make_float3(vjit[3 * i + 0], vjit[3 * i + 1], vjit[3 * i + 2]);
+    v = ou_velocity((unsigned int)i, v, __ldg(&rad[i]), kick, o, frame);
+    vjit[3 * i + 0] = v.x;
+    vjit[3 * i + 1] = v.y;
+    vjit[3 * i + 2] = v.z;
+}
+
+// integrate_jitter (dynamics.py:649-660)
+__global__ void k_ou_move(float* pos, const float* __restrict__ vjit, int n, OuParams o) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    float3 p = make_float3(pos[3 * i + 0], pos[3 * i + 1], pos[3 * i + 2]);
+    float3 v = make_float3(__ldg(&vjit[3 * i + 0]), __ldg(&vjit[3 * i + 1]),
+                           __ldg(&vjit[3 * i + 2]));
+    p = ou_move(p, v, o);
+    pos[3 * i + 0] = p.x;
+    pos[3 * i + 1] = p.y;
+    pos[3 * i + 2] = p.z;
+}
+
+// Frame step 6B (run.py:855-867): apply_brownian + integrate_jitter fused,
+// the mean radius from the fixed-point sum and the frame index from the
+// device counter.
+__global__ void k_ou_frame(float* pos, float* vjit, const float* __restrict__ rad, int n,
+                           const unsigned long long* sum, const int* frame_ptr, OuParams o) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const float kick = ou_kick(o, mean_from_fixed(*sum, n));
+    float3 p = make_float3(pos[3 * i + 0], pos[3 * i + 1], pos[3 * i + 2]);
+    p = ou_one(i, (unsigned int)i, p, vjit, __ldg(&rad[i]), kick, o, (unsigned int)*frame_ptr);
+    pos[3 * i + 0] = p.x;
+    pos[3 * i + 1] = p.y;
+    pos[3 * i + 2] = p.z;
+}
+
 // set_fsc_targets (dynamics.py:1242-1320).  With gate != NULL it runs only
 // when the warm-start gate (run.py:1184-1197) is open -- frame >=
 // warm_frames and zero-FSC fraction <= zero_thresh -- and then also resets
@@ -209,6 +266,29 @@ int fos_launch_brownian(FosCtx* c, float* pos, int n, float strength, float doma
     return FOS_OK;
 }
 
+static int launch_rad_sum(FosCtx* c, const float* rad, int n, cudaStream_t s) {
+    FOS_CUDA(cudaMemsetAsync(&c->ds->rad_sum, 0, sizeof(unsigned long long), s));
+    int blocks = fos_blocks(n > 0 ? n : 1, 256);
+    if (blocks > 2 * c->num_sms) blocks = 2 * c->num_sms;
+    k_rad_sum<<<blocks, 256, 0, s>>>(rad, n, &c->ds->rad_sum);
+    FOS_LAUNCHED(c);
+    return FOS_OK;
+}
+
+// Frame step 6B: mean radius, then the fused OU update of every particle.
+int fos_launch_ou_frame(FosCtx* c, float* pos, float* vjit, const float* rad, int n,
+                        const FosFrameParams* fp, cudaStream_t s) {
+    if (n == 0) return FOS_OK;
+    int rc = launch_rad_sum(c, rad, n, s);
+    if (rc) return rc;
+    OuParams o = ou_params(fp->jitter_rms, fp->jitter_tau, fp->max_drift_fraction,
+                           c->p.gap_fraction, (float)fp->dt, c->L, c->invL, fp->seed);
+    k_ou_frame<<<fos_blocks(n, 256), 256, 0, s>>>(pos, vjit, rad, n, &c->ds->rad_sum,
+                                                  &c->ds->frame, o);
+    FOS_LAUNCHED(c);
+    return FOS_OK;
+}
+
 int fos_launch_set_targets(FosCtx* c, const float* rad, float* rt, const int32_t* fsc,
                            const float* ema, int n, int f_low, int f_high, float growth, float rmin,
                            float rmax, FosDevState* gate, int warm_frames, double zero_thresh,
@@ -310,6 +390,53 @@ extern "C" int fos_apply_brownian(FosCtx* c, float* pos, int n, float strength, 
     if (n == 0) return FOS_OK;
     return fos_launch_brownian(c, pos, n, strength, domain_size, seed, (int)frame, nullptr, nullptr,
                                s);
+}
+
+extern "C" int fos_init_jitter_velocities(FosCtx* c, float* v_jit, int n, fos_stream_t s) {
+    int rc = check_dyn(c, n);
+    if (rc) return rc;
+    FOS_REQUIRE(n == 0 || v_jit, FOS_E_ARG, "NULL argument");
+    if (n) FOS_CUDA(cudaMemsetAsync(v_jit, 0, (size_t)n * 12, s));
+    return FOS_OK;
+}
+
+extern "C" int fos_compute_mean_radius(FosCtx* c, const float* rad, int n, float* mean_radius,
+                                       fos_stream_t s) {
+    int rc = check_dyn(c, n);
+    if (rc) return rc;
+    FOS_REQUIRE(mean_radius && (n == 0 || rad), FOS_E_ARG, "NULL argument");
+    rc = launch_rad_sum(c, rad, n, s);
+    if (rc) return rc;
+    k_mean_from_sum<<<1, 1, 0, s>>>(&c->ds->rad_sum, n, mean_radius);
+    FOS_LAUNCHED(c);
+    return FOS_OK;
+}
+
+extern "C" int fos_apply_jitter(FosCtx* c, float* v_jit, const float* rad, const float* mean_radius,
+                                int n, float dt, double jitter_rms, double jitter_tau,
+                                double max_drift_fraction, double gap_fraction, uint64_t seed,
+                                uint32_t frame, fos_stream_t s) {
+    int rc = check_dyn(c, n);
+    if (rc) return rc;
+    FOS_REQUIRE(n == 0 || (v_jit && rad && mean_radius), FOS_E_ARG, "NULL argument");
+    if (n == 0) return FOS_OK;
+    OuParams o = ou_params(jitter_rms, jitter_tau, max_drift_fraction, gap_fraction, dt, c->L,
+                           c->invL, seed);
+    k_ou_velocity<<<fos_blocks(n, 256), 256, 0, s>>>(v_jit, rad, mean_radius, n, o, frame);
+    FOS_LAUNCHED(c);
+    return FOS_OK;
+}
+
+extern "C" int fos_integrate_jitter(FosCtx* c, float* pos, const float* v_jit, int n, float dt,
+                                    fos_stream_t s) {
+    int rc = check_dyn(c, n);
+    if (rc) return rc;
+    FOS_REQUIRE(n == 0 || (pos && v_jit), FOS_E_ARG, "NULL argument");
+    if (n == 0) return FOS_OK;
+    OuParams o = ou_params(0.0, 1.0, 0.0, 0.0, dt, c->L, c->invL, 0);
+    k_ou_move<<<fos_blocks(n, 256), 256, 0, s>>>(pos, v_jit, n, o);
+    FOS_LAUNCHED(c);
+    return FOS_OK;
 }
 
 extern "C" int fos_set_fsc_targets(FosCtx* c, const float* rad, float* rad_target,

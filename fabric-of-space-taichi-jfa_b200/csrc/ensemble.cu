@@ -583,6 +583,7 @@ extern "C" int fos_ensemble_create(const FosParams* p, const FosFrameParams* fp,
     FOS_REQUIRE(nfoams >= 1 && nfoams <= 65536, FOS_E_ARG, "nfoams must be in [1, 65536]");
     FOS_REQUIRE(p->early_exit == 0, FOS_E_ARG, "ensembles run every pass: early_exit must be 0");
     FOS_REQUIRE(fp->max_eq_nei <= 16, FOS_E_ARG, "ensembles need max_eq_nei <= 16");
+    FOS_REQUIRE(!fp->ou_jitter, FOS_E_ARG, "ensembles run without the OU jitter (ou_jitter = 0)");
     for (int f = 0; f < nfoams; ++f) {
         int rc = ens_check_foam(foams[f]);
         if (rc) return rc;

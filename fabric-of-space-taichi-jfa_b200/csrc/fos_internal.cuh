@@ -40,6 +40,7 @@ struct FosDevState {
     unsigned int bar_count;       // grid barrier arrival counter
     unsigned int bar_gen;         // grid barrier generation
     int grid_ovf;                 // bit p: a fixed-capacity cell row of count buffer p overflowed
+    unsigned long long rad_sum;   // OU jitter: sum of the radii, 2^-40 fixed point
     unsigned long long changes[FOS_MAX_PASSES];
 };
 

@@ -29,6 +29,8 @@ int fos_launch_nudge(FosCtx* c, float* rad, const float* rt, const float* lmd, i
                      float max_step, float rmin, float rmax, float back, const unsigned int* back_bits,
                      int mode, const FosDevState* gate, cudaStream_t s);
 int fos_launch_wrap(FosCtx* c, float* pos, int n, cudaStream_t s);
+int fos_launch_ou_frame(FosCtx* c, float* pos, float* vjit, const float* rad, int n,
+                        const FosFrameParams* fp, cudaStream_t s);
 
 extern "C" void fos_frame_params_default(FosFrameParams* fp) {
     if (!fp) return;
@@ -52,6 +54,11 @@ extern "C" void fos_frame_params_default(FosFrameParams* fp) {
     fp->brownian_strength = 0.0002;  // BROWNIAN_STRENGTH
     fp->seed = 0;
     fp->warmup_pbd = 4;              // PBD_BASE_PASSES
+    fp->ou_jitter = 0;               // JITTER_ENABLED is True in config.py:493; off here
+    fp->jitter_rms = 0.10;           // JITTER_RMS (config.py:494)
+    fp->jitter_tau = 1.0;            // JITTER_TAU (config.py:496)
+    fp->dt = 0.016;                  // DT (config.py:400)
+    fp->max_drift_fraction = 0.20;   // MAX_DRIFT_FRACTION (config.py:498)
 }
 
 __global__ void k_frame_set(FosDevState* ds, int frame, int settle) {
@@ -69,6 +76,9 @@ static int check_state(FosCtx* c, const FosState* st, const FosFrameParams* fp) 
                     st->cell_count && st->cell_start && st->cell_indices,
                 FOS_E_ARG, "NULL state buffer");
     FOS_REQUIRE(fp->pbd_iters >= 0 && fp->pressure_iters >= 0, FOS_E_ARG, "negative iterations");
+    FOS_REQUIRE(!fp->ou_jitter || st->v_jit, FOS_E_ARG, "ou_jitter needs FosState.v_jit");
+    FOS_REQUIRE(!fp->ou_jitter || (fp->dt > 0.0 && fp->jitter_tau >= 0.0), FOS_E_ARG,
+                "ou_jitter needs dt > 0 and jitter_tau >= 0");
     return FOS_OK;
 }
 
@@ -89,6 +99,8 @@ extern "C" int fos_sim_init(FosCtx* c, const FosState* st, const FosFrameParams*
     FOS_CUDA(cudaMemsetAsync(st->local_max_depth, 0, (size_t)n * 4, s));
     FOS_CUDA(cudaMemsetAsync(st->delta_r, 0, (size_t)n * 4, s));
     FOS_CUDA(cudaMemcpyAsync(st->rad_target, st->rad, (size_t)n * 4, cudaMemcpyDeviceToDevice, s));
+    // init_jitter_velocities (run.py:346)
+    if (st->v_jit) FOS_CUDA(cudaMemsetAsync(st->v_jit, 0, (size_t)n * 12, s));
     k_frame_set<<<1, 1, 0, s>>>(c->ds, frame0, 0);
     FOS_LAUNCHED(c);
     // wrap_seeded_positions (run.py:233-237) + warmup_pbd (run.py:293-318)
@@ -170,7 +182,8 @@ static int frame_impl(FosCtx* c, const FosState* st, const FosFrameParams* fp, i
 #define MARK(id) \
     if (prof) prof->mark(id)
     const int* dframe = &c->ds->frame;
-    if (c->use_coop && !prof && fp->max_eq_nei <= 16 && fos_coop_supported(c)) {
+    if (c->use_coop && !prof && fp->max_eq_nei <= 16 && !(fp->ou_jitter && fp->pbd_iters == 0) &&
+        fos_coop_supported(c)) {
         // (1)-(7) as one persistent cooperative kernel (frame_coop.cu)
         rc = fos_frame_coop_dynamics(c, st, fp, s);
         if (rc) return rc;
@@ -215,6 +228,12 @@ static int frame_impl(FosCtx* c, const FosState* st, const FosFrameParams* fp, i
             if (rc) return rc;
             MARK(5);
             src = c->pos_tmp;
+        }
+        // (6B) OU jitter: apply_brownian + integrate_jitter (run.py:855-867)
+        if (fp->ou_jitter) {
+            rc = fos_launch_ou_frame(c, (float*)src, st->v_jit, st->rad, n, fp, s);
+            if (rc) return rc;
+            MARK(10);
         }
         rc = fos_grid_build_from(c, src, st->pos, n, st->cell_count, st->cell_start, st->cell_indices,
                                  nullptr, s);

@@ -51,6 +51,9 @@ struct CoopArgs {
     PressureArgs pa;
     float strength, domain, halfL;
     uint32_t k0, k1;
+    int ou;                     // OU jitter fused into the last PBD sweep (pbd_iters >= 1)
+    float* vjit;
+    OuParams ou_p;
     unsigned long long* trace;  // optional: %globaltimer after every phase (block 0)
     int trace_cap;
 };
@@ -136,13 +139,22 @@ __global__ void __launch_bounds__(COOP_THREADS) k_frame_coop(CoopArgs a) {
     // (5) apply_brownian_motion (run.py:807-813); the odd-sweep result is copied
     // back into rad, and settle_frames_left -= 1 (run.py:750).  Each new
     // position enters the next rebuild's histogram right away (its P1).
+    // With the OU jitter on, the final radii are also summed here for its
+    // mean radius (run.py:860-861).
     {
         unsigned int frame = (unsigned int)pa.frame;
+        long long rq = 0;
         for (int i = tid; i < a.n; i += T) {
             if (a.sweeps & 1) a.rad[i] = __ldcg(&a.rad_tmp[i]);
+            if (a.ou) rq += rad_fixed(__ldcg(&a.rad[i]));
             brownian_one<LdL2>(i, (unsigned int)i, a.pos, a.strength, a.domain, a.halfL, a.k0,
                                a.k1, frame);
             coop_p1_one(a, geo, i, a.pos, a.pos, gk & 1);
+        }
+        if (a.ou) {
+#pragma unroll
+            for (int o = 16; o >= 1; o >>= 1) rq += __shfl_xor_sync(0xffffffffu, rq, o);
+            if (lane == 0 && rq) atomicAdd(&a.ds->rad_sum, (unsigned long long)rq);
         }
         if (tid == 0 && a.ds->settle > 0) a.ds->settle -= 1;
     }
@@ -151,11 +163,19 @@ __global__ void __launch_bounds__(COOP_THREADS) k_frame_coop(CoopArgs a) {
     // (6) PBD passes, each on a fresh grid (run.py:829-846); (7) rebuild (run.py:874)
     // Every rebuild here has its P1 done by the phase that produced the
     // positions (Brownian, then each PBD sweep's lane 0).
+    // The OU jitter step (run.py:855-867) runs inside the last sweep's P1.
     const float* src = a.pos;
     for (int k = 0; k < a.pbd_iters; ++k) {
         if (!coop_grid(a, geo, src, a.pos, a.rad, false, tk, ep, true, gk & 1, false, &lay))
             return;
         ++gk;
+        OuStep ous;
+        const bool ou_here = a.ou && k == a.pbd_iters - 1;
+        if (ou_here) {
+            const unsigned long long sum = *((volatile unsigned long long*)&a.ds->rad_sum);
+            ous = OuStep{a.vjit, a.rad, a.ou_p, ou_kick(a.ou_p, mean_from_fixed(sum, a.n)),
+                         (unsigned int)pa.frame, 0};
+        }
         P1Defer p1;
         int kk_next = wid < a.n ? __ldcg(&a.slot_of[wid]) : 0;
         for (int r = 0; r < warp_rounds; ++r) {
@@ -166,10 +186,10 @@ __global__ void __launch_bounds__(COOP_THREADS) k_frame_coop(CoopArgs a) {
                 float3 nv = make_float3(0.f, 0.f, 0.f);
                 int pi = pbd_warp<LdL2>(kk, lane, lay.sp, lay.ci, a.pos_tmp, a.g, lay.cs, lay.cc,
                                         a.gap1, a.mdf, a.dmul, &nv, lay.cap);
-                p1.put(a, geo, lane, pi, nv, a.pos, gk & 1);
+                p1.put(a, geo, lane, pi, nv, a.pos, gk & 1, ou_here ? &ous : nullptr);
             }
         }
-        p1.flush(a, geo, a.pos, gk & 1);
+        p1.flush(a, geo, a.pos, gk & 1, ou_here ? &ous : nullptr);
         if (!grid_barrier(a.ds, ep)) return;
         trace_mark(a, tk);
         src = a.pos_tmp;
@@ -179,6 +199,7 @@ __global__ void __launch_bounds__(COOP_THREADS) k_frame_coop(CoopArgs a) {
 
 __global__ void k_coop_prep(FosDevState* ds) {
     ds->grid_ovf = 0;
+    ds->rad_sum = 0ull;
     ds->omax_bits = 0u;
     ds->maxabs_dr_bits = 0u;
     ds->changed = 0;
@@ -273,10 +294,16 @@ int fos_frame_coop_dynamics(FosCtx* c, const FosState* st, const FosFrameParams*
     a.halfL = (float)(0.5 * (double)c->L);
     a.k0 = (uint32_t)fp->seed;
     a.k1 = (uint32_t)(fp->seed >> 32);
+    a.ou = fp->ou_jitter ? 1 : 0;
+    a.vjit = st->v_jit;
+    a.ou_p = ou_params(fp->jitter_rms, fp->jitter_tau, fp->max_drift_fraction, c->p.gap_fraction,
+                       (float)fp->dt, c->L, c->invL, fp->seed);
     a.trace = trace;
     a.trace_cap = trace_cap;
 
     FOS_REQUIRE(fp->max_eq_nei <= 16, FOS_E_ARG, "cooperative frame needs max_eq_nei <= 16");
+    FOS_REQUIRE(!a.ou || fp->pbd_iters >= 1, FOS_E_ARG,
+                "cooperative frame runs the OU jitter inside a PBD sweep: pbd_iters >= 1");
     k_coop_prep<<<1, 1, 0, s>>>(c->ds);
     FOS_LAUNCHED(c);
     FOS_CUDA(cudaMemsetAsync(c->coop_cnt, 0, (size_t)G3 * sizeof(int32_t), s));

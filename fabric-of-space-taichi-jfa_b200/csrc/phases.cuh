@@ -8,6 +8,8 @@
 // order with explicit round-to-nearest intrinsics (no FMA contraction).
 #pragma once
 
+#include <math.h>
+
 #include "fos_internal.cuh"
 
 // Load policies.  Standalone kernels read data no thread of the same launch
@@ -401,6 +403,94 @@ __device__ __forceinline__ void brownian_one(int i, unsigned int ctr, float* pos
         else if (p >= halfL) p = fsub(p, domain);
         pos[3 * i + d] = p;
     }
+}
+
+// OU jitter (dynamics.py:607-660).  Constants the reference folds in Python
+// (double) arrive folded and rounded once to float32:
+//   tau   = max(1e-6, JITTER_TAU)
+//   sq2   = sqrt(2 / max(1e-6, JITTER_TAU))
+//   capk  = MAX_DRIFT_FRACTION * GAP_FRACTION
+struct OuParams {
+    float rms, sq2, tau, capk, dt, L, invL;
+    uint32_t k0, k1;
+};
+
+static inline OuParams ou_params(double rms, double tau, double max_drift, double gap, float dt,
+                                 float L, float invL, uint64_t seed) {
+    const double t = tau > 1e-6 ? tau : 1e-6;
+    OuParams o;
+    o.rms = (float)rms;
+    o.sq2 = (float)sqrt(2.0 / t);
+    o.tau = (float)t;
+    o.capk = (float)(max_drift * gap);
+    o.dt = dt;
+    o.L = L;
+    o.invL = invL;
+    o.k0 = (uint32_t)seed;
+    o.k1 = (uint32_t)(seed >> 32);
+    return o;
+}
+
+// Radius r as a 2^-40 fixed-point integer: exact for r in [2^-17, 2^23), so a
+// sum of these is the exact sum of the radii in any order.
+__device__ __forceinline__ long long rad_fixed(float r) {
+    return __float2ll_rn(fmul(r, 0x1p40f));
+}
+
+// mean_radius from the fixed-point sum (the radii's exact mean rounded once
+// to float32).
+__device__ __forceinline__ float mean_from_fixed(unsigned long long sum, int n) {
+    return (float)((double)(long long)sum * 0x1p-40 / (double)(n > 1 ? n : 1));
+}
+
+// sigma * sqrt(dt) of apply_brownian, from the mean radius.
+__device__ __forceinline__ float ou_kick(const OuParams& o, float mean_r) {
+    return fmul(fmul(fmul(o.rms, mean_r), o.sq2), __fsqrt_rn(o.dt));
+}
+
+// apply_brownian for particle i (counter index ctr) with kick = sigma *
+// sqrt(dt): v += (-v / tau) * dt + kick * r, r = U[-0.5, 0.5)^3 from
+// Philox-4x32-10 (ctr, frame, 'OUJT', 0); a step |v| dt above
+// capk * (r_i + r_i) is scaled back to the cap.  Returns the new velocity.
+__device__ __forceinline__ float3 ou_velocity(unsigned int ctr, float3 v, float r_i, float kick,
+                                              const OuParams& o, unsigned int frame) {
+    uint4 rr = philox4x32_10(make_uint4(ctr, frame, 0x4f554a54u, 0u), o.k0, o.k1);
+    float ux = fsub(fmul((float)(rr.x >> 8), 0x1p-24f), 0.5f);
+    float uy = fsub(fmul((float)(rr.y >> 8), 0x1p-24f), 0.5f);
+    float uz = fsub(fmul((float)(rr.z >> 8), 0x1p-24f), 0.5f);
+    v.x = fadd(v.x, fadd(fmul(fdiv(-v.x, o.tau), o.dt), fmul(kick, ux)));
+    v.y = fadd(v.y, fadd(fmul(fdiv(-v.y, o.tau), o.dt), fmul(kick, uy)));
+    v.z = fadd(v.z, fadd(fmul(fdiv(-v.z, o.tau), o.dt), fmul(kick, uz)));
+    const float cap = fmul(o.capk, fadd(r_i, r_i));
+    const float len = fmul(__fsqrt_rn(fadd(fadd(fmul(v.x, v.x), fmul(v.y, v.y)), fmul(v.z, v.z))),
+                           o.dt);
+    if (len > cap) {
+        const float sc = fdiv(fdiv(cap, fmaxf(1e-6f, len)), o.dt);
+        v.x = fmul(v.x, sc);
+        v.y = fmul(v.y, sc);
+        v.z = fmul(v.z, sc);
+    }
+    return v;
+}
+
+// integrate_jitter for one position: wrapP(p + v * dt) with grid.wrapP.
+__device__ __forceinline__ float3 ou_move(float3 p, float3 v, const OuParams& o) {
+    return make_float3(grid_wrap(fadd(p.x, fmul(v.x, o.dt)), o.L, o.invL),
+                       grid_wrap(fadd(p.y, fmul(v.y, o.dt)), o.L, o.invL),
+                       grid_wrap(fadd(p.z, fmul(v.z, o.dt)), o.L, o.invL));
+}
+
+// apply_brownian + integrate_jitter for particle i at position p: updates
+// vjit[i] and returns the moved position.
+__device__ __forceinline__ float3 ou_one(int i, unsigned int ctr, float3 p, float* vjit, float r_i,
+                                         float kick, const OuParams& o, unsigned int frame) {
+    float3 v = make_float3(__ldcg(&vjit[3 * i + 0]), __ldcg(&vjit[3 * i + 1]),
+                           __ldcg(&vjit[3 * i + 2]));
+    v = ou_velocity(ctr, v, r_i, kick, o, frame);
+    vjit[3 * i + 0] = v.x;
+    vjit[3 * i + 1] = v.y;
+    vjit[3 * i + 2] = v.z;
+    return ou_move(p, v, o);
 }
 
 // smoothstep (dynamics.py:1226-1240)

@@ -70,13 +70,15 @@ class FosFrameParams(C.Structure):
         ("pressure_k", C.c_double), ("pressure_exp", C.c_double),
         ("pressure_pair_cap", C.c_double), ("max_eq_nei", C.c_int),
         ("brownian_strength", C.c_double), ("seed", C.c_uint64), ("warmup_pbd", C.c_int),
+        ("ou_jitter", C.c_int), ("jitter_rms", C.c_double), ("jitter_tau", C.c_double),
+        ("dt", C.c_double), ("max_drift_fraction", C.c_double),
     ]
 
 
 class FosState(C.Structure):
     _fields_ = [("n", C.c_int)] + [(n, C.c_void_p) for n in (
         "pos", "rad", "rad_target", "local_max_depth", "delta_r", "cell_count", "cell_start",
-        "cell_indices")]
+        "cell_indices", "v_jit")]
 
 
 class FosSurrogateStats(C.Structure):
@@ -146,6 +148,11 @@ SIGNATURES = {
     "fos_equilibrate_pressure": [_P, _I, _I, _P, _P, _P, _P, _F, _F, _F, _I, _F, _F, _I,
                                  C.POINTER(_F), C.POINTER(_I), _P],
     "fos_apply_brownian": [_P, _P, _I, _F, _F, C.c_uint64, C.c_uint32, _P],
+    "fos_init_jitter_velocities": [_P, _P, _I, _P],
+    "fos_compute_mean_radius": [_P, _P, _I, _P, _P],
+    "fos_apply_jitter": [_P, _P, _P, _P, _I, _F, C.c_double, C.c_double, C.c_double, C.c_double,
+                         C.c_uint64, C.c_uint32, _P],
+    "fos_integrate_jitter": [_P, _P, _P, _I, _F, _P],
     "fos_set_fsc_targets": [_P, _P, _P, _P, _P, _I, _I, _I, _F, _F, _F, _P],
     "fos_nudge_radii": [_P, _P, _P, _P, _I, _F, _F, _F, _F, _F, _I, _P],
     "fos_controller_stats": [_P, _P, _P, _P, _I, _I, _I, C.POINTER(_I), C.POINTER(_I),

@@ -57,6 +57,13 @@ class FosConfig:
     R_MIN: float = 0.002                  # config.py:49
     R_MAX: float = 0.010                  # config.py:50
     PBD_BASE_PASSES: int = 4              # config.py:342
+    # OU velocity jitter after the PBD sweeps (run.py:855-867).  config.py:493
+    # has it on; the headless workloads run with the Brownian channel only.
+    JITTER_ENABLED: bool = False
+    JITTER_RMS: float = 0.10              # config.py:494
+    JITTER_TAU: float = 1.0               # config.py:496
+    DT: float = 0.016                     # config.py:400
+    MAX_DRIFT_FRACTION: float = 0.20      # config.py:498
     # per-frame schedule of the headless driver
     PBD_ITERS: int = 4
     PRESSURE_ITERS: int = 1
@@ -104,7 +111,10 @@ class FosConfig:
             r_max=float(self.R_MAX), pressure_k=float(self.PRESSURE_K),
             pressure_exp=float(self.PRESSURE_EXP), pressure_pair_cap=float(self.PRESSURE_PAIR_CAP),
             max_eq_nei=int(self.MAX_EQ_NEI), brownian_strength=float(self.BROWNIAN_STRENGTH),
-            seed=int(self.SEED) & 0xFFFFFFFFFFFFFFFF, warmup_pbd=int(self.PBD_BASE_PASSES))
+            seed=int(self.SEED) & 0xFFFFFFFFFFFFFFFF, warmup_pbd=int(self.PBD_BASE_PASSES),
+            ou_jitter=int(bool(self.JITTER_ENABLED)), jitter_rms=float(self.JITTER_RMS),
+            jitter_tau=float(self.JITTER_TAU), dt=float(self.DT),
+            max_drift_fraction=float(self.MAX_DRIFT_FRACTION))
 
     @classmethod
     def for_foam(cls, foam, **over) -> "FosConfig":

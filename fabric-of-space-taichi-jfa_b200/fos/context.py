@@ -230,6 +230,24 @@ class Context:
         call("fos_apply_brownian", self.h, ptr(pos, torch.float32, "pos"), int(n), float(strength),
              float(domain_size), int(seed) & 0xFFFFFFFFFFFFFFFF, int(frame) & 0xFFFFFFFF, stream())
 
+    def init_jitter_velocities(self, v_jit, n):
+        call("fos_init_jitter_velocities", self.h, ptr(v_jit, torch.float32, "v_jit"), int(n),
+             stream())
+
+    def compute_mean_radius(self, rad, n, mean_radius):
+        call("fos_compute_mean_radius", self.h, ptr(rad, torch.float32, "rad"), int(n),
+             ptr(mean_radius, torch.float32, "mean_radius"), stream())
+
+    def apply_jitter(self, v_jit, rad, mean_radius, n, dt, rms, tau, max_drift, gap, seed, frame):
+        call("fos_apply_jitter", self.h, ptr(v_jit, torch.float32, "v_jit"),
+             ptr(rad, torch.float32, "rad"), ptr(mean_radius, torch.float32, "mean_radius"),
+             int(n), float(dt), float(rms), float(tau), float(max_drift), float(gap),
+             int(seed) & 0xFFFFFFFFFFFFFFFF, int(frame) & 0xFFFFFFFF, stream())
+
+    def integrate_jitter(self, pos, v_jit, n, dt):
+        call("fos_integrate_jitter", self.h, ptr(pos, torch.float32, "pos"),
+             ptr(v_jit, torch.float32, "v_jit"), int(n), float(dt), stream())
+
     def set_fsc_targets(self, rad, rad_target, fsc, fsc_ema, n, f_low, f_high, growth_pct,
                         r_min, r_max):
         call("fos_set_fsc_targets", self.h, ptr(rad, torch.float32, "rad"),

@@ -46,10 +46,12 @@ class FoamSim:
         self.cell_count = torch.zeros(G3, dtype=torch.int32, device=dev)
         self.cell_start = torch.zeros(G3, dtype=torch.int32, device=dev)
         self.cell_indices = torch.zeros(n, dtype=torch.int32, device=dev)
+        self.v_jit = torch.zeros(n, 3, dtype=torch.float32, device=dev)  # run.py:151
         self.state = FosState(n, self.pos.data_ptr(), self.rad.data_ptr(),
                               self.rad_target.data_ptr(), self.local_max_depth.data_ptr(),
                               self.delta_r.data_ptr(), self.cell_count.data_ptr(),
-                              self.cell_start.data_ptr(), self.cell_indices.data_ptr())
+                              self.cell_start.data_ptr(), self.cell_indices.data_ptr(),
+                              self.v_jit.data_ptr())
         self.fp = cfg.frame_params()
         self.frame = 0
         if surrogate is not None:
@@ -102,7 +104,7 @@ class FoamSim:
         return bool(jfa)
 
     STAGES = ("grid", "max_overlap", "nudge", "pressure", "brownian", "pbd", "jfa_passes",
-              "filter_faces", "finalize_ema", "targets_end")
+              "filter_faces", "finalize_ema", "targets_end", "ou_jitter")
 
     def step_profiled(self) -> dict:
         """One frame (no graph) with CUDA events between stages -> ms per stage."""

@@ -10,6 +10,7 @@ from __future__ import annotations
 from . import runtime
 
 _brownian_calls = 0
+_jitter_calls = 0
 
 
 def _t(x):
@@ -66,6 +67,35 @@ def apply_brownian_motion(pos, n, strength, domain_size):
     runtime.ctx().apply_brownian(_t(pos), n, strength, domain_size, runtime.config().SEED,
                                  _brownian_calls)
     _brownian_calls += 1
+
+
+def init_jitter_velocities(v_jit, n: int):
+    """dynamics.init_jitter_velocities (dynamics.py:600-605)."""
+    runtime.ctx().init_jitter_velocities(_t(v_jit), n)
+
+
+def compute_mean_radius(rad, n: int, mean_radius):
+    """dynamics.compute_mean_radius (dynamics.py:675-689) into the one-element
+    float32 tensor mean_radius (exact sum, rounded once)."""
+    runtime.ctx().compute_mean_radius(_t(rad), n, _t(mean_radius))
+
+
+def apply_brownian(v_jit, rad, mean_radius, n: int, dt: float):
+    """dynamics.apply_brownian (dynamics.py:607-646): OU update of v_jit with
+    JITTER_RMS / JITTER_TAU / MAX_DRIFT_FRACTION / GAP_FRACTION of the
+    configuration; the draws are Philox-4x32-10 keyed by the configured seed
+    and a per-call counter."""
+    global _jitter_calls
+    cfg = runtime.config()
+    runtime.ctx().apply_jitter(_t(v_jit), _t(rad), _t(mean_radius), n, dt, cfg.JITTER_RMS,
+                               cfg.JITTER_TAU, cfg.MAX_DRIFT_FRACTION, cfg.GAP_FRACTION,
+                               cfg.SEED, _jitter_calls)
+    _jitter_calls += 1
+
+
+def integrate_jitter(pos, v_jit, n: int, dt: float):
+    """dynamics.integrate_jitter (dynamics.py:649-660): pos = wrapP(pos + v dt)."""
+    runtime.ctx().integrate_jitter(_t(pos), _t(v_jit), n, dt)
 
 
 def alpha_for_frames(frames: int) -> float:

@@ -198,6 +198,25 @@ int fos_equilibrate_pressure(FosCtx* ctx, int n, int frame, float* rad, float* d
  * (seed, frame, particle) in place of ti.random(). */
 int fos_apply_brownian(FosCtx* ctx, float* pos, int n, float strength, float domain_size,
                        uint64_t seed, uint32_t frame, fos_stream_t s);
+/* OU jitter (dynamics.py:600-690).  The uniform draws U[-0.5, 0.5)^3 of
+ * ti.random() come from Philox-4x32-10 with counter (i, frame, 'OUJT', 0) and
+ * key = seed.
+ * init_jitter_velocities (dynamics.py:600-605): v_jit = 0. */
+int fos_init_jitter_velocities(FosCtx* ctx, float* v_jit, int n, fos_stream_t s);
+/* compute_mean_radius (dynamics.py:675-689) into a device float.  The sum is
+ * exact (each radius as a 2^-40 fixed-point integer, summed in 64 bits), so
+ * the result does not depend on the order of the additions. */
+int fos_compute_mean_radius(FosCtx* ctx, const float* rad, int n, float* mean_radius,
+                            fos_stream_t s);
+/* apply_brownian (dynamics.py:607-646): OU update of v_jit with the mean
+ * radius read from the device float mean_radius, capped per step at
+ * max_drift_fraction * gap_fraction * 2 r_i. */
+int fos_apply_jitter(FosCtx* ctx, float* v_jit, const float* rad, const float* mean_radius, int n,
+                     float dt, double jitter_rms, double jitter_tau, double max_drift_fraction,
+                     double gap_fraction, uint64_t seed, uint32_t frame, fos_stream_t s);
+/* integrate_jitter (dynamics.py:649-660): pos = wrapP(pos + v_jit * dt). */
+int fos_integrate_jitter(FosCtx* ctx, float* pos, const float* v_jit, int n, float dt,
+                         fos_stream_t s);
 /* set_fsc_targets (dynamics.py:1242-1320) */
 int fos_set_fsc_targets(FosCtx* ctx, const float* rad, float* rad_target, const int32_t* fsc,
                         const float* fsc_ema, int n, int f_low, int f_high, float growth_pct,
@@ -218,7 +237,7 @@ int fos_pressure_stats(FosCtx* ctx, int n, const float* rad, float* rmin, float*
  * One headless frame in run.py's order (run.py:699-1261): grid build; max
  * overlap; settle nudge while the device settle counter is > 0; `pressure_iters`
  * pressure sweeps on the last JFA's face_ids/fsc; Brownian jitter; pbd_iters x
- * {grid build; PBD}; grid build; and on a JFA frame run_jfa, the warm-start
+ * {grid build; PBD}; OU jitter when ou_jitter; grid build; and on a JFA frame run_jfa, the warm-start
  * gate (frame < warmstart_frames or zero-FSC fraction > zero_rate_thresh) and
  * set_fsc_targets + settle = adjustment_frames.  The frame index, settle
  * counter and gate live on the device, so a frame does no host sync and can be
@@ -239,6 +258,13 @@ typedef struct FosFrameParams {
     double brownian_strength;     /* BROWNIAN_STRENGTH (uniform +-strength per axis) */
     uint64_t seed;                /* Philox key of the Brownian jitter */
     int warmup_pbd;               /* PBD_BASE_PASSES used by fos_sim_init */
+    /* OU velocity jitter after the PBD sweeps (run.py:855-867), a second jitter
+     * channel next to the Brownian one; 0 = off.  Needs FosState.v_jit. */
+    int ou_jitter;                /* JITTER_ENABLED */
+    double jitter_rms;            /* JITTER_RMS: RMS drift per second, in mean radii */
+    double jitter_tau;            /* JITTER_TAU: OU time scale (s) */
+    double dt;                    /* DT: time step of the OU update (s) */
+    double max_drift_fraction;    /* MAX_DRIFT_FRACTION: step cap, in GAP_FRACTION*(2r) */
 } FosFrameParams;
 
 /* Caller-owned per-particle state (run.py's fields). */
@@ -252,6 +278,8 @@ typedef struct FosState {
     int32_t* cell_count;        /* [GRID_RES^3] */
     int32_t* cell_start;        /* [GRID_RES^3] */
     int32_t* cell_indices;      /* [n] */
+    float* v_jit;               /* [n][3] OU jitter velocity (run.py:151); may be NULL
+                                   unless FosFrameParams.ou_jitter */
 } FosState;
 
 void fos_frame_params_default(FosFrameParams* fp);
@@ -270,8 +298,8 @@ int fos_frame_graph(FosCtx* ctx, const FosState* st, const FosFrameParams* fp, i
  * stage_ms[FOS_FRAME_STAGES] receives milliseconds per stage: 0 hash-grid
  * builds, 1 max overlap, 2 settle nudge, 3 pressure sweeps, 4 Brownian, 5 PBD
  * sweeps, 6 JFA init + passes, 7 majority filter + faces, 8 finalize + EMA,
- * 9 targets + frame end. */
-#define FOS_FRAME_STAGES 10
+ * 9 targets + frame end, 10 OU jitter. */
+#define FOS_FRAME_STAGES 11
 int fos_frame_profile(FosCtx* ctx, const FosState* st, const FosFrameParams* fp, int jfa_frame,
                       float* stage_ms, fos_stream_t s);
 /* Tracing: the dynamics part of a plain frame (the persistent cooperative

@@ -517,6 +517,51 @@ void orc_brownian(float* pos, int n, float strength, float domain, uint64_t seed
     }
 }
 
+#define ORC_OU_STREAM 0x4f554a54u
+
+/* compute_mean_radius (dynamics.py:675-689) as run.py:860-861 uses it: the
+ * exact sum of the radii (each one a 2^-40 fixed-point integer), divided by
+ * max(1, n) in double and rounded once to float32. */
+float orc_mean_radius(const float* rad, int n) {
+    long long s = 0;
+    for (int i = 0; i < n; ++i) s += llrintf(rad[i] * 0x1p40f);
+    return (float)((double)s * 0x1p-40 / (double)(n > 1 ? n : 1));
+}
+
+/* apply_brownian + integrate_jitter (dynamics.py:607-660), the frame's step
+ * 6B (run.py:855-867).  ti.random() - 0.5 per axis is u - 0.5 with
+ * u = (x >> 8) * 2^-24 from Philox-4x32-10 (i, frame, 'OUJT', 0), key = seed.
+ * Python-level constants fold in double and round once to float32. */
+void orc_ou_jitter(float* pos, float* v_jit, const float* rad, int n, float mean_r, float dt,
+                   double rms, double tau, double max_drift, double gap, float L, float invL,
+                   uint64_t seed, uint32_t frame) {
+    const double t = tau > 1e-6 ? tau : 1e-6;
+    const float tau_f = (float)t, sq2 = (float)sqrt(2.0 / t), rms_f = (float)rms;
+    const float capk = (float)(max_drift * gap);
+    const float sigma = (rms_f * mean_r) * sq2;
+    const float kick = sigma * sqrtf(dt);
+    for (int i = 0; i < n; ++i) {
+        uint32_t c[4] = {(uint32_t)i, frame, ORC_OU_STREAM, 0u};
+        philox4x32_10(c, (uint32_t)seed, (uint32_t)(seed >> 32));
+        float v[3];
+        for (int d = 0; d < 3; ++d) {
+            float r = (float)(c[d] >> 8) * 0x1p-24f - 0.5f;
+            float vd = v_jit[3 * i + d];
+            v[d] = vd + ((-vd / tau_f) * dt + kick * r);
+        }
+        float cap = capk * (rad[i] + rad[i]);
+        float len = sqrtf(v[0] * v[0] + v[1] * v[1] + v[2] * v[2]) * dt;
+        if (len > cap) {
+            float sc = (cap / fmaxf(1e-6f, len)) / dt;
+            for (int d = 0; d < 3; ++d) v[d] = v[d] * sc;
+        }
+        for (int d = 0; d < 3; ++d) {
+            v_jit[3 * i + d] = v[d];
+            pos[3 * i + d] = grid_wrap(pos[3 * i + d] + v[d] * dt, L, invL);
+        }
+    }
+}
+
 /* smoothstep (dynamics.py:1226-1240) */
 static inline float smoothstep(float e0, float e1, float x) {
     float t = fminf(1.0f, fmaxf(0.0f, (x - e0) / (e1 - e0)));

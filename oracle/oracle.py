@@ -62,6 +62,9 @@ def lib():
             "orc_pressure": (_f, [_i, _i, _p, _p, _p, _p, _f, _f, _f, _i, _f, _f, _p]),
             "orc_philox": (None, [C.c_uint32] * 6 + [_p]),
             "orc_brownian": (None, [_p, _i, _f, _f, C.c_uint64, C.c_uint32]),
+            "orc_mean_radius": (_f, [_p, _i]),
+            "orc_ou_jitter": (None, [_p, _p, _p, _i, _f, _f, C.c_double, C.c_double, C.c_double,
+                                     C.c_double, _f, _f, C.c_uint64, C.c_uint32]),
             "orc_set_targets": (None, [_p, _p, _p, _p, _i, _i, _i, _f, _f, _f, _f]),
             "orc_nudge": (None, [_p, _p, _p, _i, _f, _f, _f, _f, _f, _i, _f]),
             "orc_num_threads": (_i, []),
@@ -128,6 +131,11 @@ class OracleParams:
     jfa_warm: int = 20
     jfa_cadence: int = 5
     warmup_pbd: int = 4               # PBD_BASE_PASSES
+    ou: bool = False                  # JITTER_ENABLED (config.py:493; off for the workloads)
+    jitter_rms: float = 0.10          # JITTER_RMS
+    jitter_tau: float = 1.0           # JITTER_TAU
+    dt: float = 0.016                 # DT
+    max_drift: float = 0.20           # MAX_DRIFT_FRACTION
 
     @property
     def G(self) -> int:
@@ -255,6 +263,20 @@ def brownian(pos, p: OracleParams, frame: int):
     lib().orc_brownian(_ptr(pos), p.n, _f32(p.brownian), _f32(p.L), int(p.seed), int(frame))
 
 
+def mean_radius(rad, n: int) -> float:
+    return float(lib().orc_mean_radius(_ptr(rad), int(n)))
+
+
+def ou_jitter(pos, v_jit, rad, p: OracleParams, frame: int):
+    """Frame step 6B (run.py:855-867): mean radius, apply_brownian,
+    integrate_jitter."""
+    m = mean_radius(rad, p.n)
+    lib().orc_ou_jitter(_ptr(pos), _ptr(v_jit), _ptr(rad), p.n, _f32(m), _f32(p.dt),
+                        float(p.jitter_rms), float(p.jitter_tau), float(p.max_drift),
+                        float(p.gap), _f32(p.L), p.invL, int(p.seed),
+                        int(frame))
+
+
 def set_targets(rad, rad_target, fsc, ema, p: OracleParams):
     lib().orc_set_targets(_ptr(rad), _ptr(rad_target), _ptr(fsc), _ptr(ema), p.n, p.f_low,
                           p.f_high, _f32(p.growth), _f32(p.r_min), _f32(p.r_max),
@@ -296,7 +318,7 @@ class OracleSim:
 
     Frame: (1) grid build; (2) max overlap; (3) settle nudge while settle > 0;
     (4) M pressure sweeps on the last JFA's face_ids/fsc; (5) Brownian jitter;
-    (6) K x {grid build; PBD}; (7) grid build; (8) on JFA frames: JFA, majority
+    (6) K x {grid build; PBD}; (6B) OU jitter when p.ou; (7) grid build; (8) on JFA frames: JFA, majority
     filter, faces, finalize, EMA, then the warm-start gate and set_fsc_targets.
     """
     p: OracleParams
@@ -313,6 +335,7 @@ class OracleSim:
     nl: np.ndarray = None
     used: np.ndarray = None
     lmd: np.ndarray = None
+    v_jit: np.ndarray = None
     labels: np.ndarray = None
     grid: tuple = None
     last: dict = field(default_factory=dict)
@@ -330,6 +353,7 @@ class OracleSim:
         self.nl = np.full((n, S), -1, np.int32)
         self.used = np.zeros(n, np.int32)
         self.lmd = np.zeros(n, np.float32)
+        self.v_jit = np.zeros((n, 3), np.float32)  # init_jitter_velocities (run.py:346)
 
     def initialize(self):
         """wrap_seeded_positions + warmup_pbd (run.py:233-318)."""
@@ -365,6 +389,8 @@ class OracleSim:
         for _ in range(p.pbd_iters):
             self.grid = grid_build(self.pos, p)
             self.pos = pbd(self.pos, self.rad, self.grid, p)
+        if p.ou:
+            ou_jitter(self.pos, self.v_jit, self.rad, p, f)
         self.grid = grid_build(self.pos, p)
         jfa_frame = p.is_jfa_frame(f)
         if jfa_frame:
