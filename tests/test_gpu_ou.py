@@ -35,7 +35,7 @@ def _case(n, seed, big=False):
 def test_standalone_kernels_match_oracle(big):
     n, seed = 20000, 0x55AA_0000_0003
     rms = 40.0 if big else 0.1
-    cfg = FosConfig(DOMAIN_SIZE=1.0, GRID_RES=16, SEED=seed, JITTER_RMS=rms,
+    cfg = FosConfig(DOMAIN_SIZE=1.0, GRID_RES=16, JFA_RES=64, SEED=seed, JITTER_RMS=rms,
                     MAX_PARTICLES=n)
     runtime.configure(cfg)
     runtime.init(max_particles=n, max_res=64)
