@@ -208,6 +208,7 @@ extern "C" int fos_ctx_create(const FosParams* p, int max_n, int max_res, int de
     ALLOC(c->stats_i, 64 * 4);
     ALLOC(c->ds, sizeof(FosDevState));
     ALLOC(c->fin_changed, FOS_FIN_MAXIT * sizeof(int));
+    ALLOC(c->skip_part, FOS_SKIP_BLOCKS * 64 + 256);
 #undef ALLOC
     if (cudaMallocHost(&c->pinned, 4096) != cudaSuccess) {
         fos_ctx_destroy(c);
@@ -261,7 +262,7 @@ extern "C" int fos_ctx_destroy(FosCtx* c) {
                     c->cellof, c->rank, c->cell_tmp, c->stats_f, c->stats_i, c->ds,
                     c->fin_changed, c->sorted, c->ci_tmp, c->coop_bsum, c->coop_cnt,
                     c->coop_part, c->coop_cnt2, c->coop_cfix, c->coop_idsort, c->coop_spfix,
-                    c->coop_slot};
+                    c->coop_slot, c->skip_part};
     for (void* q : ptrs)
         if (q) cudaFree(q);
     if (c->pinned) cudaFreeHost(c->pinned);

@@ -56,6 +56,8 @@ struct FosGraphKey {
 
 struct FosSurBufs;  // surrogate.cu
 
+#define FOS_SKIP_BLOCKS 1024
+
 struct FosCtx {
     int device = 0;
     int max_n = 0, max_res = 0;
@@ -110,6 +112,7 @@ struct FosCtx {
     FosDevState* ds = nullptr;
     int* fin_changed = nullptr;       // [FOS_FIN_MAXIT] per-sweep change flags of the finalize
     void* pinned = nullptr;           // small host staging buffer
+    void* skip_part = nullptr;        // fos_skip_signals: FOS_SKIP_BLOCKS partials + result
     FosSurBufs* sur = nullptr;        // FSC surrogate pair/inference buffers (first use)
     int sur_mode = FOS_SUR_ABSOLUTE;  // how surrogate frames use the model (fos.h)
     // graphs, indexed by jfa_frame + 2 * (surrogate frame)

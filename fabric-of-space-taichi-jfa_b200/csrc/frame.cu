@@ -5,7 +5,7 @@
 #include <math.h>
 #include <string.h>
 
-#include "fos_internal.cuh"
+#include "phases.cuh"
 
 // launchers defined in grid.cu / dynamics.cu
 int fos_grid_build_from(FosCtx* c, const float* src, float* dst, int n, int32_t* cell_count,
@@ -136,12 +136,26 @@ struct FrameProf {
     }
 };
 
+// part: bit 0 = dynamics (steps 1-7 and the OU jitter), bit 1 = measurement
+// (step 8 on a JFA frame) and the end of the frame.
+enum { FRAME_DYNAMICS = 1, FRAME_MEASURE = 2, FRAME_ALL = 3 };
 static int frame_impl(FosCtx* c, const FosState* st, const FosFrameParams* fp, int jfa_frame,
-                      cudaStream_t s, FrameProf* prof, const FosSurrogate* sur = nullptr);
+                      cudaStream_t s, FrameProf* prof, const FosSurrogate* sur = nullptr,
+                      int part = FRAME_ALL);
 
 extern "C" int fos_frame(FosCtx* c, const FosState* st, const FosFrameParams* fp, int jfa_frame,
                          fos_stream_t s) {
     return frame_impl(c, st, fp, jfa_frame, s, nullptr);
+}
+
+extern "C" int fos_frame_dynamics(FosCtx* c, const FosState* st, const FosFrameParams* fp,
+                                  fos_stream_t s) {
+    return frame_impl(c, st, fp, 0, s, nullptr, nullptr, FRAME_DYNAMICS);
+}
+
+extern "C" int fos_frame_measure(FosCtx* c, const FosState* st, const FosFrameParams* fp,
+                                 int jfa_frame, fos_stream_t s) {
+    return frame_impl(c, st, fp, jfa_frame, s, nullptr, nullptr, FRAME_MEASURE);
 }
 
 extern "C" int fos_frame_surrogate(FosCtx* c, const FosState* st, const FosFrameParams* fp,
@@ -175,14 +189,16 @@ extern "C" int fos_frame_profile(FosCtx* c, const FosState* st, const FosFramePa
 }
 
 static int frame_impl(FosCtx* c, const FosState* st, const FosFrameParams* fp, int jfa_frame,
-                      cudaStream_t s, FrameProf* prof, const FosSurrogate* sur) {
+                      cudaStream_t s, FrameProf* prof, const FosSurrogate* sur, int part) {
     int rc = check_state(c, st, fp);
     if (rc) return rc;
     const int n = st->n;
 #define MARK(id) \
     if (prof) prof->mark(id)
     const int* dframe = &c->ds->frame;
-    if (c->use_coop && !prof && fp->max_eq_nei <= 16 && !(fp->ou_jitter && fp->pbd_iters == 0) &&
+    if (!(part & FRAME_DYNAMICS)) {
+        // measurement part only
+    } else if (c->use_coop && !prof && fp->max_eq_nei <= 16 && !(fp->ou_jitter && fp->pbd_iters == 0) &&
         fos_coop_supported(c)) {
         // (1)-(7) as one persistent cooperative kernel (frame_coop.cu)
         rc = fos_frame_coop_dynamics(c, st, fp, s);
@@ -239,7 +255,8 @@ static int frame_impl(FosCtx* c, const FosState* st, const FosFrameParams* fp, i
                                  nullptr, s);
         if (rc) return rc;
         MARK(0);
-}
+    }
+    if (!(part & FRAME_MEASURE)) return FOS_OK;
     // surrogate frames: the learned FSC between JFA runs; on a JFA frame the
     // surrogate's estimate for the same positions, judged after the JFA
     if (sur && !jfa_frame) {
@@ -279,6 +296,135 @@ static int frame_impl(FosCtx* c, const FosState* st, const FosFrameParams* fp, i
     FOS_LAUNCHED(c);
     MARK(9);
 #undef MARK
+    return FOS_OK;
+}
+
+// ------------------------------------------------------------ temporal skip
+// Activity signals of run.py's temporal skip (run.py:913-951), one pass over
+// the particles.  Each block writes its partial sums to its own slot; one
+// thread adds the slots in block order, so the result does not depend on
+// scheduling.
+struct SkipPart {
+    long long rad_fx;     // sum of radii, 2^-40 fixed point (exact)
+    long long fsc_sum;
+    double dr_sum, dr_sq;  // sum of |dr| and |dr|^2
+    unsigned int vmax_bits;
+    int oob, zero, pad;
+};
+
+__global__ void __launch_bounds__(256) k_skip_partial(const float* __restrict__ pos,
+                                                      const float* __restrict__ rad,
+                                                      const float* __restrict__ pos_prev,
+                                                      const float* __restrict__ rad_prev,
+                                                      const int32_t* __restrict__ fsc, int n,
+                                                      int f_low, int f_high, float L, float halfL,
+                                                      SkipPart* part) {
+    long long rq = 0, fq = 0;
+    double ds = 0.0, dq = 0.0;
+    unsigned int vb = 0u;
+    int oob = 0, zero = 0;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const float r = __ldg(&rad[i]);
+        rq += rad_fixed(r);
+        const int f = __ldg(&fsc[i]);
+        fq += f;
+        oob += (f < f_low || f > f_high) ? 1 : 0;
+        zero += f == 0 ? 1 : 0;
+        if (rad_prev) {
+            const double a = (double)fabsf(fsub(r, __ldg(&rad_prev[i])));
+            ds += a;
+            dq += a * a;
+        }
+        if (pos_prev) {
+            // pos_delta with the periodic fold of run.py:933-935, then its norm
+            float d2 = 0.f;
+#pragma unroll
+            for (int k = 0; k < 3; ++k) {
+                float d = fsub(__ldg(&pos[3 * i + k]), __ldg(&pos_prev[3 * i + k]));
+                if (fabsf(d) > halfL) d = fsub(d, d > 0.f ? L : -L);
+                d2 = k == 0 ? fmul(d, d) : fadd(d2, fmul(d, d));
+            }
+            const unsigned int b = __float_as_uint(__fsqrt_rn(d2));
+            vb = b > vb ? b : vb;
+        }
+    }
+#pragma unroll
+    for (int o = 16; o >= 1; o >>= 1) {
+        rq += __shfl_xor_sync(0xffffffffu, rq, o);
+        fq += __shfl_xor_sync(0xffffffffu, fq, o);
+        ds += __shfl_xor_sync(0xffffffffu, ds, o);
+        dq += __shfl_xor_sync(0xffffffffu, dq, o);
+        oob += __shfl_xor_sync(0xffffffffu, oob, o);
+        zero += __shfl_xor_sync(0xffffffffu, zero, o);
+        unsigned int ob = __shfl_xor_sync(0xffffffffu, vb, o);
+        vb = ob > vb ? ob : vb;
+    }
+    __shared__ SkipPart sw[8];
+    const int w = threadIdx.x >> 5;
+    if ((threadIdx.x & 31) == 0) sw[w] = SkipPart{rq, fq, ds, dq, vb, oob, zero, 0};
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        SkipPart t = sw[0];
+        for (int k = 1; k < (int)(blockDim.x >> 5); ++k) {
+            t.rad_fx += sw[k].rad_fx;
+            t.fsc_sum += sw[k].fsc_sum;
+            t.dr_sum += sw[k].dr_sum;
+            t.dr_sq += sw[k].dr_sq;
+            t.vmax_bits = sw[k].vmax_bits > t.vmax_bits ? sw[k].vmax_bits : t.vmax_bits;
+            t.oob += sw[k].oob;
+            t.zero += sw[k].zero;
+        }
+        part[blockIdx.x] = t;
+    }
+}
+
+__global__ void k_skip_final(const SkipPart* part, int blocks, int n, int have_rad_prev,
+                             int have_pos_prev, FosSkipSignals* out) {
+    SkipPart t = part[0];
+    for (int k = 1; k < blocks; ++k) {
+        t.rad_fx += part[k].rad_fx;
+        t.fsc_sum += part[k].fsc_sum;
+        t.dr_sum += part[k].dr_sum;
+        t.dr_sq += part[k].dr_sq;
+        t.vmax_bits = part[k].vmax_bits > t.vmax_bits ? part[k].vmax_bits : t.vmax_bits;
+        t.oob += part[k].oob;
+        t.zero += part[k].zero;
+    }
+    const double dn = (double)(n > 1 ? n : 1);
+    out->n = n;
+    out->r_mean = (double)mean_from_fixed((unsigned long long)t.rad_fx, n);
+    if (have_rad_prev) {
+        const double m = t.dr_sum / dn;
+        const double var = t.dr_sq / dn - m * m;
+        out->sigma_dr = var > 0.0 ? sqrt(var) : 0.0;
+    } else {
+        out->sigma_dr = -1.0;
+    }
+    out->vmax_dt = have_pos_prev ? (double)__uint_as_float(t.vmax_bits) : -1.0;
+    out->fsc_mean = (double)t.fsc_sum / dn;
+    out->out_of_band = t.oob;
+    out->zero_fsc = t.zero;
+}
+
+extern "C" int fos_skip_signals(FosCtx* c, const FosState* st, const float* pos_prev,
+                                const float* rad_prev, int f_low, int f_high, FosSkipSignals* out,
+                                fos_stream_t s) {
+    FOS_REQUIRE(c && st && out && st->pos && st->rad, FOS_E_ARG, "NULL argument");
+    FOS_REQUIRE(st->n >= 1 && st->n <= c->max_n, FOS_E_CAPACITY, "state n outside [1, max_n]");
+    const int n = st->n;
+    int blocks = fos_blocks(n, 256);
+    if (blocks > FOS_SKIP_BLOCKS) blocks = FOS_SKIP_BLOCKS;
+    SkipPart* part = (SkipPart*)c->skip_part;
+    k_skip_partial<<<blocks, 256, 0, s>>>(st->pos, st->rad, pos_prev, rad_prev, c->fsc, n, f_low,
+                                          f_high, c->L, c->halfL, part);
+    FOS_LAUNCHED(c);
+    FosSkipSignals* dout = (FosSkipSignals*)(part + FOS_SKIP_BLOCKS);
+    k_skip_final<<<1, 1, 0, s>>>(part, blocks, n, rad_prev != nullptr, pos_prev != nullptr, dout);
+    FOS_LAUNCHED(c);
+    FosSkipSignals* h = (FosSkipSignals*)c->pinned;
+    FOS_CUDA(cudaMemcpyAsync(h, dout, sizeof(FosSkipSignals), cudaMemcpyDeviceToHost, s));
+    FOS_CUDA(cudaStreamSynchronize(s));
+    *out = *h;
     return FOS_OK;
 }
 

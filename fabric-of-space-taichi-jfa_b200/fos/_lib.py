@@ -81,6 +81,12 @@ class FosState(C.Structure):
         "cell_indices", "v_jit")]
 
 
+class FosSkipSignals(C.Structure):
+    _fields_ = [("n", C.c_int), ("out_of_band", C.c_int), ("zero_fsc", C.c_int),
+                ("pad", C.c_int), ("r_mean", C.c_double), ("sigma_dr", C.c_double),
+                ("vmax_dt", C.c_double), ("fsc_mean", C.c_double)]
+
+
 class FosSurrogateStats(C.Structure):
     _fields_ = [("pairs", C.c_int), ("overflow", C.c_int), ("judged", C.c_int),
                 ("exact", C.c_int), ("within1", C.c_int), ("stale_exact", C.c_int),
@@ -162,6 +168,10 @@ SIGNATURES = {
     "fos_sim_init": [_P, C.POINTER(FosState), C.POINTER(FosFrameParams), _I, _P],
     "fos_frame": [_P, C.POINTER(FosState), C.POINTER(FosFrameParams), _I, _P],
     "fos_frame_graph": [_P, C.POINTER(FosState), C.POINTER(FosFrameParams), _I, _P],
+    "fos_frame_dynamics": [_P, C.POINTER(FosState), C.POINTER(FosFrameParams), _P],
+    "fos_frame_measure": [_P, C.POINTER(FosState), C.POINTER(FosFrameParams), _I, _P],
+    "fos_skip_signals": [_P, C.POINTER(FosState), _P, _P, _I, _I, C.POINTER(FosSkipSignals),
+                         _P],
     "fos_frame_profile": [_P, C.POINTER(FosState), C.POINTER(FosFrameParams), _I,
                           C.POINTER(C.c_float), _P],
     "fos_frame_trace": [_P, C.POINTER(FosState), C.POINTER(FosFrameParams),

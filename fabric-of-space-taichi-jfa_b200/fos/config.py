@@ -64,6 +64,17 @@ class FosConfig:
     JITTER_TAU: float = 1.0               # config.py:496
     DT: float = 0.016                     # config.py:400
     MAX_DRIFT_FRACTION: float = 0.20      # config.py:498
+    # run.py's own JFA schedule (fos.headless): temporal skip and adaptive
+    # resolution (run.py:898-1068)
+    JFA_TEMPORAL_SKIP_ENABLED: bool = True  # config.py:200
+    TH_RSIGMA: float = 0.004              # config.py:201
+    TH_MARGIN_SAFE: float = 0.4           # config.py:202
+    TH_FSC_DRIFT: float = 0.05            # config.py:203
+    MAX_SKIP_FRAMES: int = 15             # config.py:204
+    JFA_WARMSTART_FRAMES: int = 30        # config.py:173
+    JFA_ADAPTIVE_ENABLED: bool = True     # config.py:163
+    JFA_VOXELS_PER_DIAMETER: float = 12.0  # config.py:164
+    JFA_VOXEL_SCALE: float = 2.8          # config.py:158
     # per-frame schedule of the headless driver
     PBD_ITERS: int = 4
     PRESSURE_ITERS: int = 1

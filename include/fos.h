@@ -309,6 +309,31 @@ int fos_frame_profile(FosCtx* ctx, const FosState* st, const FosFrameParams* fp,
  * number of stamps written (<= cap). */
 int fos_frame_trace(FosCtx* ctx, const FosState* st, const FosFrameParams* fp, long long* ns_host,
                     int cap, int* count, fos_stream_t s);
+/* The frame in two parts, for hosts that decide on the JFA after the
+ * dynamics, as run.py's temporal skip does (run.py:905-1018):
+ * fos_frame_dynamics runs steps 1-7 and the OU jitter; fos_frame_measure
+ * runs step 8 when jfa_frame, then ends the frame.  The two in sequence equal
+ * fos_frame. */
+int fos_frame_dynamics(FosCtx* ctx, const FosState* st, const FosFrameParams* fp,
+                       fos_stream_t s);
+int fos_frame_measure(FosCtx* ctx, const FosState* st, const FosFrameParams* fp, int jfa_frame,
+                      fos_stream_t s);
+/* Activity signals of the temporal skip (run.py:913-976) for the current
+ * state against the previous frame's positions and radii (either may be
+ * NULL: the signal is then -1).  Synchronises. */
+typedef struct FosSkipSignals {
+    int n;
+    int out_of_band;      /* particles with fsc < f_low or fsc > f_high */
+    int zero_fsc;         /* particles with fsc == 0 */
+    int pad;
+    double r_mean;        /* mean radius: exact sum, rounded once to float32 */
+    double sigma_dr;      /* population std of |rad - rad_prev| (double) */
+    double vmax_dt;       /* max |pos - pos_prev| with the periodic fold, float32 */
+    double fsc_mean;      /* mean fsc (exact sum) */
+} FosSkipSignals;
+int fos_skip_signals(FosCtx* ctx, const FosState* st, const float* pos_prev,
+                     const float* rad_prev, int f_low, int f_high, FosSkipSignals* out,
+                     fos_stream_t s);
 /* Device frame index and settle counter (synchronises). */
 int fos_sim_counters(FosCtx* ctx, int* frame, int* settle, fos_stream_t s);
 

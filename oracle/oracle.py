@@ -311,6 +311,110 @@ def num_threads() -> int:
     return int(lib().orc_num_threads())
 
 
+# ------------------------------------------------------- run.py's JFA schedule
+def skip_signals(pos_curr, pos_prev, rad_curr, rad_prev, fsc, L: float, f_low: int, f_high: int):
+    """The temporal-skip signals as run.py:913-976 computes them with numpy
+    (float32 arrays; pos_prev / rad_prev None on the first frame)."""
+    n = len(rad_curr)
+    out = {"n": n, "r_mean": float(rad_curr.mean()) if n > 0 else 0.0001}
+    if pos_prev is not None and rad_prev is not None:
+        dr_abs = np.abs(rad_curr - rad_prev)
+        out["sigma_dr"] = float(dr_abs.std())
+        d = pos_curr - pos_prev
+        d = np.where(np.abs(d) > L * 0.5, d - np.sign(d) * L, d)
+        out["vmax_dt"] = float(np.max(np.linalg.norm(d, axis=1)))
+    else:
+        out["sigma_dr"] = -1.0
+        out["vmax_dt"] = -1.0
+    out["fsc_mean"] = float(fsc.mean())
+    out["out_of_band"] = int(np.sum((fsc < f_low) | (fsc > f_high)))
+    out["zero_fsc"] = int(np.sum(fsc == 0))
+    return out
+
+
+@dataclass
+class SkipParams:
+    """config.py:158-204"""
+    enabled: bool = True              # JFA_TEMPORAL_SKIP_ENABLED
+    th_rsigma: float = 0.004          # TH_RSIGMA
+    th_margin: float = 0.4            # TH_MARGIN_SAFE
+    th_fsc_drift: float = 0.05        # TH_FSC_DRIFT
+    max_skip: int = 15                # MAX_SKIP_FRAMES
+    warm: int = 30                    # JFA_WARMSTART_FRAMES
+    adaptive: bool = True             # JFA_ADAPTIVE_ENABLED
+    vpd: float = 12.0                 # JFA_VOXELS_PER_DIAMETER
+    voxel_scale: float = 2.8          # JFA_VOXEL_SCALE
+    res_min: int = 192                # JFA_RES_MIN
+    res_max: int = 320                # JFA_RES_MAX
+
+
+class RunPySchedule:
+    """run.py:898-1018 restated: the per-frame JFA decision and its state."""
+
+    def __init__(self, sp: SkipParams):
+        self.sp = sp
+        self.jfa_frame_counter = 0
+        self.frames_since_jfa = 0
+        self.band_change_lockout = 0
+        self.last_fsc_mu = None
+        self.have_prev = False
+
+    def decide(self, sig) -> tuple[bool, str]:
+        sp = self.sp
+        self.jfa_frame_counter += 1
+        current_frame = self.jfa_frame_counter
+        self.frames_since_jfa += 1
+        r_mean = sig["r_mean"]
+        if self.have_prev:
+            sigma_dr_over_r = sig["sigma_dr"] / max(r_mean, 1e-9)
+            vmax_dt = sig["vmax_dt"]
+        else:
+            sigma_dr_over_r = 999.0
+            vmax_dt = 999.0
+        delta_fsc_mu = (abs(sig["fsc_mean"] - self.last_fsc_mu)
+                        if self.last_fsc_mu is not None else 999.0)
+        th_margin = sp.th_margin * r_mean
+        if self.band_change_lockout > 0:
+            self.band_change_lockout -= 1
+        t_warm = current_frame <= sp.warm
+        t_watch = self.frames_since_jfa >= sp.max_skip
+        t_band = self.band_change_lockout > 0
+        t_act = (sigma_dr_over_r > sp.th_rsigma or vmax_dt > th_margin
+                 or delta_fsc_mu > sp.th_fsc_drift)
+        t_oob = False
+        pct = 0.0
+        if self.frames_since_jfa > 1:
+            pct = float(sig["out_of_band"]) / float(max(1, sig["n"]))
+            t_oob = pct > 0.10
+        run = t_warm or t_watch or t_band or t_act or t_oob or not sp.enabled
+        reason = ""
+        if run:
+            if t_warm:
+                reason = "warm-start"
+            elif t_band:
+                reason = "band-change"
+            elif t_watch:
+                reason = "watchdog"
+            elif t_oob:
+                reason = f"out-of-band-guard ({pct * 100:.1f}%)"
+            elif t_act:
+                reason = "activity"
+            else:
+                reason = "fallback"
+            self.frames_since_jfa = 0
+        self.have_prev = True
+        return run, reason
+
+    def resolution(self, r_mean: float, L: float) -> int:
+        """run.py:1049-1068"""
+        sp = self.sp
+        if sp.adaptive:
+            res = int(round(L * sp.vpd / (2.0 * r_mean)))
+        else:
+            res = int(round(L / (sp.voxel_scale * r_mean)))
+        return max(sp.res_min, min(res, sp.res_max))
+
+
 # --------------------------------------------------------------- frame driver
 @dataclass
 class OracleSim:
@@ -376,7 +480,8 @@ class OracleSim:
         self.last["changes"] = ch
         self.last["passes"] = done
 
-    def step(self):
+    def dynamics(self):
+        """Steps (1)-(7) of a frame."""
         p, f = self.p, self.frame
         self.grid = grid_build(self.pos, p)
         o_max, self.lmd = max_overlap(self.pos, self.rad, self.grid, p)
@@ -392,7 +497,11 @@ class OracleSim:
         if p.ou:
             ou_jitter(self.pos, self.v_jit, self.rad, p, f)
         self.grid = grid_build(self.pos, p)
-        jfa_frame = p.is_jfa_frame(f)
+        self.last["o_max"] = o_max
+
+    def measure(self, jfa_frame: bool):
+        """Step (8) of a frame and its end."""
+        p, f = self.p, self.frame
         if jfa_frame:
             self.run_jfa()
             f0 = float(np.sum(self.fsc == 0)) / float(max(1, p.n))
@@ -401,5 +510,26 @@ class OracleSim:
                 set_targets(self.rad, self.rad_target, self.fsc, self.ema, p)
                 self.settle = p.adjust_frames
         self.last["jfa"] = jfa_frame
-        self.last["o_max"] = o_max
         self.frame += 1
+
+    def step_run_py(self, sched: RunPySchedule, state: dict) -> tuple[bool, str, int]:
+        """A frame with run.py's own JFA schedule: dynamics, signals against
+        the previous frame, decision, adaptive resolution, measurement.
+        ``state`` carries pos_prev / rad_prev between frames."""
+        p = self.p
+        self.dynamics()
+        sig = skip_signals(self.pos, state.get("pos_prev"), self.rad, state.get("rad_prev"),
+                           self.fsc, p.L, p.f_low, p.f_high)
+        run, reason = sched.decide(sig)
+        state["pos_prev"] = self.pos.copy()
+        state["rad_prev"] = self.rad.copy()
+        if run:
+            p.R = sched.resolution(sig["r_mean"], p.L)
+        self.measure(run)
+        if run and sched.sp.enabled:
+            sched.last_fsc_mu = float(self.fsc.mean())   # run.py:1083-1085
+        return run, reason, p.R
+
+    def step(self):
+        self.dynamics()
+        self.measure(self.p.is_jfa_frame(self.frame))
