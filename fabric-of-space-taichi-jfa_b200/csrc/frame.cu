@@ -496,6 +496,14 @@ static int frame_graph_impl(FosCtx* c, const FosState* st, const FosFrameParams*
     return FOS_OK;
 }
 
+extern "C" int fos_sim_set_counters(FosCtx* c, int frame, int settle, fos_stream_t s) {
+    FOS_REQUIRE(c != nullptr, FOS_E_ARG, "ctx is NULL");
+    FOS_REQUIRE(frame >= 0 && settle >= 0, FOS_E_ARG, "negative counter");
+    k_frame_set<<<1, 1, 0, s>>>(c->ds, frame, settle);
+    FOS_LAUNCHED(c);
+    return FOS_OK;
+}
+
 extern "C" int fos_sim_counters(FosCtx* c, int* frame, int* settle, fos_stream_t s) {
     FOS_REQUIRE(c != nullptr, FOS_E_ARG, "ctx is NULL");
     int* h = (int*)c->pinned;

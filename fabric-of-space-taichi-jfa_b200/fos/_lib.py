@@ -168,6 +168,7 @@ SIGNATURES = {
     "fos_sim_init": [_P, C.POINTER(FosState), C.POINTER(FosFrameParams), _I, _P],
     "fos_frame": [_P, C.POINTER(FosState), C.POINTER(FosFrameParams), _I, _P],
     "fos_frame_graph": [_P, C.POINTER(FosState), C.POINTER(FosFrameParams), _I, _P],
+    "fos_sim_set_counters": [_P, _I, _I, _P],
     "fos_frame_dynamics": [_P, C.POINTER(FosState), C.POINTER(FosFrameParams), _P],
     "fos_frame_measure": [_P, C.POINTER(FosState), C.POINTER(FosFrameParams), _I, _P],
     "fos_skip_signals": [_P, C.POINTER(FosState), _P, _P, _I, _I, C.POINTER(FosSkipSignals),

@@ -334,7 +334,9 @@ typedef struct FosSkipSignals {
 int fos_skip_signals(FosCtx* ctx, const FosState* st, const float* pos_prev,
                      const float* rad_prev, int f_low, int f_high, FosSkipSignals* out,
                      fos_stream_t s);
-/* Device frame index and settle counter (synchronises). */
+/* Device frame index and settle counter: set (a checkpoint resume; also
+ * clears the device error word) and read (synchronises). */
+int fos_sim_set_counters(FosCtx* ctx, int frame, int settle, fos_stream_t s);
 int fos_sim_counters(FosCtx* ctx, int* frame, int* settle, fos_stream_t s);
 
 /* ------------------------------------------------------------ FSC surrogate
