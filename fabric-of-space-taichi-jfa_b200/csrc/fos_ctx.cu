@@ -204,6 +204,7 @@ extern "C" int fos_ctx_create(const FosParams* p, int max_n, int max_res, int de
     ALLOC(c->cellof, (size_t)max_n * 4);
     ALLOC(c->rank, (size_t)max_n * 4);
     ALLOC(c->coop_slot, (size_t)max_n * 4);
+    ALLOC(c->pvol, (size_t)max_n * 8);
     ALLOC(c->stats_f, 64 * 4);
     ALLOC(c->stats_i, 64 * 4);
     ALLOC(c->ds, sizeof(FosDevState));
@@ -262,7 +263,7 @@ extern "C" int fos_ctx_destroy(FosCtx* c) {
                     c->cellof, c->rank, c->cell_tmp, c->stats_f, c->stats_i, c->ds,
                     c->fin_changed, c->sorted, c->ci_tmp, c->coop_bsum, c->coop_cnt,
                     c->coop_part, c->coop_cnt2, c->coop_cfix, c->coop_idsort, c->coop_spfix,
-                    c->coop_slot, c->skip_part};
+                    c->coop_slot, c->skip_part, c->pvol};
     for (void* q : ptrs)
         if (q) cudaFree(q);
     if (c->pinned) cudaFreeHost(c->pinned);

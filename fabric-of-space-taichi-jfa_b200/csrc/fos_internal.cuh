@@ -102,6 +102,7 @@ struct FosCtx {
     float4* coop_spfix = nullptr;     // [G^3 * COOP_CAP] (pos, rad) by cell row
     int coop_fixed = 0;               // the fixed-capacity rows are allocated
     int32_t* coop_slot = nullptr;     // [max_n] slot of each particle in the last rebuild
+    float* pvol = nullptr;            // [2 * max_n] r^P ping-pong of the pressure sweeps
     int32_t* coop_bsum = nullptr;     // [1024]
     int32_t* ci_tmp = nullptr;        // [max_n]
     int use_coop = 1;                 // plain-frame dynamics as one cooperative kernel

@@ -41,6 +41,8 @@ struct CoopArgs {
     int32_t* idsort;
     float4* spfix;
     int32_t* slot_of;
+    float* vol0;                // [n] r^P ping-pong of the pressure sweeps
+    float* vol1;
     int32_t* part;
     int32_t* bsum;
     float4* sp;
@@ -95,14 +97,21 @@ __global__ void __launch_bounds__(COOP_THREADS) k_frame_coop(CoopArgs a) {
     }
     if (!grid_barrier(a.ds, ep)) return;
     trace_mark(a, tk);
-    // (3) nudge_radii_adaptive_ema while settle_frames_left > 0 (run.py:744-750)
-    if (*((volatile int*)&a.ds->settle) > 0) {
-        float bg = back_global_from_bits(*((volatile unsigned int*)&a.ds->omax_bits),
-                                         a.contact_tol_d);
-        for (int i = tid; i < a.n; i += T)
-            a.rad[i] = nudge_one(__ldcg(&a.rad[i]), __ldcg(&a.rad_target[i]), __ldcg(&a.lmd[i]),
-                                 a.alpha, a.max_step, a.rmin, a.rmax, bg, a.bp_mode,
-                                 a.contact_tol);
+    // (3) nudge_radii_adaptive_ema while settle_frames_left > 0 (run.py:744-750);
+    // each final radius's power r^P seeds the pressure sweeps
+    {
+        const bool nudge = *((volatile int*)&a.ds->settle) > 0;
+        const float bg = back_global_from_bits(*((volatile unsigned int*)&a.ds->omax_bits),
+                                               a.contact_tol_d);
+        for (int i = tid; i < a.n; i += T) {
+            float r = __ldcg(&a.rad[i]);
+            if (nudge) {
+                r = nudge_one(r, __ldcg(&a.rad_target[i]), __ldcg(&a.lmd[i]), a.alpha,
+                              a.max_step, a.rmin, a.rmax, bg, a.bp_mode, a.contact_tol);
+                a.rad[i] = r;
+            }
+            if (a.sweeps > 0) a.vol0[i] = powf(r, a.pa.P);
+        }
     }
     if (!grid_barrier(a.ds, ep)) return;
     trace_mark(a, tk);
@@ -113,17 +122,22 @@ __global__ void __launch_bounds__(COOP_THREADS) k_frame_coop(CoopArgs a) {
     const int groups_per_round = T / 8;
     const int p_rounds = (a.n + groups_per_round - 1) / groups_per_round;
     // with one round (n <= T/8) each lane keeps its neighbours in registers
-    // for all sweeps: a sweep then waits for one round of radius loads
+    // for all sweeps, and particle i goes to block i % blocks, so every SM
+    // issues the same share of the sweep
     const bool keep_nbr = p_rounds == 1;
-    const PressureNbr nb0 = pressure_nbr8x2<LdL2>(tid / 8, lane, pa);
+    const int i_one = (int)(threadIdx.x >> 3) * (int)gridDim.x + (int)blockIdx.x;
+    const PressureNbr nb0 = pressure_nbr8x2<LdL2>(i_one, lane, pa);
     for (int w = 0; w < a.sweeps; ++w) {
         const float* rin = (w & 1) ? a.rad_tmp : a.rad;
         float* rout = (w & 1) ? a.rad : a.rad_tmp;
+        const float* vin = (w & 1) ? a.vol1 : a.vol0;
+        float* vout = (w & 1) ? a.vol0 : a.vol1;
         bool last = (w == a.sweeps - 1);
         for (int r = 0; r < p_rounds; ++r) {
-            int i = r * groups_per_round + tid / 8;
-            float d = keep_nbr ? pressure_sweep8x2<LdL2>(i, lane, pa, nb0, rin, rout, a.delta_r)
-                               : pressure_group8x2<LdL2>(i, lane, pa, rin, rout, a.delta_r);
+            const int i = keep_nbr ? i_one : r * groups_per_round + tid / 8;
+            const PressureNbr nb = keep_nbr ? nb0 : pressure_nbr8x2<LdL2>(i, lane, pa);
+            float d = pressure_sweep8x2v<LdL2>(i, lane, pa, nb, rin, vin, rout,
+                                               last ? nullptr : vout, a.delta_r);
             if (last) {
                 float ad = fabsf(d);
                 int ch = (i < a.n && (lane & 7) == 0) && ad > 1e-12f;
@@ -264,6 +278,8 @@ int fos_frame_coop_dynamics(FosCtx* c, const FosState* st, const FosFrameParams*
     a.idsort = c->coop_idsort;
     a.spfix = c->coop_spfix;
     a.slot_of = c->coop_slot;
+    a.vol0 = c->pvol;
+    a.vol1 = c->pvol + c->max_n;
     a.part = c->coop_part;
     a.bsum = c->coop_bsum;
     a.sp = c->sorted;

@@ -377,6 +377,57 @@ __device__ __forceinline__ float pressure_sweep8x2(int i, int lane, const Pressu
     return d;
 }
 
+// pressure_sweep8x2 with the particle powers V = r^P carried between sweeps:
+// vin[j] == powf(rin[j], P) for every j, so a neighbour costs one powf (its
+// new-radius term) instead of two, and lane 0 also writes vout[i] =
+// powf(rout[i], P) for the next sweep (vout may be NULL).  The result is
+// pressure_sweep8x2's bit for bit: the same powf of the same values.
+template <class LD>
+__device__ __forceinline__ float pressure_sweep8x2v(int i, int lane, const PressureArgs a,
+                                                    const PressureNbr& nb, const float* rin,
+                                                    const float* vin, float* rout, float* vout,
+                                                    float* delta_r) {
+    const int gl = lane & 7;
+    const int base_lane = lane & 24;
+    const unsigned int gmask = 0xffu << base_lane;
+    const bool live = i < a.n;
+    const float ri = live ? LD::ld(&rin[i]) : 0.f;
+    float d = 0.f;
+    if (nb.fc > 0) {
+        const float Vi = LD::ld(&vin[i]);
+        const float vj0 = nb.ok[0] ? LD::ld(&vin[nb.j[0]]) : 0.f;
+        const float vj1 = nb.ok[1] ? LD::ld(&vin[nb.j[1]]) : 0.f;
+        const float invP = fdiv(1.0f, a.P);
+        float term[2] = {0.f, 0.f};
+#pragma unroll
+        for (int h = 0; h < 2; ++h) {
+            if (nb.ok[h]) {
+                const float Vj = h == 0 ? vj0 : vj1;
+                const float dvr = fmul(a.k, fsub(Vi, Vj));
+                const float vmin = fminf(Vi, Vj);
+                const float dv = fmaxf(fmul(-a.cap, vmin), fminf(fmul(a.cap, vmin), dvr));
+                term[h] = fsub(powf(fsub(Vi, dv), invP), ri);
+            }
+        }
+#pragma unroll
+        for (int h = 0; h < 2; ++h) {
+            unsigned int m = (__ballot_sync(gmask, nb.ok[h]) & gmask) >> base_lane;
+            while (m) {
+                const int b = __ffs(m) - 1;
+                m &= m - 1;
+                d = fadd(d, __shfl_sync(gmask, term[h], b, 8));
+            }
+        }
+    }
+    if (live && gl == 0) {
+        delta_r[i] = d;
+        const float rn = fmaxf(a.rmin, fminf(a.rmax, fadd(ri, d)));
+        rout[i] = rn;
+        if (vout) vout[i] = powf(rn, a.P);
+    }
+    return d;
+}
+
 template <class LD>
 __device__ __forceinline__ float pressure_group8x2(int i, int lane, const PressureArgs a,
                                                    const float* rin, float* rout, float* delta_r) {
