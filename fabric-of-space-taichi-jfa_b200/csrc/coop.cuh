@@ -78,16 +78,17 @@ struct CoopLayout {
     __device__ __forceinline__ int count(int c) const { return __ldcg(&cc[c]); }
 };
 
-// P1 of a rebuild for one particle whose source position is v: wrap v into
-// dst[i], find its cell, take an arrival rank in the count buffer `par`
-// (all-zero before the first arrival) and drop the particle into slot rank
-// of the cell's fixed-capacity row (a full row sets overflow bit par, and
-// the rebuild then takes the CSR form).  A phase that produces particle i's
-// new position can run this for the next rebuild right away, so that rebuild
-// needs no P1 phase or barrier of its own.
+// P1 of a rebuild for one particle whose source position is v and radius r:
+// wrap v into dst[i], find its cell, take an arrival rank in the count
+// buffer `par` (all-zero before the first arrival) and drop the particle into
+// slot rank of the cell's fixed-capacity rows: its index into cfix and its
+// (wrapped position, radius) into spst, so the row sort needs no gather (a
+// full row sets overflow bit par, and the rebuild then takes the CSR form).
+// A phase that produces particle i's new position can run this for the next
+// rebuild right away, so that rebuild needs no P1 phase or barrier of its own.
 template <class Args, class Geo>
 __device__ __forceinline__ void coop_p1_val(const Args& a, const Geo& geo, int i, float3 v,
-                                            float* dst, int par) {
+                                            float r, float* dst, int par) {
     float wx = grid_wrap(v.x, geo.L, geo.invL);
     float wy = grid_wrap(v.y, geo.L, geo.invL);
     float wz = grid_wrap(v.z, geo.L, geo.invL);
@@ -96,26 +97,27 @@ __device__ __forceinline__ void coop_p1_val(const Args& a, const Geo& geo, int i
     dst[3 * i + 2] = wz;
     int c = geo.cell(i, wx, wy, wz);
     a.cellof[i] = c;
-    int r = atomicAdd(&(par ? a.cnt2 : a.cnt)[c], 1);
-    a.rank[i] = r;
+    int k = atomicAdd(&(par ? a.cnt2 : a.cnt)[c], 1);
+    a.rank[i] = k;
     if (a.cfix) {
-        if (r < COOP_CAP) a.cfix[(size_t)c * COOP_CAP + r] = i;
-        else atomicOr(&a.ds->grid_ovf, 1 << par);
+        if (k < COOP_CAP) {
+            const size_t slot = (size_t)c * COOP_CAP + k;
+            a.cfix[slot] = i;
+            a.spst[slot] = make_float4(wx, wy, wz, r);
+        } else {
+            atomicOr(&a.ds->grid_ovf, 1 << par);
+        }
     }
 }
 
 template <class Args, class Geo>
 __device__ __forceinline__ void coop_p1_one(const Args& a, const Geo& geo, int i, const float* src,
-                                            float* dst, int par) {
+                                            const float* rad, float* dst, int par) {
     float3 v = make_float3(__ldcg(&src[3 * i + 0]), __ldcg(&src[3 * i + 1]),
                            __ldcg(&src[3 * i + 2]));
-    coop_p1_val(a, geo, i, v, dst, par);
+    coop_p1_val(a, geo, i, v, rad ? __ldcg(&rad[i]) : 0.f, dst, par);
 }
 
-// Deferred P1 for a warp's PBD results: the warp's q-th particle goes to
-// lane q % 32 by shuffle, and the lanes run coop_p1_val together every 32
-// particles, so the cell atomics of a warp's particles cost one round trip,
-// not one per particle.
 // With ou != NULL each deferred particle first takes the frame's OU jitter
 // step (apply_brownian + integrate_jitter, run.py:855-867) at its new
 // position, which is what the rebuild after the last PBD sweep then sees.
@@ -130,19 +132,20 @@ struct OuStep {
 
 struct P1Defer {
     int i = -1;
-    float3 v;
+    float4 v;  // new position, radius
     int q = 0;
     template <class Args, class Geo>
-    __device__ __forceinline__ void put(const Args& a, const Geo& geo, int lane, int pi, float3 pv,
+    __device__ __forceinline__ void put(const Args& a, const Geo& geo, int lane, int pi, float4 pv,
                                         float* dst, int par, const OuStep* ou = nullptr) {
         const int slot = q & 31;
         const int si = __shfl_sync(0xffffffffu, pi, 0);
         const float sx = __shfl_sync(0xffffffffu, pv.x, 0);
         const float sy = __shfl_sync(0xffffffffu, pv.y, 0);
         const float sz = __shfl_sync(0xffffffffu, pv.z, 0);
+        const float sr = __shfl_sync(0xffffffffu, pv.w, 0);
         if (lane == slot) {
             i = si;
-            v = make_float3(sx, sy, sz);
+            v = make_float4(sx, sy, sz, sr);
         }
         ++q;
         if (slot == 31) flush(a, geo, dst, par, ou);
@@ -151,10 +154,11 @@ struct P1Defer {
     __device__ __forceinline__ void flush(const Args& a, const Geo& geo, float* dst, int par,
                                           const OuStep* ou = nullptr) {
         if (i >= 0) {
+            float3 p = make_float3(v.x, v.y, v.z);
             if (ou)
-                v = ou_one(i, (unsigned int)(i - ou->ctr_base), v, ou->vjit, __ldcg(&ou->rad[i]),
-                           ou->kick, ou->o, ou->frame);
-            coop_p1_val(a, geo, i, v, dst, par);
+                p = ou_one(i, (unsigned int)(i - ou->ctr_base), p, ou->vjit, v.w, ou->kick, ou->o,
+                           ou->frame);
+            coop_p1_val(a, geo, i, p, v.w, dst, par);
         }
         i = -1;
     }
@@ -187,7 +191,7 @@ __device__ bool coop_grid(const Args& a, const Geo& geo, const float* src, float
     int32_t* cnt = par ? a.cnt2 : a.cnt;
     int32_t* cnt_next = par ? a.cnt : a.cnt2;
     if (!p1_done) {
-        for (int i = tid; i < a.n; i += T) coop_p1_one(a, geo, i, src, dst, par);
+        for (int i = tid; i < a.n; i += T) coop_p1_one(a, geo, i, src, rad, dst, par);
         if (!grid_barrier(a.ds, ep)) return false;
         trace_mark(a, tk);
     }
@@ -195,20 +199,34 @@ __device__ bool coop_grid(const Args& a, const Geo& geo, const float* src, float
     for (int c = tid; c < a.G3; c += T) cnt_next[c] = 0;
     if (tid == 0) atomicAnd(&a.ds->grid_ovf, ~(1 << (par ^ 1)));
     if (a.cfix && !want_csr && !ovf && rad) {
-        // fixed-capacity rows: sort each cell's (<= COOP_CAP) arrivals by index
+        // fixed-capacity rows: sort each cell's (<= COOP_CAP) arrivals by
+        // index.  A warp takes two cells per round and loads both rows whole
+        // (slots past the count hold stale entries and are ignored) together
+        // with the counts, so a round waits for one load latency.
         const int lane = threadIdx.x & 31, W = T >> 5, wid = tid >> 5;
-        for (int c = wid; c < a.G3; c += W) {
-            const int m = __ldcg(&cnt[c]);  // warp-uniform, <= COOP_CAP
-            if (m == 0) continue;
-            const size_t base = (size_t)c * COOP_CAP;
-            const int id = lane < m ? __ldcg(&a.cfix[base + lane]) : 0x7fffffff;
-            int r = 0;
-            for (int k = 0; k < m; ++k) r += __shfl_sync(0xffffffffu, id, k) < id;
-            if (lane < m) {
-                a.idsort[base + r] = id;
-                a.spfix[base + r] = make_float4(__ldcg(&dst[3 * id + 0]), __ldcg(&dst[3 * id + 1]),
-                                                __ldcg(&dst[3 * id + 2]), __ldcg(&rad[id]));
-                a.slot_of[id] = (int)(base + r);
+        for (int c0 = wid; c0 < a.G3; c0 += 2 * W) {
+            const int cc2[2] = {c0, c0 + W};
+            int m[2], id[2];
+            float4 pr[2];
+#pragma unroll
+            for (int h = 0; h < 2; ++h) {
+                const bool ok = cc2[h] < a.G3;  // warp-uniform
+                const size_t base = (size_t)(ok ? cc2[h] : 0) * COOP_CAP;
+                m[h] = ok ? __ldcg(&cnt[cc2[h]]) : 0;  // <= COOP_CAP
+                id[h] = ok ? __ldcg(&a.cfix[base + lane]) : 0;
+                pr[h] = ok ? __ldcg(&a.spst[base + lane]) : make_float4(0.f, 0.f, 0.f, 0.f);
+            }
+#pragma unroll
+            for (int h = 0; h < 2; ++h) {
+                const int key = lane < m[h] ? id[h] : 0x7fffffff;
+                int r = 0;
+                for (int k = 0; k < m[h]; ++k) r += __shfl_sync(0xffffffffu, key, k) < key;
+                if (lane < m[h]) {
+                    const size_t base = (size_t)cc2[h] * COOP_CAP;
+                    a.idsort[base + r] = key;
+                    a.spfix[base + r] = pr[h];
+                    a.slot_of[key] = (int)(base + r);
+                }
             }
         }
         if (out) *out = CoopLayout{a.idsort, a.spfix, nullptr, cnt, COOP_CAP};

@@ -279,6 +279,7 @@ struct EnsArgs {
     int32_t* cfix;
     int32_t* idsort;
     float4* spfix;
+    float4* spst;
     int32_t* slot_of;
     int32_t* part;
     int32_t* bsum;
@@ -320,7 +321,7 @@ __device__ __forceinline__ void ens_pbd(const EnsArgs& a, const EnsGeo& geo, con
         if (i < a.n) {  // warp-uniform
             const EnsFoamDev& d = a.F[a.foam_of[i]];
             const GridGeom g{d.G, a.L, a.invL, a.halfL};
-            float3 nv = make_float3(0.f, 0.f, 0.f);
+            float4 nv = make_float4(0.f, 0.f, 0.f, 0.f);
             int pi = pbd_warp<LdL2>(kk, lane, lay.sp, lay.ci, a.pos_tmp, g,
                                     lay.cs ? lay.cs + d.cell_off : nullptr, lay.cc + d.cell_off,
                                     a.gap1, a.mdf, a.dmul, &nv, lay.cap, d.cell_off);
@@ -421,7 +422,7 @@ __global__ void __launch_bounds__(THREADS) k_ens_coop(EnsArgs a) {
         const EnsFoamDev& d = a.F[a.foam_of[i]];
         brownian_one<LdL2>(i, (unsigned int)(i - d.part_off), a.pos, a.strength, a.domain, a.halfL,
                            d.k0, d.k1, (unsigned int)frame);
-        coop_p1_one(a, geo, i, a.pos, a.pos, gk & 1);
+        coop_p1_one(a, geo, i, a.pos, a.rad, a.pos, gk & 1);
     }
     for (int f = tid; f < a.nf; f += T)
         if (a.W[f].settle > 0) a.W[f].settle -= 1;
@@ -702,6 +703,7 @@ static int ens_coop_launch(FosEnsemble* e, int mode, cudaStream_t s) {
     a.cfix = c->coop_fixed ? c->coop_cfix : nullptr;
     a.idsort = c->coop_idsort;
     a.spfix = c->coop_spfix;
+    a.spst = c->coop_spst;
     a.slot_of = c->coop_slot;
     a.part = c->coop_part;
     a.bsum = c->coop_bsum;

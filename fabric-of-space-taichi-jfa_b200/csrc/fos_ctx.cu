@@ -98,20 +98,21 @@ static int alloc_cells(FosCtx* c) {
         if (*b) cudaFree(*b);
         *b = nullptr;
     }
-    void* rows[3] = {c->coop_cfix, c->coop_idsort, c->coop_spfix};
+    void* rows[4] = {c->coop_cfix, c->coop_idsort, c->coop_spfix, c->coop_spst};
     for (void* q : rows)
         if (q) cudaFree(q);
     c->coop_cfix = c->coop_idsort = nullptr;
-    c->coop_spfix = nullptr;
+    c->coop_spfix = c->coop_spst = nullptr;
     c->coop_fixed = 0;
     for (int32_t** b : bufs) FOS_CUDA(cudaMalloc((void**)b, need * sizeof(int32_t)));
     FOS_CUDA(cudaMemset(c->coop_cnt, 0, need * sizeof(int32_t)));
     FOS_CUDA(cudaMemset(c->coop_cnt2, 0, need * sizeof(int32_t)));
     const size_t slots = need * 32;
-    if (slots * (4 + 4 + sizeof(float4)) <= FOS_COOP_FIXED_MAX_BYTES) {
+    if (slots * (4 + 4 + 2 * sizeof(float4)) <= FOS_COOP_FIXED_MAX_BYTES) {
         FOS_CUDA(cudaMalloc((void**)&c->coop_cfix, slots * 4));
         FOS_CUDA(cudaMalloc((void**)&c->coop_idsort, slots * 4));
         FOS_CUDA(cudaMalloc((void**)&c->coop_spfix, slots * sizeof(float4)));
+        FOS_CUDA(cudaMalloc((void**)&c->coop_spst, slots * sizeof(float4)));
         c->coop_fixed = 1;
     }
     c->cell_tmp_n = need;
@@ -263,6 +264,7 @@ extern "C" int fos_ctx_destroy(FosCtx* c) {
                     c->cellof, c->rank, c->cell_tmp, c->stats_f, c->stats_i, c->ds,
                     c->fin_changed, c->sorted, c->ci_tmp, c->coop_bsum, c->coop_cnt,
                     c->coop_part, c->coop_cnt2, c->coop_cfix, c->coop_idsort, c->coop_spfix,
+                    c->coop_spst,
                     c->coop_slot, c->skip_part, c->pvol};
     for (void* q : ptrs)
         if (q) cudaFree(q);

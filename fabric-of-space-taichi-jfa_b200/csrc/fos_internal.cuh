@@ -100,6 +100,7 @@ struct FosCtx {
     int32_t* coop_cnt2 = nullptr;     // [G^3] second count buffer (rebuilds alternate)
     int32_t *coop_cfix = nullptr, *coop_idsort = nullptr;  // [G^3 * COOP_CAP] cell rows
     float4* coop_spfix = nullptr;     // [G^3 * COOP_CAP] (pos, rad) by cell row
+    float4* coop_spst = nullptr;      // [G^3 * COOP_CAP] (pos, rad) in arrival order
     int coop_fixed = 0;               // the fixed-capacity rows are allocated
     int32_t* coop_slot = nullptr;     // [max_n] slot of each particle in the last rebuild
     float* pvol = nullptr;            // [2 * max_n] r^P ping-pong of the pressure sweeps

@@ -40,6 +40,7 @@ struct CoopArgs {
     int32_t* cfix;
     int32_t* idsort;
     float4* spfix;
+    float4* spst;
     int32_t* slot_of;
     float* vol0;                // [n] r^P ping-pong of the pressure sweeps
     float* vol1;
@@ -163,7 +164,7 @@ __global__ void __launch_bounds__(COOP_THREADS) k_frame_coop(CoopArgs a) {
             if (a.ou) rq += rad_fixed(__ldcg(&a.rad[i]));
             brownian_one<LdL2>(i, (unsigned int)i, a.pos, a.strength, a.domain, a.halfL, a.k0,
                                a.k1, frame);
-            coop_p1_one(a, geo, i, a.pos, a.pos, gk & 1);
+            coop_p1_one(a, geo, i, a.pos, a.rad, a.pos, gk & 1);
         }
         if (a.ou) {
 #pragma unroll
@@ -197,7 +198,7 @@ __global__ void __launch_bounds__(COOP_THREADS) k_frame_coop(CoopArgs a) {
             const int kk = kk_next;
             kk_next = i + W < a.n ? __ldcg(&a.slot_of[i + W]) : 0;
             if (i < a.n) {  // warp-uniform
-                float3 nv = make_float3(0.f, 0.f, 0.f);
+                float4 nv = make_float4(0.f, 0.f, 0.f, 0.f);
                 int pi = pbd_warp<LdL2>(kk, lane, lay.sp, lay.ci, a.pos_tmp, a.g, lay.cs, lay.cc,
                                         a.gap1, a.mdf, a.dmul, &nv, lay.cap);
                 p1.put(a, geo, lane, pi, nv, a.pos, gk & 1, ou_here ? &ous : nullptr);
@@ -277,6 +278,7 @@ int fos_frame_coop_dynamics(FosCtx* c, const FosState* st, const FosFrameParams*
     a.cfix = c->coop_fixed ? c->coop_cfix : nullptr;
     a.idsort = c->coop_idsort;
     a.spfix = c->coop_spfix;
+    a.spst = c->coop_spst;
     a.slot_of = c->coop_slot;
     a.vol0 = c->pvol;
     a.vol1 = c->pvol + c->max_n;

@@ -123,6 +123,57 @@ struct GridGeom {
     float L, invL, halfL;
 };
 
+// Correction of project_overlaps (dynamics.py:120-160) from candidate q on a
+// particle at p with radius ri (md = mdf * ri); false when they do not overlap.
+__device__ __forceinline__ bool pbd_term(float4 q, float px, float py, float pz, float ri,
+                                         float md, float gap1, const GridGeom& g, float& vx,
+                                         float& vy, float& vz) {
+    float ddx = grid_wrap(fsub(q.x, px), g.L, g.invL);
+    float ddy = grid_wrap(fsub(q.y, py), g.L, g.invL);
+    float ddz = grid_wrap(fsub(q.z, pz), g.L, g.invL);
+    float d2 = fadd(fadd(fadd(fmul(ddx, ddx), fmul(ddy, ddy)), fmul(ddz, ddz)), 1e-12f);
+    float dist = __fsqrt_rn(d2);
+    float tsep = fmul(fadd(ri, q.w), gap1);
+    if (!(dist < tsep)) return false;
+    float ov = fsub(tsep, dist);
+    float ux = fdiv(ddx, dist), uy = fdiv(ddy, dist), uz = fdiv(ddz, dist);
+    float mag = fminf(fmul(ov, 0.5f), md);
+    vx = fmaxf(-md, fminf(md, fmul(-ux, mag)));
+    vy = fmaxf(-md, fminf(md, fmul(-uy, mag)));
+    vz = fmaxf(-md, fminf(md, fmul(-uz, mag)));
+    return true;
+}
+
+// Adds the hits' corrections in lane order (candidate order).  All 32 lanes.
+__device__ __forceinline__ void warp_ordered_add3(bool hit, float vx, float vy, float vz,
+                                                  float& cx, float& cy, float& cz) {
+    unsigned int m = __ballot_sync(0xffffffffu, hit);
+    while (m) {
+        int b = __ffs(m) - 1;
+        m &= m - 1;
+        cx = fadd(cx, __shfl_sync(0xffffffffu, vx, b));
+        cy = fadd(cy, __shfl_sync(0xffffffffu, vy, b));
+        cz = fadd(cz, __shfl_sync(0xffffffffu, vz, b));
+    }
+}
+
+// End of project_overlaps for one particle (dynamics.py:160-171): cap the
+// summed correction at mdf * ri * dmul and return the wrapped new position.
+__device__ __forceinline__ float3 pbd_move(float px, float py, float pz, float ri, float cx,
+                                           float cy, float cz, float mdf, float dmul,
+                                           const GridGeom& g) {
+    float mt = fmul(fmul(mdf, ri), dmul);
+    float cm = __fsqrt_rn(fadd(fadd(fmul(cx, cx), fmul(cy, cy)), fmul(cz, cz)));
+    if (cm > mt) {
+        float sc = fdiv(mt, cm);
+        cx = fmul(cx, sc);
+        cy = fmul(cy, sc);
+        cz = fmul(cz, sc);
+    }
+    return make_float3(grid_wrap(fadd(px, cx), g.L, g.invL), grid_wrap(fadd(py, cy), g.L, g.invL),
+                       grid_wrap(fadd(pz, cz), g.L, g.invL));
+}
+
 // project_overlaps (dynamics.py:77-171) for the particle at sorted position
 // kk, as one Jacobi sweep: reads the pre-sweep positions (the cell-ordered
 // copy sp holds pos and rad) and writes pout[i].  The whole warp cooperates:
@@ -130,13 +181,13 @@ struct GridGeom {
 // pairs are added in candidate order, so the FP32 sum is the reference loop's
 // sum bit for bit.  Must be called by all 32 lanes.
 // Returns particle i to lane 0 (-1 to the other lanes); with np != NULL,
-// lane 0 also gets the new (wrapped) position in *np.  cap / cell_base as in
-// stencil_ranges.
+// lane 0 also gets the new (wrapped) position and the radius in *np.
+// cap / cell_base as in stencil_ranges.
 template <class LD>
 __device__ __forceinline__ int pbd_warp(int kk, int lane, const float4* sp, const int32_t* ci,
                                         float* pout, const GridGeom g, const int32_t* cs,
                                         const int32_t* cc, float gap1, float mdf, float dmul,
-                                        float3* np = nullptr, int cap = 0, int cell_base = 0) {
+                                        float4* np = nullptr, int cap = 0, int cell_base = 0) {
     float4 me = LD::ld(&sp[kk]);
     float px = me.x, py = me.y, pz = me.z, ri = me.w;
     Stencil r = stencil_ranges<LD>(px, py, pz, g.L, g.invL, g.halfL, g.G, cs, cc, lane, cap,
@@ -148,53 +199,31 @@ __device__ __forceinline__ int pbd_warp(int kk, int lane, const float4* sp, cons
         int k = stencil_locate(r, t < r.total ? t : r.total - 1);
         bool hit = false;
         float vx = 0.f, vy = 0.f, vz = 0.f;
-        if (t < r.total && k != kk) {
-            float4 q = LD::ld(&sp[k]);
-            float ddx = grid_wrap(fsub(q.x, px), g.L, g.invL);
-            float ddy = grid_wrap(fsub(q.y, py), g.L, g.invL);
-            float ddz = grid_wrap(fsub(q.z, pz), g.L, g.invL);
-            float d2 = fadd(fadd(fadd(fmul(ddx, ddx), fmul(ddy, ddy)), fmul(ddz, ddz)), 1e-12f);
-            float dist = __fsqrt_rn(d2);
-            float tsep = fmul(fadd(ri, q.w), gap1);
-            if (dist < tsep) {
-                hit = true;
-                float ov = fsub(tsep, dist);
-                float ux = fdiv(ddx, dist), uy = fdiv(ddy, dist), uz = fdiv(ddz, dist);
-                float mag = fminf(fmul(ov, 0.5f), md);
-                vx = fmaxf(-md, fminf(md, fmul(-ux, mag)));
-                vy = fmaxf(-md, fminf(md, fmul(-uy, mag)));
-                vz = fmaxf(-md, fminf(md, fmul(-uz, mag)));
-            }
-        }
-        unsigned int m = __ballot_sync(0xffffffffu, hit);
-        while (m) {
-            int b = __ffs(m) - 1;
-            m &= m - 1;
-            cx = fadd(cx, __shfl_sync(0xffffffffu, vx, b));
-            cy = fadd(cy, __shfl_sync(0xffffffffu, vy, b));
-            cz = fadd(cz, __shfl_sync(0xffffffffu, vz, b));
-        }
+        if (t < r.total && k != kk)
+            hit = pbd_term(LD::ld(&sp[k]), px, py, pz, ri, md, gap1, g, vx, vy, vz);
+        warp_ordered_add3(hit, vx, vy, vz, cx, cy, cz);
     }
     if (lane == 0) {
-        float mt = fmul(fmul(mdf, ri), dmul);
-        float cm = __fsqrt_rn(fadd(fadd(fmul(cx, cx), fmul(cy, cy)), fmul(cz, cz)));
-        if (cm > mt) {
-            float sc = fdiv(mt, cm);
-            cx = fmul(cx, sc);
-            cy = fmul(cy, sc);
-            cz = fmul(cz, sc);
-        }
         int i = LD::ld(&ci[kk]);
-        const float nx = grid_wrap(fadd(px, cx), g.L, g.invL);
-        const float ny = grid_wrap(fadd(py, cy), g.L, g.invL);
-        const float nz = grid_wrap(fadd(pz, cz), g.L, g.invL);
-        pout[3 * i + 0] = nx;
-        pout[3 * i + 1] = ny;
-        pout[3 * i + 2] = nz;
-        if (np) *np = make_float3(nx, ny, nz);
+        const float3 n3 = pbd_move(px, py, pz, ri, cx, cy, cz, mdf, dmul, g);
+        pout[3 * i + 0] = n3.x;
+        pout[3 * i + 1] = n3.y;
+        pout[3 * i + 2] = n3.z;
+        if (np) *np = make_float4(n3.x, n3.y, n3.z, ri);
         return i;
     }
     return -1;
+}
+
+// Deepest overlap of candidate q below a particle at `me` (dynamics.py:330-345).
+__device__ __forceinline__ float maxov_term(float4 q, float4 me, float eps, const GridGeom& g) {
+    float ddx = grid_wrap(fsub(q.x, me.x), g.L, g.invL);
+    float ddy = grid_wrap(fsub(q.y, me.y), g.L, g.invL);
+    float ddz = grid_wrap(fsub(q.z, me.z), g.L, g.invL);
+    float dist =
+        __fsqrt_rn(fadd(fadd(fadd(fmul(ddx, ddx), fmul(ddy, ddy)), fmul(ddz, ddz)), eps));
+    float td = fadd(me.w, q.w);
+    return dist < td ? fsub(td, dist) : 0.f;
 }
 
 // compute_local_max_overlaps (dynamics.py:304-352) for the particle at
@@ -215,16 +244,7 @@ __device__ __forceinline__ unsigned int maxov_warp(int kk, int lane, const float
         int k = stencil_locate(r, t < r.total ? t : r.total - 1);
         if (t < r.total) {
             int j = LD::ld(&ci[k]);
-            if (i < j) {
-                float4 q = LD::ld(&sp[k]);
-                float ddx = grid_wrap(fsub(q.x, me.x), g.L, g.invL);
-                float ddy = grid_wrap(fsub(q.y, me.y), g.L, g.invL);
-                float ddz = grid_wrap(fsub(q.z, me.z), g.L, g.invL);
-                float dist = __fsqrt_rn(
-                    fadd(fadd(fadd(fmul(ddx, ddx), fmul(ddy, ddy)), fmul(ddz, ddz)), eps));
-                float td = fadd(me.w, q.w);
-                if (dist < td) lm = fmaxf(lm, fsub(td, dist));
-            }
+            if (i < j) lm = fmaxf(lm, maxov_term(LD::ld(&sp[k]), me, eps, g));
         }
     }
     unsigned int b = __reduce_max_sync(0xffffffffu, __float_as_uint(lm));
