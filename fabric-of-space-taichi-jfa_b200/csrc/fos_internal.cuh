@@ -228,6 +228,14 @@ __device__ __forceinline__ int wrap_small(int v, int R) {  // |v| < 2R
 
 __device__ __forceinline__ int wrap_mod(int v, int R) { return ((v % R) + R) % R; }
 
+// wrap_mod for v in [-R, 2R) without integer division; anything outside
+// (only a non-finite position can produce it) is clamped into [0, R).
+__device__ __forceinline__ int wrap_near(int v, int R) {
+    v += (v < 0) ? R : 0;
+    v -= (v >= R) ? R : 0;
+    return min(max(v, 0), R - 1);
+}
+
 // Order-preserving map of a float to uint32 (-0 folded onto +0 so that equal
 // floats map to equal keys, matching the reference's strict '<').
 __device__ __forceinline__ unsigned int float_order_key(float f) {

@@ -33,9 +33,9 @@ __device__ __forceinline__ int cell_of_wrapped(float wx, float wy, float wz, flo
     float q0 = fmul(fadd(fadd(wx, halfL), 1e-7f), invL);
     float q1 = fmul(fadd(fadd(wy, halfL), 1e-7f), invL);
     float q2 = fmul(fadd(fadd(wz, halfL), 1e-7f), invL);
-    int c0 = wrap_mod((int)floorf(fmul(q0, (float)G)), G);
-    int c1 = wrap_mod((int)floorf(fmul(q1, (float)G)), G);
-    int c2 = wrap_mod((int)floorf(fmul(q2, (float)G)), G);
+    int c0 = wrap_near((int)floorf(fmul(q0, (float)G)), G);
+    int c1 = wrap_near((int)floorf(fmul(q1, (float)G)), G);
+    int c2 = wrap_near((int)floorf(fmul(q2, (float)G)), G);
     return (c0 * G + c1) * G + c2;
 }
 
@@ -83,9 +83,9 @@ __device__ __forceinline__ Stencil stencil_ranges(float px, float py, float pz, 
     int hz = home_coord(pz, L, invL, halfL, G);
     int st = 0, ct = 0;
     if (lane < 27) {
-        int nx = wrap_mod(hx + lane / 9 - 1, G);
-        int ny = wrap_mod(hy + (lane / 3) % 3 - 1, G);
-        int nz = wrap_mod(hz + lane % 3 - 1, G);
+        int nx = wrap_near(hx + lane / 9 - 1, G);
+        int ny = wrap_near(hy + (lane / 3) % 3 - 1, G);
+        int nz = wrap_near(hz + lane % 3 - 1, G);
         int cid = (nx * G + ny) * G + nz;
         st = cap ? (cell_base + cid) * cap : LD::ld(&cs[cid]);
         ct = LD::ld(&cc[cid]);
