@@ -210,6 +210,41 @@ __device__ __forceinline__ float power_dist_unit(float vx, float vy, float vz, f
     return fsub(d2, s.w);
 }
 
+// Packed float32 pairs (Blackwell add/sub/mul .f32x2): each half is the
+// IEEE round-to-nearest result of its own pair, so a packed op equals two
+// fsub / fmul bit for bit at half the issue slots.
+__device__ __forceinline__ float2 f2sub(float2 a, float2 b) {
+    float2 o;
+    asm("{\n\t.reg .b64 ra, rb, rc;\n\t"
+        "mov.b64 ra, {%2, %3};\n\tmov.b64 rb, {%4, %5};\n\t"
+        "sub.rn.f32x2 rc, ra, rb;\n\tmov.b64 {%0, %1}, rc;\n\t}"
+        : "=f"(o.x), "=f"(o.y)
+        : "f"(a.x), "f"(a.y), "f"(b.x), "f"(b.y));
+    return o;
+}
+
+__device__ __forceinline__ float2 f2mul(float2 a, float2 b) {
+    float2 o;
+    asm("{\n\t.reg .b64 ra, rb, rc;\n\t"
+        "mov.b64 ra, {%2, %3};\n\tmov.b64 rb, {%4, %5};\n\t"
+        "mul.rn.f32x2 rc, ra, rb;\n\tmov.b64 {%0, %1}, rc;\n\t}"
+        : "=f"(o.x), "=f"(o.y)
+        : "f"(a.x), "f"(a.y), "f"(b.x), "f"(b.y));
+    return o;
+}
+
+// power_dist_unit with the x and y axes in packed pairs: the same roundings
+// in the same order, so the same float.
+__device__ __forceinline__ float power_dist_unit2(float2 vxy, float vz, float4 s) {
+    float2 d = f2sub(vxy, make_float2(s.x, s.y));
+    float dz = fsub(vz, s.z);
+    d = f2sub(d, make_float2(rintf(d.x), rintf(d.y)));
+    dz = fsub(dz, rintf(dz));
+    const float2 q = f2mul(d, d);
+    float d2 = fadd(fadd(q.x, q.y), fmul(dz, dz));
+    return fsub(d2, s.w);
+}
+
 // voxel_to_world (jfa.py:273-287)
 __device__ __forceinline__ float voxel_centre(int idx, float vs, float halfL) {
     return fsub(fmul(fadd((float)idx, 0.5f), vs), halfL);

@@ -94,6 +94,7 @@ __device__ __forceinline__ void jfa_pass_body(const int32_t* __restrict__ in,
     int best = own;
     float bd = 1e10f;
     if (own >= 0) bd = jfa_dist<UNIT_L>(vx, vy, vz, __ldg(&seeds[own]), L);
+    const float2 vxy = make_float2(vx, vy);
 #pragma unroll
     for (int g = 0; g < 3; ++g) {
         bool ok[9];
@@ -107,14 +108,16 @@ __device__ __forceinline__ void jfa_pass_body(const int32_t* __restrict__ in,
             any |= ok[k];
         }
         if (!__any_sync(0xffffffffu, any)) continue;
+        // a skipped candidate loads seed 0 (a cached line) and its distance
+        // is ignored, so the loads need no predicate or fill
         float4 sv[9];
 #pragma unroll
-        for (int k = 0; k < 9; ++k)
-            sv[k] = ok[k] ? __ldg(&seeds[ids[g * 9 + k]]) : make_float4(0.f, 0.f, 0.f, 0.f);
+        for (int k = 0; k < 9; ++k) sv[k] = __ldg(&seeds[ok[k] ? ids[g * 9 + k] : 0]);
 #pragma unroll
         for (int k = 0; k < 9; ++k) {
             int id = ids[g * 9 + k];
-            float d = jfa_dist<UNIT_L>(vx, vy, vz, sv[k], L);
+            float d = UNIT_L ? power_dist_unit2(vxy, vz, sv[k])
+                             : jfa_dist<false>(vx, vy, vz, sv[k], L);
             if (ok[k] && (d < bd || (TIE_LOWER && d == bd && id < best))) {
                 bd = d;
                 best = id;
