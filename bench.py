@@ -354,6 +354,7 @@ def run_fos(args):
             dist.destroy_process_group()
         return 0
 
+    topo = run_topology(sim, foam, not args.no_cpu_baseline)
     cpu = None
     if not args.no_cpu_baseline:
         fps, dt, cores = time_cpu(foam, args.cpu_sample_steps, 0)
@@ -394,12 +395,72 @@ def run_fos(args):
                         "finalize_iterations": st.finalize_iterations,
                         "face_pairs": st.face_pairs, "mean_fsc": round(st.mean_fsc, 3),
                         "voxel_passes_per_s": round(V * passes * value / FRAMES_PER_STEP, 1),
-                        "fp32_peak_tflops_nominal": round(fp32_peak_tflops, 2)},
+                        "fp32_peak_tflops_nominal": round(fp32_peak_tflops, 2),
+                        "topology": topo},
     }
     print(json.dumps(line), flush=True)
     if world > 1:
         dist.destroy_process_group()
     return 0
+
+
+def run_topology(sim, foam, with_cpu):
+    """One Gabriel-degree update (run.py:1273-1277: build_topo_candidates +
+    gabriel_test_topological_degree) on the relaxed headline foam and its
+    final grid: device time with CUDA events (median of 10), beside the oracle's
+    serial restatement on the same state."""
+    import ctypes as C
+
+    import numpy as np
+    import torch
+
+    from fos._lib import call
+    from fos.context import stream
+
+    cfg, n = sim.cfg, sim.n
+    cap = int(cfg.MAX_TOPO_NEIGHBORS)
+    dev = sim.pos.device
+    pairs = torch.zeros((n, cap), dtype=torch.int32, device=dev)
+    cnt = torch.zeros(n, dtype=torch.int32, device=dev)
+    tr = torch.zeros(n, dtype=torch.int32, device=dev)
+    deg = torch.zeros(n, dtype=torch.int32, device=dev)
+    ema = torch.zeros(n, dtype=torch.float32, device=dev)
+    vp = lambda t: C.c_void_p(t.data_ptr())
+    g = (vp(sim.cell_start), vp(sim.cell_count), vp(sim.cell_indices))
+    s = torch.cuda.current_stream()
+    times = []
+    for r in range(13):
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record(s)
+        call("fos_topo_candidates", sim.ctx.h, vp(sim.pos), vp(sim.rad), *g, n,
+             float(cfg.TOPO_MAX_RADIUS_MULTIPLE), cap, vp(pairs), vp(cnt), vp(tr), stream())
+        call("fos_topo_gabriel", sim.ctx.h, vp(sim.pos), *g, n, 60 * r, cfg.cell_size(),
+             int(cfg.TOPO_PAIR_SUBSAMPLING_STRIDE), int(bool(cfg.TOPO_EARLY_EXIT_HIGH_DEGREE)),
+             float(cfg.TOPO_DEG_HIGH), cap, vp(pairs), vp(cnt), vp(ema), vp(deg), stream())
+        b.record(s)
+        b.synchronize()
+        if r >= 3:
+            times.append(a.elapsed_time(b))
+    out = {"workload": "Gabriel degree of the relaxed headline foam (candidates + witness test, "
+                       "stride 3)", "gpu_ms": round(float(np.median(times)), 4),
+           "mean_degree": round(float(deg.float().mean().item()), 3)}
+    if with_cpu:
+        from oracle import oracle as O
+        p = O.OracleParams(n=n, L=1.0, R=foam.res, r_max_cell=foam.r_max)
+        tp = O.TopoParams(mult=cfg.TOPO_MAX_RADIUS_MULTIPLE, cap=cap,
+                          stride=cfg.TOPO_PAIR_SUBSAMPLING_STRIDE,
+                          early_exit=cfg.TOPO_EARLY_EXIT_HIGH_DEGREE,
+                          deg_high=cfg.TOPO_DEG_HIGH, cell_size=cfg.cell_size())
+        pos, rad = sim.pos.cpu().numpy(), sim.rad.cpu().numpy()
+        grid = (sim.cell_count.cpu().numpy(), sim.cell_start.cpu().numpy(),
+                sim.cell_indices.cpu().numpy())
+        t0 = time.perf_counter()
+        op, opc, _ = O.topo_candidates(pos, rad, grid, p, tp)
+        odeg = O.topo_gabriel(pos, grid, op, opc, np.zeros(n, np.float32), 60 * 12, p, tp)
+        out["cpu_oracle_ms"] = round((time.perf_counter() - t0) * 1e3, 3)
+        out["cpu_cores"] = O.num_threads()
+        out["degrees_equal_oracle"] = bool(np.array_equal(odeg, deg.cpu().numpy()))
+    return out
 
 
 def run_surrogate_arm(args, foam, flush, barrier, world):

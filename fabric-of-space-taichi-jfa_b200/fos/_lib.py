@@ -160,6 +160,14 @@ SIGNATURES = {
                          C.c_uint64, C.c_uint32, _P],
     "fos_integrate_jitter": [_P, _P, _P, _I, _F, _P],
     "fos_set_fsc_targets": [_P, _P, _P, _P, _P, _I, _I, _I, _F, _F, _F, _P],
+    "fos_topo_candidates": [_P, _P, _P, _P, _P, _P, _I, C.c_double, _I, _P, _P, _P, _P],
+    "fos_topo_gabriel": [_P, _P, _P, _P, _P, _I, _I, C.c_double, _I, _I, C.c_double, _I, _P,
+                         _P, _P, _P, _P],
+    "fos_topo_batched": [_P, _P, _P, _P, _P, _P, _I, _I, _I, _I, _I, C.c_double, C.c_double,
+                         _I, _P, _P, _P, _P, _P],
+    "fos_topo_knn": [_P, _P, _P, _P, _P, _P, _I, _I, C.c_double, _P, _P],
+    "fos_topo_ema": [_P, _P, _P, _F, _I, _P],
+    "fos_topo_update_radii": [_P, _P, _P, _F, _F, _F, _F, _F, _F, _I, _P],
     "fos_nudge_radii": [_P, _P, _P, _P, _I, _F, _F, _F, _F, _F, _I, _P],
     "fos_controller_stats": [_P, _P, _P, _P, _I, _I, _I, C.POINTER(_I), C.POINTER(_I),
                              C.POINTER(_I), C.POINTER(_F), C.POINTER(_F), _P],

@@ -75,6 +75,20 @@ class FosConfig:
     JFA_ADAPTIVE_ENABLED: bool = True     # config.py:163
     JFA_VOXELS_PER_DIAMETER: float = 12.0  # config.py:164
     JFA_VOXEL_SCALE: float = 2.8          # config.py:158
+    # topological degree (topology.py), off in the reference (config.py:453-487)
+    TOPO_ENABLED: bool = False
+    TOPO_UPDATE_CADENCE: int = 60
+    TOPO_EMA_ALPHA: float = 0.1
+    TOPO_BATCHES: int = 12
+    TOPO_PAIR_SUBSAMPLE_Q: int = 3
+    TOPO_DEG_LOW: int = 10
+    TOPO_DEG_HIGH: int = 18
+    TOPO_MAX_RADIUS_MULTIPLE: float = 2.2
+    MAX_TOPO_NEIGHBORS: int = 28
+    TOPO_PAIR_SUBSAMPLING_STRIDE: int = 3
+    TOPO_EARLY_EXIT_HIGH_DEGREE: bool = True
+    USE_KNN_TOPO: bool = False
+    KNN_TOPO_K: int = 14
     # per-frame schedule of the headless driver
     PBD_ITERS: int = 4
     PRESSURE_ITERS: int = 1
@@ -91,6 +105,12 @@ class FosConfig:
         import numpy as np
         r = self.JFA_RES if res is None else res
         return int(np.ceil(np.log2(r))) + 1  # jfa.py:223
+
+    def cell_size(self) -> float:
+        """CELL_SIZE as the topology stencil uses it (config.py:317); with
+        GRID_RES given directly, the grid's own cell L / GRID_RES."""
+        return float(self.CELL_SIZE) if self.CELL_SIZE is not None else \
+            float(self.DOMAIN_SIZE) / float(self.GRID_RES)
 
     def bp_mode(self) -> int:
         return {"local": 2, "global": 1}.get(self.BACKPRESSURE_MODE, 0)

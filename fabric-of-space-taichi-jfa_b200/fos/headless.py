@@ -1,5 +1,6 @@
 """run.py's own headless frame flow on libfos: temporal skip, adaptive JFA
-resolution, OU jitter and the telemetry lines.
+resolution, OU jitter, the optional topological degree and the telemetry
+lines.
 
 ``FoamSim`` runs the workloads' fixed schedule (JFA on warm-start frames, then
 every k-th frame).  The reference's ``run.py`` decides instead, frame by
@@ -142,6 +143,15 @@ class HeadlessRun:
         self.res = int(cfg.JFA_RES)
         self.history: list[dict] = []
         self.on_signals = None     # optional callback(sig) before each decision
+        self.topo = None
+        if cfg.TOPO_ENABLED:       # topology.allocate_fields (run.py:199)
+            dev = self.sim.pos.device
+            cap = int(cfg.MAX_TOPO_NEIGHBORS)
+            self.topo = {"deg": torch.zeros(n, dtype=torch.int32, device=dev),
+                         "ema": torch.zeros(n, dtype=torch.float32, device=dev),
+                         "pairs": torch.zeros((n, cap), dtype=torch.int32, device=dev),
+                         "count": torch.zeros(n, dtype=torch.int32, device=dev),
+                         "trunc": torch.zeros(n, dtype=torch.int32, device=dev)}
 
     @classmethod
     def from_foam(cls, foam, log=None, **over) -> "HeadlessRun":
@@ -183,6 +193,8 @@ class HeadlessRun:
             self.skip.jfa_done()
             if self.log:
                 self._log_jfa()
+        if self.topo is not None:
+            self._topology()
         rec = {"frame": self.frame, "jfa": run, "reason": reason, "res": self.res} | info
         self.history.append(rec)
         self.frame += 1
@@ -192,6 +204,26 @@ class HeadlessRun:
     def run(self, frames: int):
         for _ in range(frames):
             self.step()
+
+    def _topology(self):
+        """run.py:1266-1280: every TOPO_UPDATE_CADENCE frames the Gabriel
+        degree on the frame's final grid, every frame its EMA."""
+        cfg, sim, t = self.cfg, self.sim, self.topo
+        g = (C.c_void_p(sim.cell_start.data_ptr()), C.c_void_p(sim.cell_count.data_ptr()),
+             C.c_void_p(sim.cell_indices.data_ptr()))
+        cap = int(cfg.MAX_TOPO_NEIGHBORS)
+        if self.frame % cfg.TOPO_UPDATE_CADENCE == 0:
+            call("fos_topo_candidates", self.ctx.h, C.c_void_p(sim.pos.data_ptr()),
+                 C.c_void_p(sim.rad.data_ptr()), *g, sim.n, float(cfg.TOPO_MAX_RADIUS_MULTIPLE),
+                 cap, C.c_void_p(t["pairs"].data_ptr()), C.c_void_p(t["count"].data_ptr()),
+                 C.c_void_p(t["trunc"].data_ptr()), stream())
+            call("fos_topo_gabriel", self.ctx.h, C.c_void_p(sim.pos.data_ptr()), *g, sim.n,
+                 int(self.frame), cfg.cell_size(), int(cfg.TOPO_PAIR_SUBSAMPLING_STRIDE),
+                 int(bool(cfg.TOPO_EARLY_EXIT_HIGH_DEGREE)), float(cfg.TOPO_DEG_HIGH), cap,
+                 C.c_void_p(t["pairs"].data_ptr()), C.c_void_p(t["count"].data_ptr()),
+                 C.c_void_p(t["ema"].data_ptr()), C.c_void_p(t["deg"].data_ptr()), stream())
+        call("fos_topo_ema", self.ctx.h, C.c_void_p(t["deg"].data_ptr()),
+             C.c_void_p(t["ema"].data_ptr()), float(cfg.TOPO_EMA_ALPHA), sim.n, stream())
 
     # ------------------------------------------------------------- telemetry
     def _log_decision(self, run, reason, info):

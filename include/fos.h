@@ -339,6 +339,52 @@ int fos_skip_signals(FosCtx* ctx, const FosState* st, const float* pos_prev,
 int fos_sim_set_counters(FosCtx* ctx, int frame, int settle, fos_stream_t s);
 int fos_sim_counters(FosCtx* ctx, int* frame, int* settle, fos_stream_t s);
 
+/* ------------------------------------------------------------ topology
+ * Gabriel-graph / k-NN topological degree over the hash grid (topology.py),
+ * an FSC-independent neighbour count.  The grid arguments are the CSR cell
+ * arrays of the last rebuild (each cell's particles ascending).  Candidate
+ * lists are [n][cap] int32 (MAX_TOPO_NEIGHBORS = 28 in the reference).
+ * build_topo_candidates (topology.py:68-135): the first `cap` j > i within
+ * max_radius_multiple * (r_i + r_j) in serial scan order; truncated[i] = 1
+ * when more qualify. */
+int fos_topo_candidates(FosCtx* ctx, const float* pos, const float* rad, const int32_t* cell_start,
+                        const int32_t* cell_count, const int32_t* cell_indices, int n,
+                        double max_radius_multiple, int cap, int32_t* topo_pairs,
+                        int32_t* pair_count, int32_t* truncated, fos_stream_t s);
+/* gabriel_test_topological_degree (topology.py:140-262): deg is zeroed, then
+ * every kept candidate pair whose open diameter sphere holds no witness adds
+ * 1 to both ends.  stride = TOPO_PAIR_SUBSAMPLING_STRIDE (pairs kept when
+ * the frame hash is divisible by it), early_exit with deg_high =
+ * TOPO_EARLY_EXIT_HIGH_DEGREE / TOPO_DEG_HIGH against deg_ema, cell_size =
+ * CELL_SIZE (witness stencil radius). */
+int fos_topo_gabriel(FosCtx* ctx, const float* pos, const int32_t* cell_start,
+                     const int32_t* cell_count, const int32_t* cell_indices, int n, int frame,
+                     double cell_size, int stride, int early_exit, double deg_high, int cap,
+                     const int32_t* topo_pairs, const int32_t* pair_count, const float* deg_ema,
+                     int32_t* deg, fos_stream_t s);
+/* gabriel_update_batched (topology.py:335-446): particles i with
+ * i % num_batches == batch rebuild their subsampled candidates and add their
+ * Gabriel edges to deg (not zeroed).  pair_count keeps the reference's
+ * uncapped count; only the `cap` stored candidates are tested. */
+int fos_topo_batched(FosCtx* ctx, const float* pos, const float* rad, const int32_t* cell_start,
+                     const int32_t* cell_count, const int32_t* cell_indices, int n, int batch,
+                     int num_batches, int subsample_q, int frame, double max_radius_multiple,
+                     double cell_size, int cap, int32_t* topo_pairs, int32_t* pair_count,
+                     int32_t* truncated, int32_t* deg, fos_stream_t s);
+/* knn_topo_degree (topology.py:458-505): neighbours within
+ * (max_radius_multiple * r_i)^2, capped at k. */
+int fos_topo_knn(FosCtx* ctx, const float* pos, const float* rad, const int32_t* cell_start,
+                 const int32_t* cell_count, const int32_t* cell_indices, int n, int k,
+                 double max_radius_multiple, int32_t* deg, fos_stream_t s);
+/* update_topo_ema / commit_topo_to_ema (topology.py:265-283, 448-455):
+ * ema = alpha * deg + (1 - alpha) * ema. */
+int fos_topo_ema(FosCtx* ctx, const int32_t* deg, float* deg_ema, float alpha, int n,
+                 fos_stream_t s);
+/* update_radii_topological (topology.py:286-322). */
+int fos_topo_update_radii(FosCtx* ctx, float* rad, const float* deg_effective, float deg_low,
+                          float deg_high, float gain_grow, float gain_shrink, float r_min,
+                          float r_max, int n, fos_stream_t s);
+
 /* ------------------------------------------------------------ FSC surrogate
  * No counterpart in the reference: run.py reuses the last JFA's fsc on the
  * frames between JFA runs (run.py:1230-1261).  A learned per-pair model gives

@@ -517,6 +517,200 @@ void orc_brownian(float* pos, int n, float strength, float domain, uint64_t seed
     }
 }
 
+/* ------------------------------------------------------------- topology
+ * topology.py restated with serial semantics.  Grid arguments are the CSR
+ * arrays of orc_grid_build (each cell's particles ascending). */
+
+/* grid.pdelta (grid.py:51-66): wrapP(b - a) */
+static inline void topo_pdelta(const float* a, const float* b, float L, float invL, float d[3]) {
+    for (int k = 0; k < 3; ++k) d[k] = grid_wrap(b[k] - a[k], L, invL);
+}
+
+static inline float topo_dot(const float d[3]) { return d[0] * d[0] + d[1] * d[1] + d[2] * d[2]; }
+
+/* build_topo_candidates (topology.py:68-135) */
+void orc_topo_candidates(const float* pos, const float* rad, const int32_t* cs, const int32_t* cc,
+                         const int32_t* ci, int n, int G, float L, float invL, float halfL,
+                         float mult, int cap, int32_t* pairs, int32_t* pcount, int32_t* trunc) {
+#pragma omp parallel for schedule(static)
+    for (int i = 0; i < n; ++i) {
+        pcount[i] = 0;
+        trunc[i] = 0;
+        int h[3];
+        home_cell(&pos[3 * i], L, invL, halfL, G, h);
+        for (int dx = -1; dx <= 1; ++dx)
+            for (int dy = -1; dy <= 1; ++dy)
+                for (int dz = -1; dz <= 1; ++dz) {
+                    int c = (wrapi(h[0] + dx, G) * G + wrapi(h[1] + dy, G)) * G + wrapi(h[2] + dz, G);
+                    for (int k = cs[c]; k < cs[c] + cc[c]; ++k) {
+                        int j = ci[k];
+                        if (j <= i) continue;
+                        float d[3];
+                        topo_pdelta(&pos[3 * i], &pos[3 * j], L, invL, d);
+                        float th = mult * (rad[i] + rad[j]);
+                        if (topo_dot(d) <= th * th) {
+                            if (pcount[i] < cap) {
+                                pairs[(size_t)i * cap + pcount[i]] = j;
+                                pcount[i] += 1;
+                            } else {
+                                trunc[i] = 1;
+                                break;
+                            }
+                        }
+                    }
+                }
+    }
+}
+
+/* the witness search of topology.py:218-253 (rev = 0) / 407-443 (rev = 1) */
+static int topo_is_gabriel(const float* pos, const int32_t* cs, const int32_t* cc,
+                           const int32_t* ci, int i, int j, float d2, int G, float L, float invL,
+                           float halfL, float cell_size, int rev) {
+    float d[3], m[3];
+    topo_pdelta(&pos[3 * i], &pos[3 * j], L, invL, d);
+    for (int k = 0; k < 3; ++k) m[k] = grid_wrap(pos[3 * i + k] + 0.5f * d[k], L, invL);
+    float r_sq = 0.25f * d2;
+    int mc[3];
+    for (int k = 0; k < 3; ++k) mc[k] = wrapi((int)(((m[k] + halfL) * invL) * (float)G), G);
+    float r_d = sqrtf(d2) * 0.5f;
+    int sc = (int)ceilf(r_d / cell_size);
+    sc = sc < 1 ? 1 : (sc > 3 ? 3 : sc);
+    if (sc > G / 2) sc = G / 2;
+    float eps = fmaxf(1e-12f, 1e-6f * r_sq);
+    for (int dx = -sc; dx <= sc; ++dx)
+        for (int dy = -sc; dy <= sc; ++dy)
+            for (int dz = -sc; dz <= sc; ++dz) {
+                int c = (wrapi(mc[0] + dx, G) * G + wrapi(mc[1] + dy, G)) * G + wrapi(mc[2] + dz, G);
+                for (int q = cs[c]; q < cs[c] + cc[c]; ++q) {
+                    int k = ci[q];
+                    if (k == i || k == j) continue;
+                    float e[3];
+                    if (rev) topo_pdelta(m, &pos[3 * k], L, invL, e);
+                    else topo_pdelta(&pos[3 * k], m, L, invL, e);
+                    if (topo_dot(e) < r_sq - eps) return 0;
+                }
+            }
+    return 1;
+}
+
+static inline int topo_keep(int i, int j, int frame, int q) {
+    uint32_t h = ((uint32_t)i * 73856093u) ^ ((uint32_t)j * 19349663u) ^ ((uint32_t)frame * 83492791u);
+    return q <= 1 || ((int32_t)h % q) == 0;
+}
+
+/* gabriel_test_topological_degree (topology.py:140-262) */
+void orc_topo_gabriel(const float* pos, const int32_t* cs, const int32_t* cc, const int32_t* ci,
+                      int n, int G, float L, float invL, float halfL, float cell_size, int frame,
+                      int stride, int early_exit, float deg_high, int cap, const int32_t* pairs,
+                      const int32_t* pcount, const float* deg_ema, int32_t* deg) {
+    for (int i = 0; i < n; ++i) deg[i] = 0;
+    for (int i = 0; i < n; ++i) {
+        for (int p = 0; p < pcount[i]; ++p) {
+            int j = pairs[(size_t)i * cap + p];
+            if (!topo_keep(i, j, frame, stride)) continue;
+            if (early_exit && deg_ema[i] >= deg_high && deg_ema[j] >= deg_high) continue;
+            float d[3];
+            topo_pdelta(&pos[3 * i], &pos[3 * j], L, invL, d);
+            float d2 = topo_dot(d);
+            if (d2 < 1e-16f) continue;
+            if (topo_is_gabriel(pos, cs, cc, ci, i, j, d2, G, L, invL, halfL, cell_size, 0) && j > i) {
+                deg[i] += 1;
+                deg[j] += 1;
+            }
+        }
+    }
+}
+
+/* gabriel_update_batched (topology.py:335-446); only the `cap` stored
+ * candidates are tested (the reference's count runs past the row) */
+void orc_topo_batched(const float* pos, const float* rad, const int32_t* cs, const int32_t* cc,
+                      const int32_t* ci, int n, int G, float L, float invL, float halfL,
+                      float mult, float cell_size, int batch, int num_batches, int q, int frame,
+                      int cap, int32_t* pairs, int32_t* pcount, int32_t* trunc, int32_t* deg) {
+    for (int i = 0; i < n; ++i) {
+        if (i % num_batches != batch) continue;
+        pcount[i] = 0;
+        trunc[i] = 0;
+        int h[3];
+        home_cell(&pos[3 * i], L, invL, halfL, G, h);
+        for (int dx = -1; dx <= 1; ++dx)
+            for (int dy = -1; dy <= 1; ++dy)
+                for (int dz = -1; dz <= 1; ++dz) {
+                    int c = (wrapi(h[0] + dx, G) * G + wrapi(h[1] + dy, G)) * G + wrapi(h[2] + dz, G);
+                    for (int k = cs[c]; k < cs[c] + cc[c]; ++k) {
+                        int j = ci[k];
+                        if (j <= i || !topo_keep(i, j, frame, q)) continue;
+                        float d[3];
+                        topo_pdelta(&pos[3 * i], &pos[3 * j], L, invL, d);
+                        float th = mult * (rad[i] + rad[j]);
+                        if (topo_dot(d) <= th * th) {
+                            int cur = pcount[i]++;
+                            if (cur < cap) pairs[(size_t)i * cap + cur] = j;
+                            else trunc[i] = 1;
+                        }
+                    }
+                }
+        int pc = pcount[i] < cap ? pcount[i] : cap;
+        for (int p = 0; p < pc; ++p) {
+            int j = pairs[(size_t)i * cap + p];
+            float d[3];
+            topo_pdelta(&pos[3 * i], &pos[3 * j], L, invL, d);
+            float d2 = topo_dot(d);
+            if (d2 < 1e-16f) continue;
+            if (topo_is_gabriel(pos, cs, cc, ci, i, j, d2, G, L, invL, halfL, cell_size, 1)) {
+                deg[i] += 1;
+                deg[j] += 1;
+            }
+        }
+    }
+}
+
+/* knn_topo_degree (topology.py:458-505) */
+void orc_topo_knn(const float* pos, const float* rad, const int32_t* cs, const int32_t* cc,
+                  const int32_t* ci, int n, int G, float L, float invL, float halfL, float mult,
+                  int kmax, int32_t* deg) {
+#pragma omp parallel for schedule(static)
+    for (int i = 0; i < n; ++i) {
+        int cnt = 0;
+        float lim = mult * rad[i];
+        float lim2 = lim * lim;
+        int h[3];
+        home_cell(&pos[3 * i], L, invL, halfL, G, h);
+        for (int dx = -1; dx <= 1 && cnt < kmax; ++dx)
+            for (int dy = -1; dy <= 1 && cnt < kmax; ++dy)
+                for (int dz = -1; dz <= 1 && cnt < kmax; ++dz) {
+                    int c = (wrapi(h[0] + dx, G) * G + wrapi(h[1] + dy, G)) * G + wrapi(h[2] + dz, G);
+                    for (int k = cs[c]; k < cs[c] + cc[c]; ++k) {
+                        int j = ci[k];
+                        if (j == i) continue;
+                        float d[3];
+                        topo_pdelta(&pos[3 * i], &pos[3 * j], L, invL, d);
+                        if (topo_dot(d) <= lim2) {
+                            cnt += 1;
+                            if (cnt >= kmax) break;
+                        }
+                    }
+                }
+        deg[i] = cnt < kmax ? cnt : kmax;
+    }
+}
+
+/* update_topo_ema / commit_topo_to_ema (topology.py:265-283, 448-455) */
+void orc_topo_ema(const int32_t* deg, float* ema, float alpha, int n) {
+    for (int i = 0; i < n; ++i) ema[i] = alpha * (float)deg[i] + (1.0f - alpha) * ema[i];
+}
+
+/* update_radii_topological (topology.py:286-322) */
+void orc_topo_radii(float* rad, const float* deg_eff, float lo, float hi, float grow, float shrink,
+                    float rmin, float rmax, int n) {
+    for (int i = 0; i < n; ++i) {
+        float d = deg_eff[i], r = rad[i];
+        if (d < lo) r = r * (1.0f + grow);
+        else if (d > hi) r = r * (1.0f - shrink);
+        rad[i] = fmaxf(rmin, fminf(rmax, r));
+    }
+}
+
 #define ORC_OU_STREAM 0x4f554a54u
 
 /* compute_mean_radius (dynamics.py:675-689) as run.py:860-861 uses it: the

@@ -63,6 +63,15 @@ def lib():
             "orc_philox": (None, [C.c_uint32] * 6 + [_p]),
             "orc_brownian": (None, [_p, _i, _f, _f, C.c_uint64, C.c_uint32]),
             "orc_mean_radius": (_f, [_p, _i]),
+            "orc_topo_candidates": (None, [_p, _p, _p, _p, _p, _i, _i, _f, _f, _f, _f, _i, _p,
+                                           _p, _p]),
+            "orc_topo_gabriel": (None, [_p, _p, _p, _p, _i, _i, _f, _f, _f, _f, _i, _i, _i,
+                                        _f, _i, _p, _p, _p, _p]),
+            "orc_topo_batched": (None, [_p, _p, _p, _p, _p, _i, _i, _f, _f, _f, _f, _f, _i, _i,
+                                        _i, _i, _i, _p, _p, _p, _p]),
+            "orc_topo_knn": (None, [_p, _p, _p, _p, _p, _i, _i, _f, _f, _f, _f, _i, _p]),
+            "orc_topo_ema": (None, [_p, _p, _f, _i]),
+            "orc_topo_radii": (None, [_p, _p, _f, _f, _f, _f, _f, _f, _i]),
             "orc_ou_jitter": (None, [_p, _p, _p, _i, _f, _f, C.c_double, C.c_double, C.c_double,
                                      C.c_double, _f, _f, C.c_uint64, C.c_uint32]),
             "orc_set_targets": (None, [_p, _p, _p, _p, _i, _i, _i, _f, _f, _f, _f]),
@@ -309,6 +318,65 @@ def set_threads(t: int):
 
 def num_threads() -> int:
     return int(lib().orc_num_threads())
+
+
+# ------------------------------------------------------------------ topology
+@dataclass
+class TopoParams:
+    """config.py:453-487 (topology constants)."""
+    mult: float = 2.2                 # TOPO_MAX_RADIUS_MULTIPLE
+    cap: int = 28                     # MAX_TOPO_NEIGHBORS
+    stride: int = 3                   # TOPO_PAIR_SUBSAMPLING_STRIDE
+    early_exit: bool = True           # TOPO_EARLY_EXIT_HIGH_DEGREE
+    deg_high: float = 18.0            # TOPO_DEG_HIGH
+    cell_size: float = 0.06           # CELL_SIZE
+
+
+def topo_candidates(pos, rad, grid, p: OracleParams, tp: TopoParams):
+    cc, cs, ci = grid
+    pairs = np.zeros((p.n, tp.cap), np.int32)
+    pc = np.zeros(p.n, np.int32)
+    tr = np.zeros(p.n, np.int32)
+    lib().orc_topo_candidates(_ptr(pos), _ptr(rad), _ptr(cs), _ptr(cc), _ptr(ci), p.n, p.G,
+                              _f32(p.L), p.invL, p.halfL, _f32(tp.mult), tp.cap, _ptr(pairs),
+                              _ptr(pc), _ptr(tr))
+    return pairs, pc, tr
+
+
+def topo_gabriel(pos, grid, pairs, pc, deg_ema, frame: int, p: OracleParams, tp: TopoParams):
+    cc, cs, ci = grid
+    deg = np.zeros(p.n, np.int32)
+    lib().orc_topo_gabriel(_ptr(pos), _ptr(cs), _ptr(cc), _ptr(ci), p.n, p.G, _f32(p.L), p.invL,
+                           p.halfL, _f32(tp.cell_size), int(frame), tp.stride,
+                           int(tp.early_exit), _f32(tp.deg_high), tp.cap, _ptr(pairs), _ptr(pc),
+                           _ptr(deg_ema), _ptr(deg))
+    return deg
+
+
+def topo_batched(pos, rad, grid, batch, num_batches, q, frame, pairs, pc, tr, deg,
+                 p: OracleParams, tp: TopoParams):
+    cc, cs, ci = grid
+    lib().orc_topo_batched(_ptr(pos), _ptr(rad), _ptr(cs), _ptr(cc), _ptr(ci), p.n, p.G,
+                           _f32(p.L), p.invL, p.halfL, _f32(tp.mult), _f32(tp.cell_size),
+                           int(batch), int(num_batches), int(q), int(frame), tp.cap, _ptr(pairs),
+                           _ptr(pc), _ptr(tr), _ptr(deg))
+
+
+def topo_knn(pos, rad, grid, k: int, p: OracleParams, tp: TopoParams):
+    cc, cs, ci = grid
+    deg = np.zeros(p.n, np.int32)
+    lib().orc_topo_knn(_ptr(pos), _ptr(rad), _ptr(cs), _ptr(cc), _ptr(ci), p.n, p.G, _f32(p.L),
+                       p.invL, p.halfL, _f32(tp.mult), int(k), _ptr(deg))
+    return deg
+
+
+def topo_ema(deg, ema, alpha: float):
+    lib().orc_topo_ema(_ptr(deg), _ptr(ema), _f32(alpha), len(deg))
+
+
+def topo_radii(rad, deg_eff, lo, hi, grow, shrink, rmin, rmax):
+    lib().orc_topo_radii(_ptr(rad), _ptr(deg_eff), _f32(lo), _f32(hi), _f32(grow), _f32(shrink),
+                         _f32(rmin), _f32(rmax), len(rad))
 
 
 # ------------------------------------------------------- run.py's JFA schedule

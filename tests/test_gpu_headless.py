@@ -145,3 +145,17 @@ def test_watchdog_schedule():
     runs = [r["frame"] for r in hr.history if r["jfa"]]
     assert runs == [0, 1, 2, 3, 4, 5, 9, 13, 17]
     assert {r["reason"] for r in hr.history if r["jfa"] and r["frame"] > 5} == {"watchdog"}
+
+
+def test_topology_step_runs_on_cadence():
+    """run.py:1266-1280 with TOPO_ENABLED: degrees on cadence frames, EMA every frame."""
+    hr = HeadlessRun.from_foam(inputs.small(), TOPO_ENABLED=True, TOPO_UPDATE_CADENCE=3, **OVER)
+    hr.initialize()
+    hr.run(2)
+    ema1 = hr.topo["ema"].clone()
+    assert torch.count_nonzero(hr.topo["deg"]).item() > 0   # frame 0 computed degrees
+    hr.run(1)                                                # frame 2: EMA only
+    torch.cuda.synchronize()
+    deg = hr.topo["deg"].float()
+    want = 0.1 * deg + (1.0 - 0.1) * ema1
+    assert torch.allclose(hr.topo["ema"], want, rtol=1e-6, atol=1e-6)
