@@ -51,6 +51,8 @@ def parse():
     ap.add_argument("--no-surrogate", action="store_true",
                     help="skip the surrogate-FSC arm of the metric")
     ap.add_argument("--surrogate-mode", default="absolute", choices=["absolute", "anchored"])
+    ap.add_argument("--no-warm-jfa", action="store_true",
+                    help="skip the warm-started JFA arm (frames/s and agreement with the exact JFA)")
     ap.add_argument("--no-ensemble", action="store_true",
                     help="skip the batched-ensemble measurement")
     ap.add_argument("--ensemble-frames", type=int, default=500)
@@ -346,6 +348,7 @@ def run_fos(args):
 
     surrogate = None if args.no_surrogate else run_surrogate_arm(args, foam, flush, barrier, world)
     ensemble = None if args.no_ensemble else run_ensemble(args, barrier, world, rank)
+    warm = None if args.no_warm_jfa else run_warm_jfa(foam, flush)
 
     if world > 1:
         dist.barrier()
@@ -387,6 +390,7 @@ def run_fos(args):
                               "note": "issue bound (27 candidate evaluations per voxel); "
                                       "labels are L2-resident at 128^3"},
         "surrogate": surrogate,
+        "warm_jfa": warm,
         "ensemble": ensemble,
         "gpu_launches": int(launches),
         "clocks": clk,
@@ -536,6 +540,79 @@ def run_surrogate_arm(args, foam, flush, barrier, world):
                   "frames": "JFA frames 20-200", "rows": "3,000,000 sampled pairs",
                   "epochs": 30, "lr": 1e-3, "batch": 65536},
     }
+
+
+def run_warm_jfa(foam, flush):
+    """The warm-started JFA (fos_jfa_warm, steps 4, 2, 1, 1 from the previous
+    owner grid) beside the exact one: frames/s of the same 5-frame cycles
+    (device time, graph replay), owner-label and FSC agreement from one
+    relaxed state, and the dirty-tile fraction of the reference's marking
+    between two JFA frames."""
+    import ctypes as C
+
+    import torch
+
+    from fos import jfa as J
+    from fos import runtime
+    from fos._lib import call
+    from fos.context import stream
+    from fos.driver import FoamSim
+
+    s = torch.cuda.current_stream()
+    out = {"workload": foam.name, "first_step": None}
+    fps = {}
+    for name, warm in (("exact", False), ("warm", True)):
+        sim = FoamSim.from_foam(foam, jfa_warm=warm)
+        out["first_step"] = sim.cfg.JFA_WARM_STEP
+        sim.initialize()
+        sim.run(40)
+        tot = 0.0
+        for _ in range(20):
+            flush.fill_(1.0)
+            a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            a.record(s)
+            sim.run(5)
+            b.record(s)
+            b.synchronize()
+            tot += a.elapsed_time(b)
+        fps[name] = 100.0 / (tot / 1000.0)
+        if warm:
+            # agreement from one relaxed state: frames 40..44 ran, the last JFA on frame 40
+            fields = ("fsc", "fsc_ema", "face_ids", "face_counts", "neighbor_list",
+                      "neighbor_used_count", "neighbor_prev_scores")
+            snap = {k: getattr(sim.ctx, k).clone() for k in fields}
+            n = sim.n
+
+            def finish():
+                lab = sim.ctx.labels().clone()
+                sim.ctx.majority_filter()
+                sim.ctx.accumulate_faces(n)
+                sim.ctx.finalize(sim.rad, n)
+                return lab, sim.fsc.clone()
+
+            call("fos_jfa_warm", sim.ctx.h, C.c_void_p(sim.pos.data_ptr()),
+                 C.c_void_p(sim.rad.data_ptr()), n, sim.cfg.JFA_WARM_STEP, stream())
+            lw, fw = finish()
+            for k, v in snap.items():
+                getattr(sim.ctx, k).copy_(v)
+            sim.ctx.jfa_init(sim.pos, sim.rad, n)
+            sim.ctx.jfa_passes(n)
+            lx, fx = finish()
+            out["voxel_agreement"] = round((lw == lx).float().mean().item(), 6)
+            out["fsc_agreement"] = round((fw == fx).float().mean().item(), 6)
+            # dirty tiles between two JFA frames, as run.py marks them
+            pp, rp = sim.pos.clone(), sim.rad.clone()
+            sim.run(5)
+            runtime.configure(sim.cfg)
+            J.init_jfa(max_particles=n, max_res=sim.ctx.max_res)
+            J.update_tile_cache(pp, rp, n)
+            J.clear_dirty_tiles()
+            J.mark_dirty_tiles(sim.pos, sim.rad, n)
+            out["dirty_tiles"] = [J.count_dirty_tiles(), J.tiles_per_axis ** 3]
+            runtime.ctx().close()
+    out["frames_per_s"] = {k: round(v, 2) for k, v in fps.items()}
+    out["speedup"] = round(fps["warm"] / fps["exact"], 4)
+    return out
 
 
 def run_ensemble(args, barrier, world, rank):

@@ -134,7 +134,7 @@ extern "C" int fos_set_params(FosCtx* c, const FosParams* p) {
     FOS_CUDA(cudaSetDevice(c->device));
     c->p = *p;
     fold_params(c);
-    for (int k = 0; k < 4; ++k) c->gvalid[k] = false;
+    for (int k = 0; k < FOS_GRAPH_SLOTS; ++k) c->gvalid[k] = false;
     return alloc_cells(c);
 }
 
@@ -254,7 +254,7 @@ extern "C" int fos_ctx_create(const FosParams* p, int max_n, int max_res, int de
 extern "C" int fos_ctx_destroy(FosCtx* c) {
     if (!c) return FOS_OK;
     cudaSetDevice(c->device);
-    for (int k = 0; k < 4; ++k)
+    for (int k = 0; k < FOS_GRAPH_SLOTS; ++k)
         if (c->gexec[k]) cudaGraphExecDestroy(c->gexec[k]);
     fos_sur_free(c);
     void* ptrs[] = {c->labA, c->labB, c->filt, c->seedslot, c->seeds, c->fsc, c->used, c->ema,
@@ -280,7 +280,7 @@ extern "C" int fos_set_resolution(FosCtx* c, int res) {
     c->vs = (float)(c->p.domain_size / (double)res);      // VOXEL_SIZE = L / JFA_RES
     c->passes = (int)ceil(log2((double)res)) + 1;         // ceil(log2 R) + 1
     if (c->passes > FOS_MAX_PASSES) c->passes = FOS_MAX_PASSES;
-    for (int k = 0; k < 4; ++k) c->gvalid[k] = false;
+    for (int k = 0; k < FOS_GRAPH_SLOTS; ++k) c->gvalid[k] = false;
     return FOS_OK;
 }
 

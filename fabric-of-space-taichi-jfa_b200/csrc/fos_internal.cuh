@@ -41,6 +41,8 @@ struct FosDevState {
     unsigned int bar_gen;         // grid barrier generation
     int grid_ovf;                 // bit p: a fixed-capacity cell row of count buffer p overflowed
     unsigned long long rad_sum;   // OU jitter: sum of the radii, 2^-40 fixed point
+    int tile_count;               // fos_dirty_count: marked tiles
+    int pad_tc;
     unsigned long long changes[FOS_MAX_PASSES];
 };
 
@@ -57,6 +59,7 @@ struct FosGraphKey {
 struct FosSurBufs;  // surrogate.cu
 
 #define FOS_SKIP_BLOCKS 1024
+#define FOS_GRAPH_SLOTS 6
 
 struct FosCtx {
     int device = 0;
@@ -117,11 +120,11 @@ struct FosCtx {
     void* skip_part = nullptr;        // fos_skip_signals: FOS_SKIP_BLOCKS partials + result
     FosSurBufs* sur = nullptr;        // FSC surrogate pair/inference buffers (first use)
     int sur_mode = FOS_SUR_ABSOLUTE;  // how surrogate frames use the model (fos.h)
-    // graphs, indexed by jfa_frame + 2 * (surrogate frame)
-    cudaGraphExec_t gexec[4] = {nullptr, nullptr, nullptr, nullptr};
-    FosGraphKey gkey[4];
-    bool gvalid[4] = {false, false, false, false};
-    long long glaunch[4] = {0, 0, 0, 0};  // kernels per captured frame graph
+    // graphs, indexed by jfa_frame (0 none, 1 exact, 2 warm) + 3 * (surrogate frame)
+    cudaGraphExec_t gexec[FOS_GRAPH_SLOTS] = {};
+    FosGraphKey gkey[FOS_GRAPH_SLOTS];
+    bool gvalid[FOS_GRAPH_SLOTS] = {};
+    long long glaunch[FOS_GRAPH_SLOTS] = {};  // kernels per captured frame graph
     long long launches = 0;
 };
 

@@ -59,6 +59,7 @@ extern "C" void fos_frame_params_default(FosFrameParams* fp) {
     fp->jitter_tau = 1.0;            // JITTER_TAU (config.py:496)
     fp->dt = 0.016;                  // DT (config.py:400)
     fp->max_drift_fraction = 0.20;   // MAX_DRIFT_FRACTION (config.py:498)
+    fp->jfa_warm_step = 4;           // first step of a warm-started JFA (jfa_frame == 2)
 }
 
 __global__ void k_frame_set(FosDevState* ds, int frame, int settle) {
@@ -77,6 +78,7 @@ static int check_state(FosCtx* c, const FosState* st, const FosFrameParams* fp) 
                 FOS_E_ARG, "NULL state buffer");
     FOS_REQUIRE(fp->pbd_iters >= 0 && fp->pressure_iters >= 0, FOS_E_ARG, "negative iterations");
     FOS_REQUIRE(!fp->ou_jitter || st->v_jit, FOS_E_ARG, "ou_jitter needs FosState.v_jit");
+    FOS_REQUIRE(fp->jfa_warm_step >= 0, FOS_E_ARG, "jfa_warm_step must be >= 0");
     FOS_REQUIRE(!fp->ou_jitter || (fp->dt > 0.0 && fp->jitter_tau >= 0.0), FOS_E_ARG,
                 "ou_jitter needs dt > 0 and jitter_tau >= 0");
     return FOS_OK;
@@ -192,6 +194,7 @@ static int frame_impl(FosCtx* c, const FosState* st, const FosFrameParams* fp, i
                       cudaStream_t s, FrameProf* prof, const FosSurrogate* sur, int part) {
     int rc = check_state(c, st, fp);
     if (rc) return rc;
+    FOS_REQUIRE(jfa_frame >= 0 && jfa_frame <= 2, FOS_E_ARG, "jfa_frame must be 0, 1 or 2");
     const int n = st->n;
 #define MARK(id) \
     if (prof) prof->mark(id)
@@ -269,10 +272,15 @@ static int frame_impl(FosCtx* c, const FosState* st, const FosFrameParams* fp, i
     }
     // (8) measurement frame: run_jfa, warm-start gate, set_fsc_targets, settle reset
     if (jfa_frame) {
-        rc = fos_jfa_init(c, st->pos, st->rad, n, s);
-        if (rc) return rc;
-        rc = fos_jfa_passes(c, n, s);
-        if (rc) return rc;
+        if (jfa_frame == 2) {
+            rc = fos_jfa_warm(c, st->pos, st->rad, n, fp->jfa_warm_step, s);
+            if (rc) return rc;
+        } else {
+            rc = fos_jfa_init(c, st->pos, st->rad, n, s);
+            if (rc) return rc;
+            rc = fos_jfa_passes(c, n, s);
+            if (rc) return rc;
+        }
         MARK(6);
         rc = fos_jfa_majority_filter(c, s);
         if (rc) return rc;
@@ -450,7 +458,8 @@ static int frame_graph_impl(FosCtx* c, const FosState* st, const FosFrameParams*
         rc = fos_sur_prepare(c);  // allocation stays outside the capture
         if (rc) return rc;
     }
-    int g = (jfa_frame ? 1 : 0) + (sur ? 2 : 0);
+    FOS_REQUIRE(jfa_frame >= 0 && jfa_frame <= 2, FOS_E_ARG, "jfa_frame must be 0, 1 or 2");
+    int g = jfa_frame + (sur ? 3 : 0);
     FosGraphKey key;
     memset(&key, 0, sizeof(key));
     key.st = *st;

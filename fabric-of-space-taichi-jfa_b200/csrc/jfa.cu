@@ -434,41 +434,88 @@ extern "C" int fos_jfa_init(FosCtx* c, const float* pos, const float* rad, int n
 
 template <bool UL, bool P2, bool TIE>
 static void launch_pass(FosCtx* c, const int32_t* in, int32_t* out, int step, int pass,
-                        cudaStream_t s) {
+                        int early_exit, cudaStream_t s) {
     const int R = c->res;
     long long V = (long long)R * R * R;
     k_jfa_pass<UL, P2, TIE><<<fos_blocks(V, 256), 256, 0, s>>>(
-        in, out, c->seeds, R, ilog2(R), c->vs, c->halfL, c->L, step, c->ds, pass, c->p.early_exit,
+        in, out, c->seeds, R, ilog2(R), c->vs, c->halfL, c->L, step, c->ds, pass, early_exit,
         c->p.min_jfa_passes, c->p.th_pass_delta);
+}
+
+// `npass` passes from labA, steps first_step, first_step/2, ... (never below 1).
+static int run_passes(FosCtx* c, int first_step, int npass, int early_exit, cudaStream_t s) {
+    const int R = c->res;
+    long long V = (long long)R * R * R;
+    FOS_CUDA(cudaMemsetAsync(c->ds->changes, 0, sizeof(c->ds->changes), s));
+    bool ul = (c->L == 1.0f), p2 = is_pow2(R), tie = c->p.tie_lower_index != 0;
+    int step = first_step;
+    for (int p = 0; p < npass; ++p) {
+        if (step < 1) step = 1;
+        const int32_t* in = (p & 1) ? c->labB : c->labA;
+        int32_t* out = (p & 1) ? c->labA : c->labB;
+        const int ee = early_exit;
+        if (ul && p2 && !tie) launch_pass<true, true, false>(c, in, out, step, p, ee, s);
+        else if (ul && p2 && tie) launch_pass<true, true, true>(c, in, out, step, p, ee, s);
+        else if (ul && !p2 && !tie) launch_pass<true, false, false>(c, in, out, step, p, ee, s);
+        else if (ul && !p2 && tie) launch_pass<true, false, true>(c, in, out, step, p, ee, s);
+        else if (!ul && p2 && !tie) launch_pass<false, true, false>(c, in, out, step, p, ee, s);
+        else if (!ul && p2 && tie) launch_pass<false, true, true>(c, in, out, step, p, ee, s);
+        else if (!ul && !p2 && !tie) launch_pass<false, false, false>(c, in, out, step, p, ee, s);
+        else launch_pass<false, false, true>(c, in, out, step, p, ee, s);
+        FOS_LAUNCHED(c);
+        step /= 2;
+    }
+    k_jfa_finish<<<1, 1, 0, s>>>(c->ds, npass, V, early_exit, c->p.min_jfa_passes,
+                                 c->p.th_pass_delta);
+    FOS_LAUNCHED(c);
+    return FOS_OK;
 }
 
 extern "C" int fos_jfa_passes(FosCtx* c, int n, fos_stream_t s) {
     int rc = check_n(c, n);
     if (rc) return rc;
+    return run_passes(c, c->res / 2, c->passes, c->p.early_exit, s);
+}
+
+// The previous run's final owner grid into labA (the warm start's input).
+__global__ void k_take_final(int32_t* __restrict__ labA, const int32_t* __restrict__ labB,
+                             const FosDevState* ds, long long V) {
+    if (ds->final_buf == 0) return;  // already in labA
+    for (long long l = (long long)blockIdx.x * blockDim.x + threadIdx.x; l < V;
+         l += (long long)gridDim.x * blockDim.x)
+        labA[l] = labB[l];
+}
+
+extern "C" int fos_jfa_warm(FosCtx* c, const float* pos, const float* rad, int n, int first_step,
+                            fos_stream_t s) {
+    int rc = check_n(c, n);
+    if (rc) return rc;
+    FOS_REQUIRE(n == 0 || (pos && rad), FOS_E_ARG, "pos/rad is NULL");
     const int R = c->res;
-    long long V = (long long)R * R * R;
-    FOS_CUDA(cudaMemsetAsync(c->ds->changes, 0, sizeof(c->ds->changes), s));
-    bool ul = (c->L == 1.0f), p2 = is_pow2(R), tie = c->p.tie_lower_index != 0;
-    int step = R / 2;
-    for (int p = 0; p < c->passes; ++p) {
-        if (step < 1) step = 1;
-        const int32_t* in = (p & 1) ? c->labB : c->labA;
-        int32_t* out = (p & 1) ? c->labA : c->labB;
-        if (ul && p2 && !tie) launch_pass<true, true, false>(c, in, out, step, p, s);
-        else if (ul && p2 && tie) launch_pass<true, true, true>(c, in, out, step, p, s);
-        else if (ul && !p2 && !tie) launch_pass<true, false, false>(c, in, out, step, p, s);
-        else if (ul && !p2 && tie) launch_pass<true, false, true>(c, in, out, step, p, s);
-        else if (!ul && p2 && !tie) launch_pass<false, true, false>(c, in, out, step, p, s);
-        else if (!ul && p2 && tie) launch_pass<false, true, true>(c, in, out, step, p, s);
-        else if (!ul && !p2 && !tie) launch_pass<false, false, false>(c, in, out, step, p, s);
-        else launch_pass<false, false, true>(c, in, out, step, p, s);
-        FOS_LAUNCHED(c);
-        step /= 2;
-    }
-    k_jfa_finish<<<1, 1, 0, s>>>(c->ds, c->passes, V, c->p.early_exit, c->p.min_jfa_passes,
-                                 c->p.th_pass_delta);
+    FOS_REQUIRE(first_step >= 1 && first_step <= (R > 1 ? R / 2 : 1) && is_pow2(first_step),
+                FOS_E_ARG, "first_step must be a power of two in [1, res/2]");
+    const long long V = (long long)R * R * R;
+    int blocks = fos_blocks(V, 256);
+    if (blocks > 8 * c->num_sms) blocks = 8 * c->num_sms;
+    k_take_final<<<blocks, 256, 0, s>>>(c->labA, c->labB, c->ds, V);
     FOS_LAUNCHED(c);
-    return FOS_OK;
+    if (n > 0) {
+        // re-plant every seed at its current voxel over the previous owners
+        int nb = fos_blocks(n, 256);
+        k_seed_prepare<<<nb, 256, 0, s>>>(pos, rad, n, R, c->halfL, c->L, c->beta, c->seeds,
+                                          c->cellof, c->seedslot);
+        FOS_LAUNCHED(c);
+        if (c->L == 1.0f)
+            k_seed_min<true><<<nb, 256, 0, s>>>(c->seeds, c->cellof, n, R, c->vs, c->halfL, c->L,
+                                               c->seedslot);
+        else
+            k_seed_min<false><<<nb, 256, 0, s>>>(c->seeds, c->cellof, n, R, c->vs, c->halfL, c->L,
+                                                c->seedslot);
+        FOS_LAUNCHED(c);
+        k_seed_write<<<nb, 256, 0, s>>>(c->cellof, n, c->seedslot, c->labA);
+        FOS_LAUNCHED(c);
+    }
+    return run_passes(c, first_step, ilog2(first_step) + 2, 0, s);
 }
 
 extern "C" int fos_jfa_load_labels(FosCtx* c, const int32_t* labels, fos_stream_t s) {

@@ -71,7 +71,7 @@ class FosFrameParams(C.Structure):
         ("pressure_pair_cap", C.c_double), ("max_eq_nei", C.c_int),
         ("brownian_strength", C.c_double), ("seed", C.c_uint64), ("warmup_pbd", C.c_int),
         ("ou_jitter", C.c_int), ("jitter_rms", C.c_double), ("jitter_tau", C.c_double),
-        ("dt", C.c_double), ("max_drift_fraction", C.c_double),
+        ("dt", C.c_double), ("max_drift_fraction", C.c_double), ("jfa_warm_step", C.c_int),
     ]
 
 
@@ -160,6 +160,9 @@ SIGNATURES = {
                          C.c_uint64, C.c_uint32, _P],
     "fos_integrate_jitter": [_P, _P, _P, _I, _F, _P],
     "fos_set_fsc_targets": [_P, _P, _P, _P, _P, _I, _I, _I, _F, _F, _F, _P],
+    "fos_jfa_warm": [_P, _P, _P, _I, _I, _P],
+    "fos_dirty_mark": [_P, _P, _P, _P, _P, _I, C.c_double, C.c_double, _I, _P, _P],
+    "fos_dirty_count": [_P, _P, C.POINTER(_I), _P],
     "fos_topo_candidates": [_P, _P, _P, _P, _P, _P, _I, C.c_double, _I, _P, _P, _P, _P],
     "fos_topo_gabriel": [_P, _P, _P, _P, _P, _I, _I, C.c_double, _I, _I, C.c_double, _I, _P,
                          _P, _P, _P, _P],

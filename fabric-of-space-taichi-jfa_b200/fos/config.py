@@ -75,6 +75,16 @@ class FosConfig:
     JFA_ADAPTIVE_ENABLED: bool = True     # config.py:163
     JFA_VOXELS_PER_DIAMETER: float = 12.0  # config.py:164
     JFA_VOXEL_SCALE: float = 2.8          # config.py:158
+    # warm-started JFA (no reference counterpart): first step of its pass
+    # schedule; FoamSim uses it on JFA frames when jfa_warm is set
+    JFA_WARM_STEP: int = 4
+    # dirty-tile bookkeeping of the JFA grid (config.py:181-191)
+    JFA_DIRTY_TILES_ENABLED: bool = True
+    JFA_TILE_SIZE: int = 16
+    JFA_DIRTY_HALO: int = 1
+    JFA_DIRTY_WARMSTART: bool = True
+    JFA_DIRTY_POS_THRESHOLD: float = 0.5
+    JFA_DIRTY_RAD_THRESHOLD: float = 0.25
     # topological degree (topology.py), off in the reference (config.py:453-487)
     TOPO_ENABLED: bool = False
     TOPO_UPDATE_CADENCE: int = 60
@@ -145,7 +155,8 @@ class FosConfig:
             seed=int(self.SEED) & 0xFFFFFFFFFFFFFFFF, warmup_pbd=int(self.PBD_BASE_PASSES),
             ou_jitter=int(bool(self.JITTER_ENABLED)), jitter_rms=float(self.JITTER_RMS),
             jitter_tau=float(self.JITTER_TAU), dt=float(self.DT),
-            max_drift_fraction=float(self.MAX_DRIFT_FRACTION))
+            max_drift_fraction=float(self.MAX_DRIFT_FRACTION),
+            jfa_warm_step=int(self.JFA_WARM_STEP))
 
     @classmethod
     def for_foam(cls, foam, **over) -> "FosConfig":

@@ -22,7 +22,8 @@ from .context import Context, stream
 class FoamSim:
     def __init__(self, cfg: FosConfig, pos: np.ndarray, rad: np.ndarray, use_graph: bool = True,
                  ctx: Context | None = None, device: int | None = None, surrogate=None,
-                 policy=None, surrogate_mode: str = "anchored"):
+                 policy=None, surrogate_mode: str = "anchored", jfa_warm: bool = False,
+                 warm_refresh: int = 0):
         n = int(rad.shape[0])
         self.cfg = cfg
         # learned FSC between JFA runs (fos.surrogate); None = the reference's stale reuse
@@ -32,6 +33,11 @@ class FoamSim:
             policy = RefreshPolicy(every=2 * cfg.JFA_CADENCE, warm_frames=cfg.JFA_WARM_FRAMES)
         self.policy = policy
         self.surrogate_mode = surrogate_mode
+        # warm-started JFA (fos_jfa_warm) on JFA frames after the first; with
+        # warm_refresh = k > 0 every k-th JFA frame is exact again
+        self.jfa_warm = bool(jfa_warm)
+        self.warm_refresh = int(warm_refresh)
+        self._jfa_runs = 0
         self.n = n
         self.use_graph = use_graph
         self.ctx = ctx or Context(cfg, max_n=n, max_res=cfg.JFA_RES, device=device)
@@ -60,20 +66,33 @@ class FoamSim:
 
     @classmethod
     def from_foam(cls, foam, use_graph: bool = True, surrogate=None, policy=None,
-                  surrogate_mode: str = "anchored", **over) -> "FoamSim":
+                  surrogate_mode: str = "anchored", jfa_warm: bool = False, warm_refresh: int = 0,
+                  **over) -> "FoamSim":
         return cls(FosConfig.for_foam(foam, **over), foam.pos, foam.rad, use_graph=use_graph,
-                   surrogate=surrogate, policy=policy, surrogate_mode=surrogate_mode)
+                   surrogate=surrogate, policy=policy, surrogate_mode=surrogate_mode,
+                   jfa_warm=jfa_warm, warm_refresh=warm_refresh)
+
+    def _jfa_kind(self, jfa: bool) -> int:
+        """0 no JFA, 1 the exact JFA, 2 the warm-started one."""
+        if not jfa:
+            return 0
+        k = self._jfa_runs
+        self._jfa_runs += 1
+        if not self.jfa_warm or k == 0 or (self.warm_refresh and k % self.warm_refresh == 0):
+            return 1
+        return 2
 
     def initialize(self, frame0: int = 0):
         """initialize_simulation's device part (run.py:320-382)."""
         call("fos_sim_init", self.ctx.h, C.byref(self.state), C.byref(self.fp), int(frame0),
              stream())
         self.frame = int(frame0)
+        self._jfa_runs = 0
 
     def step(self):
         if self.surrogate is not None:
             return self._step_surrogate()
-        jfa = 1 if self.cfg.is_jfa_frame(self.frame) else 0
+        jfa = self._jfa_kind(self.cfg.is_jfa_frame(self.frame))
         fn = "fos_frame_graph" if self.use_graph else "fos_frame"
         call(fn, self.ctx.h, C.byref(self.state), C.byref(self.fp), jfa, stream())
         self.frame += 1
@@ -108,7 +127,7 @@ class FoamSim:
 
     def step_profiled(self) -> dict:
         """One frame (no graph) with CUDA events between stages -> ms per stage."""
-        jfa = 1 if self.cfg.is_jfa_frame(self.frame) else 0
+        jfa = self._jfa_kind(self.cfg.is_jfa_frame(self.frame))
         ms = (C.c_float * len(self.STAGES))()
         call("fos_frame_profile", self.ctx.h, C.byref(self.state), C.byref(self.fp), jfa, ms,
              stream())

@@ -28,6 +28,7 @@ fsc = fsc_ema = face_ids = face_counts = neighbor_list = None
 neighbor_count = neighbor_used_count = neighbor_prev_scores = None
 power_beta_current = None
 tile_dirty = pos_prev = rad_prev = None
+_tile_store = None
 
 
 class Field:
@@ -90,8 +91,10 @@ def init_jfa(max_particles: int | None = None, max_res: int | None = None):
     neighbor_count = neighbor_used_count
     neighbor_prev_scores = Field(ctx.neighbor_prev_scores)
     power_beta_current = _PowerBeta()
+    global _tile_store
     max_tiles = (ctx.max_res + 15) // 16
-    tile_dirty = Field(torch.zeros((max_tiles,) * 3, dtype=torch.uint8, device="cuda"))
+    _tile_store = torch.zeros(max_tiles ** 3, dtype=torch.uint8, device="cuda")
+    tile_dirty = Field(_tile_store[:1].view(1, 1, 1))
     pos_prev = Field(torch.zeros((ctx.max_n, 3), dtype=torch.float32, device="cuda"))
     rad_prev = Field(torch.zeros((ctx.max_n,), dtype=torch.float32, device="cuda"))
     set_resolution(cfg.JFA_RES)
@@ -109,6 +112,10 @@ def set_resolution(new_res: int):
     VOXEL_SIZE = cfg.DOMAIN_SIZE / JFA_RES
     JFA_NUM_PASSES = ctx.num_passes
     tiles_per_axis = (JFA_RES + 15) // 16  # JFA_TILE_SIZE = 16 (config.py:182)
+    if tile_dirty is not None:
+        # [t, t, t] view of the contiguous first t^3 bytes (fos_dirty_* layout)
+        t = tiles_per_axis
+        tile_dirty.tensor = _tile_store[: t ** 3].view(t, t, t)
 
 
 def run_jfa(pos, rad, active_n: int):
@@ -131,34 +138,28 @@ def validate_jfa(active_n: int) -> dict:
 
 # ---------------------------------------------------------------- dirty tiles
 # Instrumentation only in the reference (jfa.py:966-1049; run.py:1021-1047):
-# it never changes JFA output.  Kept for call-surface parity.
+# it never changes JFA output.
 def mark_dirty_tiles(pos, rad, n: int):
-    """jfa.mark_dirty_tiles (jfa.py:966-1008)."""
+    """jfa.mark_dirty_tiles (jfa.py:966-1008) on libfos (fos_dirty_mark)."""
+    from ._lib import call
+    from .context import ptr, stream
     cfg = runtime.config()
-    p, r = _tensor(pos)[:n], _tensor(rad)[:n]
-    pp, rp = pos_prev.tensor[:n], rad_prev.tensor[:n]
-    vs = cfg.DOMAIN_SIZE / JFA_RES
-    R = JFA_RES
-
-    def tile(x):
-        v = torch.floor(((x + 0.5 * cfg.DOMAIN_SIZE) / cfg.DOMAIN_SIZE) * R).to(torch.int64)
-        return torch.remainder(v, R) // 16
-
-    tc, tp = tile(p), tile(pp)
-    dirty = ((p - pp).norm(dim=1) > 0.5 * vs) | ((r - rp).abs() > 0.25 * vs) | (tc != tp).any(1)
-    t = tiles_per_axis
-    idx = tc[dirty]
-    for dz in (-1, 0, 1):
-        for dy in (-1, 0, 1):
-            for dx in (-1, 0, 1):
-                q = torch.remainder(idx + torch.tensor([dx, dy, dz], device=idx.device), t)
-                tile_dirty.tensor[q[:, 0], q[:, 1], q[:, 2]] = 1
+    call("fos_dirty_mark", runtime.ctx().h, ptr(_tensor(pos), torch.float32, "pos"),
+         ptr(_tensor(rad), torch.float32, "rad"), ptr(pos_prev.tensor, torch.float32, "pos_prev"),
+         ptr(rad_prev.tensor, torch.float32, "rad_prev"), int(n),
+         float(cfg.JFA_DIRTY_POS_THRESHOLD), float(cfg.JFA_DIRTY_RAD_THRESHOLD),
+         int(cfg.JFA_DIRTY_HALO), ptr(tile_dirty.tensor, torch.uint8, "tile_dirty"), stream())
 
 
 def count_dirty_tiles() -> int:
-    """jfa.count_dirty_tiles (jfa.py:1011-1024)."""
-    t = tiles_per_axis
-    return int((tile_dirty.tensor[:t, :t, :t] == 1).sum().item())
+    """jfa.count_dirty_tiles (jfa.py:1011-1024) on libfos (fos_dirty_count)."""
+    import ctypes as C
+    from ._lib import call
+    from .context import ptr, stream
+    out = C.c_int()
+    call("fos_dirty_count", runtime.ctx().h, ptr(tile_dirty.tensor, torch.uint8, "tile_dirty"),
+         C.byref(out), stream())
+    return int(out.value)
 
 
 def clear_dirty_tiles():

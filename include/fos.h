@@ -102,6 +102,16 @@ int fos_jfa_fields(FosCtx* ctx, FosJfaFields* out);
  * land in the context's fields; nothing is copied to the host. */
 int fos_jfa_run(FosCtx* ctx, const float* pos, const float* rad, int n, fos_stream_t s);
 
+/* Warm-started JFA (no reference counterpart; run.py only plans it,
+ * docs/GITHUB_ISSUES.md:225-300): the previous run's final owner grid is the
+ * starting point, every seed is planted again at its current voxel, and the
+ * passes run with steps first_step, first_step/2, ..., 1, 1 (first_step a
+ * power of two <= res/2) instead of res/2 ... 1, 1.  Needs a previous run at
+ * the same resolution.  An approximation of fos_jfa_init + fos_jfa_passes:
+ * agreement with the exact run is measured, not guaranteed. */
+int fos_jfa_warm(FosCtx* ctx, const float* pos, const float* rad, int n, int first_step,
+                 fos_stream_t s);
+
 /* The stages of fos_jfa_run one by one (for tests and the Python mirror). */
 int fos_jfa_init(FosCtx* ctx, const float* pos, const float* rad, int n, fos_stream_t s); /* jfa.py:484-520 */
 int fos_jfa_passes(FosCtx* ctx, int n, fos_stream_t s);          /* jfa.py:1082-1116 (uses the seed table) */
@@ -265,6 +275,7 @@ typedef struct FosFrameParams {
     double jitter_tau;            /* JITTER_TAU: OU time scale (s) */
     double dt;                    /* DT: time step of the OU update (s) */
     double max_drift_fraction;    /* MAX_DRIFT_FRACTION: step cap, in GAP_FRACTION*(2r) */
+    int jfa_warm_step;            /* first step of a warm-started JFA (jfa_frame == 2) */
 } FosFrameParams;
 
 /* Caller-owned per-particle state (run.py's fields). */
@@ -288,6 +299,8 @@ void fos_frame_params_default(FosFrameParams* fp);
  * rad and reset the device frame index to frame0 and the settle counter. */
 int fos_sim_init(FosCtx* ctx, const FosState* st, const FosFrameParams* fp, int frame0,
                  fos_stream_t s);
+/* jfa_frame: 0 no JFA, 1 the exact JFA, 2 the warm-started JFA (fos_jfa_warm
+ * with fp->jfa_warm_step). */
 int fos_frame(FosCtx* ctx, const FosState* st, const FosFrameParams* fp, int jfa_frame,
               fos_stream_t s);
 /* Same frame replayed from a CUDA graph captured on first use per
@@ -338,6 +351,19 @@ int fos_skip_signals(FosCtx* ctx, const FosState* st, const float* pos_prev,
  * clears the device error word) and read (synchronises). */
 int fos_sim_set_counters(FosCtx* ctx, int frame, int settle, fos_stream_t s);
 int fos_sim_counters(FosCtx* ctx, int* frame, int* settle, fos_stream_t s);
+
+/* ------------------------------------------------------------ dirty tiles
+ * mark_dirty_tiles (jfa.py:966-1008) on the current resolution's tiles of
+ * 16^3 voxels (tiles_per_axis = ceil(res / 16)), tile_dirty [t][t][t] uint8:
+ * a particle whose position moved more than pos_threshold * VOXEL_SIZE, whose
+ * radius changed more than rad_threshold * VOXEL_SIZE, or whose tile changed
+ * since (pos_prev, rad_prev) marks its tile and the halo around it.
+ * clear_dirty_tiles and update_tile_cache are a memset and a copy. */
+int fos_dirty_mark(FosCtx* ctx, const float* pos, const float* rad, const float* pos_prev,
+                   const float* rad_prev, int n, double pos_threshold, double rad_threshold,
+                   int halo, uint8_t* tile_dirty, fos_stream_t s);
+/* count_dirty_tiles (jfa.py:1011-1024).  Synchronises. */
+int fos_dirty_count(FosCtx* ctx, const uint8_t* tile_dirty, int* count, fos_stream_t s);
 
 /* ------------------------------------------------------------ topology
  * Gabriel-graph / k-NN topological degree over the hash grid (topology.py),

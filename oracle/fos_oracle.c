@@ -517,6 +517,40 @@ void orc_brownian(float* pos, int n, float strength, float domain, uint64_t seed
     }
 }
 
+/* ---------------------------------------------------------- dirty tiles
+ * mark_dirty_tiles / count_dirty_tiles (jfa.py:966-1024); tiles of 16^3
+ * voxels, dirty[t][t][t] uint8; pos_thr / rad_thr already scaled by
+ * VOXEL_SIZE (folded in double, rounded to float32). */
+void orc_dirty_mark(const float* pos, const float* rad, const float* pos_prev,
+                    const float* rad_prev, int n, int R, float halfL, float L, float pos_thr,
+                    float rad_thr, int halo, uint8_t* dirty) {
+    int t = (R + 15) / 16;
+    for (int i = 0; i < n; ++i) {
+        const float* p = &pos[3 * i];
+        const float* q = &pos_prev[3 * i];
+        float dx = p[0] - q[0], dy = p[1] - q[1], dz = p[2] - q[2];
+        float dpos = sqrtf(dx * dx + dy * dy + dz * dz);
+        float drad = fabsf(rad[i] - rad_prev[i]);
+        int tc[3], moved = 0;
+        for (int k = 0; k < 3; ++k) {
+            tc[k] = w2v(p[k], halfL, L, R) / 16;
+            moved |= tc[k] != w2v(q[k], halfL, L, R) / 16;
+        }
+        if (!(dpos > pos_thr || drad > rad_thr || moved)) continue;
+        for (int oz = -halo; oz <= halo; ++oz)
+            for (int oy = -halo; oy <= halo; ++oy)
+                for (int ox = -halo; ox <= halo; ++ox)
+                    dirty[((size_t)wrapi(tc[0] + ox, t) * t + wrapi(tc[1] + oy, t)) * t +
+                          wrapi(tc[2] + oz, t)] = 1;
+    }
+}
+
+int orc_dirty_count(const uint8_t* dirty, int R) {
+    int t = (R + 15) / 16, c = 0;
+    for (int k = 0; k < t * t * t; ++k) c += dirty[k] == 1;
+    return c;
+}
+
 /* ------------------------------------------------------------- topology
  * topology.py restated with serial semantics.  Grid arguments are the CSR
  * arrays of orc_grid_build (each cell's particles ascending). */

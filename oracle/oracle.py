@@ -63,6 +63,8 @@ def lib():
             "orc_philox": (None, [C.c_uint32] * 6 + [_p]),
             "orc_brownian": (None, [_p, _i, _f, _f, C.c_uint64, C.c_uint32]),
             "orc_mean_radius": (_f, [_p, _i]),
+            "orc_dirty_mark": (None, [_p, _p, _p, _p, _i, _i, _f, _f, _f, _f, _i, _p]),
+            "orc_dirty_count": (_i, [_p, _i]),
             "orc_topo_candidates": (None, [_p, _p, _p, _p, _p, _i, _i, _f, _f, _f, _f, _i, _p,
                                            _p, _p]),
             "orc_topo_gabriel": (None, [_p, _p, _p, _p, _i, _i, _f, _f, _f, _f, _i, _i, _i,
@@ -318,6 +320,19 @@ def set_threads(t: int):
 
 def num_threads() -> int:
     return int(lib().orc_num_threads())
+
+
+# --------------------------------------------------------------- dirty tiles
+def dirty_mark(pos, rad, pos_prev, rad_prev, dirty, p: OracleParams, pos_frac=0.5,
+               rad_frac=0.25, halo=1):
+    vs = p.L / p.R
+    lib().orc_dirty_mark(_ptr(pos), _ptr(rad), _ptr(pos_prev), _ptr(rad_prev), p.n, p.R,
+                         p.halfL, _f32(p.L), _f32(pos_frac * vs), _f32(rad_frac * vs), int(halo),
+                         _ptr(dirty))
+
+
+def dirty_count(dirty, R: int) -> int:
+    return int(lib().orc_dirty_count(_ptr(dirty), int(R)))
 
 
 # ------------------------------------------------------------------ topology
