@@ -610,6 +610,7 @@ def run_warm_jfa(foam, flush):
             J.mark_dirty_tiles(sim.pos, sim.rad, n)
             out["dirty_tiles"] = [J.count_dirty_tiles(), J.tiles_per_axis ** 3]
             runtime.ctx().close()
+            runtime._ctx = None
     out["frames_per_s"] = {k: round(v, 2) for k, v in fps.items()}
     out["speedup"] = round(fps["warm"] / fps["exact"], 4)
     return out
