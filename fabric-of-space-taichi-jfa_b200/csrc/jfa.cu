@@ -306,7 +306,9 @@ __device__ __forceinline__ int fin_row(int i, const int32_t* __restrict__ revsta
     return changed;
 }
 
-__global__ void __launch_bounds__(256) k_finalize(int n, const int32_t* __restrict__ revstart,
+#define FIN_THREADS 64
+
+__global__ void __launch_bounds__(FIN_THREADS) k_finalize(int n, const int32_t* __restrict__ revstart,
                                                   const int32_t* __restrict__ rev,
                                                   uint8_t* acc0, uint8_t* acc1,
                                                   const float* __restrict__ score,
@@ -569,16 +571,18 @@ static int finalize_impl(FosCtx* c, const float* rad, int n, bool apply_ema, cud
     FOS_LAUNCHED(c);
     k_rev_sort<<<fos_blocks(32LL * n, 256), 256, 0, s>>>(n, c->revstart, c->rev);
     FOS_LAUNCHED(c);
+    // 64-thread blocks spread the rows over every SM (each row is a serial
+    // chain of dependent loads, so more SMs in flight, not more threads per SM)
     int per_sm = 0;
-    FOS_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_finalize, 256, 0));
-    int grid = nb;
+    FOS_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_finalize, FIN_THREADS, 0));
+    int grid = fos_blocks(n, FIN_THREADS);
     int cap = per_sm * c->num_sms;
     if (grid > cap) grid = cap;
     if (grid < 1) grid = 1;
     int max_it = n + 2 < FOS_FIN_MAXIT ? n + 2 : FOS_FIN_MAXIT;
     cudaLaunchConfig_t cfg = {};
     cfg.gridDim = dim3(grid);
-    cfg.blockDim = dim3(256);
+    cfg.blockDim = dim3(FIN_THREADS);
     cfg.stream = s;
     cudaLaunchAttribute attr[1];
     attr[0].id = cudaLaunchAttributeCooperative;
