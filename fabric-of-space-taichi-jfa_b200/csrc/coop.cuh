@@ -64,6 +64,15 @@ __device__ __forceinline__ int coop_block_scan(int v, int* total) {
 
 #define COOP_CAP 32  // slots per cell of the fixed-capacity rows (one warp sorts a row)
 
+// Thread index for per-particle loops of the persistent kernels: 32
+// consecutive particles per warp (coalesced accesses), consecutive warps of
+// particles on consecutive blocks, so n < gridDim.x * blockDim.x particles
+// spread over every SM instead of filling the first blocks.  A bijection of
+// [0, gridDim.x * blockDim.x) for blockDim.x a multiple of 32.
+__device__ __forceinline__ int spread_tid() {
+    return (int)((((threadIdx.x >> 5) * gridDim.x + blockIdx.x) << 5) + (threadIdx.x & 31));
+}
+
 // One rebuild's grid as its consumers (max overlap, PBD) see it.  Both forms
 // hold each cell's particles in ascending index order, so a stencil walk
 // visits candidates in the reference's order either way; slot_of[i] (an
@@ -191,7 +200,7 @@ __device__ bool coop_grid(const Args& a, const Geo& geo, const float* src, float
     int32_t* cnt = par ? a.cnt2 : a.cnt;
     int32_t* cnt_next = par ? a.cnt : a.cnt2;
     if (!p1_done) {
-        for (int i = tid; i < a.n; i += T) coop_p1_one(a, geo, i, src, rad, dst, par);
+        for (int i = spread_tid(); i < a.n; i += T) coop_p1_one(a, geo, i, src, rad, dst, par);
         if (!grid_barrier(a.ds, ep)) return false;
         trace_mark(a, tk);
     }
@@ -258,12 +267,12 @@ __device__ bool coop_grid(const Args& a, const Geo& geo, const float* src, float
         }
         if (threadIdx.x == 0) s_tab[a.G3] = tot;
         __syncthreads();
-        for (int i = tid; i < a.n; i += T)
+        for (int i = spread_tid(); i < a.n; i += T)
             a.ci_tmp[s_tab[__ldcg(&a.cellof[i])] + __ldcg(&a.rank[i])] = i;
         if (!grid_barrier(a.ds, ep)) return false;
         trace_mark(a, tk);
         // P3: stable placement from the block's copy of the starts
-        for (int i = tid; i < a.n; i += T) {
+        for (int i = spread_tid(); i < a.n; i += T) {
             int c = __ldcg(&a.cellof[i]);
             int b = s_tab[c], e = s_tab[c + 1];
             int r = 0;
@@ -310,7 +319,7 @@ __device__ bool coop_grid(const Args& a, const Geo& geo, const float* src, float
         for (int c = c0 + threadIdx.x; c < c0 + a.chunk && c < a.G3; c += blockDim.x) {
             a.cs[c] = __ldcg(&a.part[c]) + s_pre[blockIdx.x];
         }
-        for (int i = tid; i < a.n; i += T) {
+        for (int i = spread_tid(); i < a.n; i += T) {
             int c = __ldcg(&a.cellof[i]);
             int slot = __ldcg(&a.part[c]) + s_pre[c / a.chunk] + __ldcg(&a.rank[i]);
             a.ci_tmp[slot] = i;
@@ -319,7 +328,7 @@ __device__ bool coop_grid(const Args& a, const Geo& geo, const float* src, float
     if (!grid_barrier(a.ds, ep)) return false;
     trace_mark(a, tk);
     // P4: stable placement: slot = cell start + #(lower-indexed particles in the cell)
-    for (int i = tid; i < a.n; i += T) {
+    for (int i = spread_tid(); i < a.n; i += T) {
         int c = __ldcg(&a.cellof[i]);
         int b = __ldcg(&a.cs[c]), e = b + __ldcg(&a.cc[c]);
         int r = 0;

@@ -882,14 +882,14 @@ static int ens_finalize_targets(FosEnsemble* e, cudaStream_t s) {
     k_rev_sort<<<fos_blocks(32LL * n, 256), 256, 0, s>>>(n, c->revstart, c->rev);
     FOS_LAUNCHED(c);
     int per_sm = 0;
-    FOS_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_finalize, 256, 0));
-    int grid = nb, cap = per_sm * c->num_sms;
+    FOS_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_finalize, FIN_THREADS, 0));
+    int grid = fos_blocks(n, FIN_THREADS), cap = per_sm * c->num_sms;
     if (grid > cap) grid = cap;
     if (grid < 1) grid = 1;
     const int max_it = n + 2 < FOS_FIN_MAXIT ? n + 2 : FOS_FIN_MAXIT;
     cudaLaunchConfig_t cfg = {};
     cfg.gridDim = dim3(grid);
-    cfg.blockDim = dim3(256);
+    cfg.blockDim = dim3(FIN_THREADS);
     cfg.stream = s;
     cudaLaunchAttribute attr[1];
     attr[0].id = cudaLaunchAttributeCooperative;

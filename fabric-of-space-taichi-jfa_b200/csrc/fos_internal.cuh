@@ -60,6 +60,9 @@ struct FosSurBufs;  // surrogate.cu
 
 #define FOS_SKIP_BLOCKS 1024
 #define FOS_GRAPH_SLOTS 6
+// block size of the cooperative finalize kernel: small blocks spread its rows
+// (serial chains of dependent loads) over every SM
+#define FIN_THREADS 64
 
 struct FosCtx {
     int device = 0;

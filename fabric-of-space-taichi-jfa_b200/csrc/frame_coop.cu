@@ -104,7 +104,7 @@ __global__ void __launch_bounds__(COOP_THREADS) k_frame_coop(CoopArgs a) {
         const bool nudge = *((volatile int*)&a.ds->settle) > 0;
         const float bg = back_global_from_bits(*((volatile unsigned int*)&a.ds->omax_bits),
                                                a.contact_tol_d);
-        for (int i = tid; i < a.n; i += T) {
+        for (int i = spread_tid(); i < a.n; i += T) {
             float r = __ldcg(&a.rad[i]);
             if (nudge) {
                 r = nudge_one(r, __ldcg(&a.rad_target[i]), __ldcg(&a.lmd[i]), a.alpha,
@@ -159,7 +159,7 @@ __global__ void __launch_bounds__(COOP_THREADS) k_frame_coop(CoopArgs a) {
     {
         unsigned int frame = (unsigned int)pa.frame;
         long long rq = 0;
-        for (int i = tid; i < a.n; i += T) {
+        for (int i = spread_tid(); i < a.n; i += T) {
             if (a.sweeps & 1) a.rad[i] = __ldcg(&a.rad_tmp[i]);
             if (a.ou) rq += rad_fixed(__ldcg(&a.rad[i]));
             brownian_one<LdL2>(i, (unsigned int)i, a.pos, a.strength, a.domain, a.halfL, a.k0,

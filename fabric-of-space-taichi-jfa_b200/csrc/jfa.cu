@@ -306,8 +306,6 @@ __device__ __forceinline__ int fin_row(int i, const int32_t* __restrict__ revsta
     return changed;
 }
 
-#define FIN_THREADS 64
-
 __global__ void __launch_bounds__(FIN_THREADS) k_finalize(int n, const int32_t* __restrict__ revstart,
                                                   const int32_t* __restrict__ rev,
                                                   uint8_t* acc0, uint8_t* acc1,
