@@ -123,10 +123,13 @@ __global__ void __launch_bounds__(COOP_THREADS) k_frame_coop(CoopArgs a) {
     const int groups_per_round = T / 8;
     const int p_rounds = (a.n + groups_per_round - 1) / groups_per_round;
     // with one round (n <= T/8) each lane keeps its neighbours in registers
-    // for all sweeps, and particle i goes to block i % blocks, so every SM
-    // issues the same share of the sweep
+    // for all sweeps, and the particles are spread over every block, so every
+    // SM issues the same share of the sweep
     const bool keep_nbr = p_rounds == 1;
-    const int i_one = (int)(threadIdx.x >> 3) * (int)gridDim.x + (int)blockIdx.x;
+    // four consecutive particles per warp (one sector of each per-particle
+    // array), consecutive warps of particles on consecutive blocks
+    const int i_one =
+        (int)((((threadIdx.x >> 5) * gridDim.x + blockIdx.x) << 2) + ((threadIdx.x >> 3) & 3));
     const PressureNbr nb0 = pressure_nbr8x2<LdL2>(i_one, lane, pa);
     for (int w = 0; w < a.sweeps; ++w) {
         const float* rin = (w & 1) ? a.rad_tmp : a.rad;
