@@ -62,10 +62,12 @@ __device__ __forceinline__ void jfa_pass_body(const int32_t* __restrict__ in,
         z = (int)(l & (R - 1));
         y = (int)((l >> lgR) & (R - 1));
         x = (int)(l >> (2 * lgR));
-    } else {
-        z = (int)(l % R);
-        y = (int)((l / R) % R);
-        x = (int)(l / ((long long)R * R));
+    } else {  // 32-bit: R <= 512
+        const int l32 = (int)l;
+        z = l32 % R;
+        const int t = l32 / R;
+        y = t % R;
+        x = t / R;
     }
     int xs[3], ys[3], zs[3];
 #pragma unroll
@@ -134,24 +136,42 @@ __device__ __forceinline__ void jfa_pass_body(const int32_t* __restrict__ in,
     if (threadIdx.x == 0 && cnt) atomicAdd(&changes[pass], (unsigned long long)cnt);
 }
 
+// Voxel coordinates of linear index l (z fastest) in 32-bit arithmetic
+// (R <= 512, so R^3 < 2^31): shifts for a power-of-two R, else divisions.
+__device__ __forceinline__ void vox_xyz(int l, int R, int& x, int& y, int& z) {
+    if ((R & (R - 1)) == 0) {
+        const int lg = __ffs(R) - 1;
+        z = l & (R - 1);
+        y = (l >> lg) & (R - 1);
+        x = l >> (2 * lg);
+    } else {
+        z = l % R;
+        const int t = l / R;
+        y = t % R;
+        x = t / R;
+    }
+}
+
 // One voxel of the majority filter: lab is the final owner grid of R^3.
 __device__ __forceinline__ void majority_body(const int32_t* __restrict__ lab, int R,
                                               int32_t* __restrict__ outp, long long lin) {
-    long long V = (long long)R * R * R;
+    const int V = R * R * R;
     if (lin >= V) return;
-    int z = (int)(lin % R), y = (int)((lin / R) % R), x = (int)(lin / ((long long)R * R));
-    int me = lab[lin];
+    const int l = (int)lin;
+    int x, y, z;
+    vox_xyz(l, R, x, y, z);
+    int me = lab[l];
     if (me < 0) {
-        outp[lin] = -1;
+        outp[l] = -1;
         return;
     }
     int nb[6];
-    nb[0] = lab[((long long)wrap_small(x - 1, R) * R + y) * R + z];
-    nb[1] = lab[((long long)wrap_small(x + 1, R) * R + y) * R + z];
-    nb[2] = lab[((long long)x * R + wrap_small(y - 1, R)) * R + z];
-    nb[3] = lab[((long long)x * R + wrap_small(y + 1, R)) * R + z];
-    nb[4] = lab[((long long)x * R + y) * R + wrap_small(z - 1, R)];
-    nb[5] = lab[((long long)x * R + y) * R + wrap_small(z + 1, R)];
+    nb[0] = lab[(wrap_small(x - 1, R) * R + y) * R + z];
+    nb[1] = lab[(wrap_small(x + 1, R) * R + y) * R + z];
+    nb[2] = lab[(x * R + wrap_small(y - 1, R)) * R + z];
+    nb[3] = lab[(x * R + wrap_small(y + 1, R)) * R + z];
+    nb[4] = lab[(x * R + y) * R + wrap_small(z - 1, R)];
+    nb[5] = lab[(x * R + y) * R + wrap_small(z + 1, R)];
     int ids[7], cnt[7], nu = 1;
     ids[0] = me;
     cnt[0] = 1;
@@ -184,7 +204,7 @@ __device__ __forceinline__ void majority_body(const int32_t* __restrict__ lab, i
             mc = cnt[u];
             best = ids[u];
         }
-    outp[lin] = best;
+    outp[l] = best;
 }
 
 // ------------------------------------------------------------ face pairs
@@ -238,24 +258,21 @@ __device__ __forceinline__ void faces_body(const int32_t* __restrict__ filt, int
                                            unsigned int* hcnt, unsigned int* claimed,
                                            FosDevState* ds, unsigned long long mask,
                                            long long lin) {
-    long long V = (long long)R * R * R;
+    const int V = R * R * R;
     bool live = lin < V;
+    const int l = live ? (int)lin : 0;
     int lane = threadIdx.x & 31;
-    int a = live ? filt[lin] : -1;
+    int a = live ? filt[l] : -1;
     bool va = a >= 0 && a < n;
     int z = 0, y = 0, x = 0;
-    if (live) {
-        z = (int)(lin % R);
-        y = (int)((lin / R) % R);
-        x = (int)(lin / ((long long)R * R));
-    }
+    if (live) vox_xyz(l, R, x, y, z);
 #pragma unroll
     for (int ax = 0; ax < 3; ++ax) {
-        long long nlin = 0;
+        int nlin = 0;
         if (live) {
-            if (ax == 0) nlin = ((long long)wrap_small(x + 1, R) * R + y) * R + z;
-            else if (ax == 1) nlin = ((long long)x * R + wrap_small(y + 1, R)) * R + z;
-            else nlin = ((long long)x * R + y) * R + wrap_small(z + 1, R);
+            if (ax == 0) nlin = (wrap_small(x + 1, R) * R + y) * R + z;
+            else if (ax == 1) nlin = (x * R + wrap_small(y + 1, R)) * R + z;
+            else nlin = (x * R + y) * R + wrap_small(z + 1, R);
         }
         int b = va ? filt[nlin] : -1;
         bool valid = va && b >= 0 && b < n && b != a;
@@ -264,7 +281,8 @@ __device__ __forceinline__ void faces_body(const int32_t* __restrict__ filt, int
         if (valid) {
             int lo = a < b ? a : b, hi = a < b ? b : a;
             pk = ((unsigned long long)(unsigned int)lo << 32) | (unsigned int)hi;
-            fk = (a < b) ? (unsigned int)(lin * 6 + ax * 2 + 1) : (unsigned int)(nlin * 6 + ax * 2);
+            fk = (a < b) ? (unsigned int)l * 6u + (unsigned int)(ax * 2 + 1)
+                         : (unsigned int)nlin * 6u + (unsigned int)(ax * 2);
         }
         unsigned int m = __ballot_sync(0xffffffffu, valid);
         if (valid) {
