@@ -299,6 +299,8 @@ struct EnsArgs {
     const float* rad_target;
     float* lmd;
     float* delta_r;
+    float* vol0;  // [n] r^P ping-pong of the pressure sweeps
+    float* vol1;
     float gap1, mdf, dmul, eps, contact_tol;
     double contact_tol_d;
     float alpha, max_step;
@@ -380,17 +382,20 @@ __global__ void __launch_bounds__(THREADS) k_ens_coop(EnsArgs a) {
         }
     }
     if (!grid_barrier(a.ds, ep)) return;
-    // (3) settle nudge of the foams whose settle counter is > 0
+    // (3) settle nudge of the foams whose settle counter is > 0; each final
+    // radius's power r^P seeds the pressure sweeps
     for (int i = tid; i < a.n; i += T) {
         const int f = a.foam_of[i];
+        float r = __ldcg(&a.rad[i]);
         if (*((volatile int*)&a.W[f].settle) > 0) {
             const EnsFoamDev& d = a.F[f];
             float bg = back_global_from_bits(*((volatile unsigned int*)&a.W[f].omax_bits),
                                              a.contact_tol_d);
-            a.rad[i] = nudge_one(__ldcg(&a.rad[i]), __ldcg(&a.rad_target[i]), __ldcg(&a.lmd[i]),
-                                 a.alpha, a.max_step, d.r_min, d.r_max, bg, a.bp_mode,
-                                 a.contact_tol);
+            r = nudge_one(r, __ldcg(&a.rad_target[i]), __ldcg(&a.lmd[i]), a.alpha, a.max_step,
+                          d.r_min, d.r_max, bg, a.bp_mode, a.contact_tol);
+            a.rad[i] = r;
         }
+        if (a.sweeps > 0) a.vol0[i] = powf(r, a.pa.P);
     }
     if (!grid_barrier(a.ds, ep)) return;
     // (4) pressure sweeps with each foam's bounds and local hash index
@@ -401,6 +406,8 @@ __global__ void __launch_bounds__(THREADS) k_ens_coop(EnsArgs a) {
         for (int w = 0; w < a.sweeps; ++w) {
             const float* rin = (w & 1) ? a.rad_tmp : a.rad;
             float* rout = (w & 1) ? a.rad : a.rad_tmp;
+            const float* vin = (w & 1) ? a.vol1 : a.vol0;
+            float* vout = (w == a.sweeps - 1) ? nullptr : ((w & 1) ? a.vol0 : a.vol1);
             for (int r = 0; r < p_rounds; ++r) {
                 int i = r * groups_per_round + tid / 8;
                 PressureArgs pa = a.pa;
@@ -411,7 +418,8 @@ __global__ void __launch_bounds__(THREADS) k_ens_coop(EnsArgs a) {
                     pa.rmax = d.r_max;
                     pa.hoff = d.part_off;
                 }
-                pressure_group8x2<LdL2>(i, lane, pa, rin, rout, a.delta_r);
+                const PressureNbr nb = pressure_nbr8x2<LdL2>(i, lane, pa);
+                pressure_sweep8x2v<LdL2>(i, lane, pa, nb, rin, vin, rout, vout, a.delta_r);
             }
             if (!grid_barrier(a.ds, ep)) return;
         }
@@ -725,6 +733,8 @@ static int ens_coop_launch(FosEnsemble* e, int mode, cudaStream_t s) {
     a.rad_target = e->rad_target;
     a.lmd = e->lmd;
     a.delta_r = e->delta_r;
+    a.vol0 = c->pvol;
+    a.vol1 = c->pvol + c->max_n;
     a.gap1 = c->gap1;
     a.mdf = c->mdf;
     a.dmul = c->dmul;
