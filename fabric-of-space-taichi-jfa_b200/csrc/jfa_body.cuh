@@ -172,37 +172,27 @@ __device__ __forceinline__ void majority_body(const int32_t* __restrict__ lab, i
     nb[3] = lab[(x * R + wrap_small(y + 1, R)) * R + z];
     nb[4] = lab[(x * R + y) * R + wrap_small(z - 1, R)];
     nb[5] = lab[(x * R + y) * R + wrap_small(z + 1, R)];
-    int ids[7], cnt[7], nu = 1;
-    ids[0] = me;
-    cnt[0] = 1;
+    // The most frequent label among me and the six neighbours (unassigned
+    // neighbours do not count), ties to the first seen in the order me, nb[0],
+    // ..., nb[5]: the reference's insertion-order count, as 21 pairwise
+    // comparisons.  A later copy of a label has the same count as its first
+    // copy, so the strict '>' keeps the first.
+    int v[7] = {me, nb[0], nb[1], nb[2], nb[3], nb[4], nb[5]};
+    int c[7] = {1, 1, 1, 1, 1, 1, 1};
 #pragma unroll
-    for (int k = 0; k < 6; ++k) {
-        int id = nb[k];
-        if (id >= 0) {
-            bool found = false;
+    for (int a = 0; a < 7; ++a)
 #pragma unroll
-            for (int u = 0; u < 7; ++u)
-                if (!found && u < nu && ids[u] == id) {
-                    cnt[u]++;
-                    found = true;
-                }
-            if (!found) {
-#pragma unroll
-                for (int u = 0; u < 7; ++u)
-                    if (u == nu) {
-                        ids[u] = id;
-                        cnt[u] = 1;
-                    }
-                nu++;
-            }
+        for (int b = a + 1; b < 7; ++b) {
+            const int e = v[a] == v[b] ? 1 : 0;
+            c[a] += e;
+            c[b] += e;
         }
-    }
     int mc = 0, best = me;
 #pragma unroll
-    for (int u = 0; u < 7; ++u)
-        if (u < nu && cnt[u] > mc) {
-            mc = cnt[u];
-            best = ids[u];
+    for (int k = 0; k < 7; ++k)
+        if (v[k] >= 0 && c[k] > mc) {
+            mc = c[k];
+            best = v[k];
         }
     outp[l] = best;
 }
@@ -218,13 +208,17 @@ __device__ __forceinline__ unsigned long long fmix64(unsigned long long k) {
     return k;
 }
 
-__device__ __forceinline__ void pair_insert(unsigned long long pk, unsigned int fk, unsigned int c,
-                                            unsigned long long* keys, unsigned int* hmin,
-                                            unsigned int* hcnt, unsigned int* claimed,
-                                            FosDevState* ds, unsigned long long mask) {
-    unsigned long long h = fmix64(pk) & mask;
+// Insert (or find) pair key pk in the open-addressed table and add its
+// count c and first-touch key fk.  h is the pair's home slot and k the key
+// already loaded from it (the caller issues the first probes of a warp's
+// three axes together).
+__device__ __forceinline__ void pair_insert_at(unsigned long long pk, unsigned int fk,
+                                               unsigned int c, unsigned long long h,
+                                               unsigned long long k, unsigned long long* keys,
+                                               unsigned int* hmin, unsigned int* hcnt,
+                                               unsigned int* claimed, FosDevState* ds,
+                                               unsigned long long mask) {
     for (unsigned long long probe = 0; probe <= mask; ++probe) {
-        unsigned long long k = keys[h];
         bool hit = (k == pk);
         if (!hit && k == EMPTY_KEY) {
             unsigned long long prev = atomicCAS(&keys[h], EMPTY_KEY, pk);
@@ -242,6 +236,7 @@ __device__ __forceinline__ void pair_insert(unsigned long long pk, unsigned int 
             return;
         }
         h = (h + 1) & mask;
+        k = keys[h];
     }
     atomicCAS(&ds->error, 0, (int)FOS_E_CAPACITY);
 }
@@ -266,31 +261,52 @@ __device__ __forceinline__ void faces_body(const int32_t* __restrict__ filt, int
     bool va = a >= 0 && a < n;
     int z = 0, y = 0, x = 0;
     if (live) vox_xyz(l, R, x, y, z);
+    // the three neighbour labels first, so their loads are in flight together
+    int nlin[3] = {0, 0, 0}, b[3];
+    if (live) {
+        nlin[0] = (wrap_small(x + 1, R) * R + y) * R + z;
+        nlin[1] = (x * R + wrap_small(y + 1, R)) * R + z;
+        nlin[2] = (x * R + y) * R + wrap_small(z + 1, R);
+    }
+#pragma unroll
+    for (int ax = 0; ax < 3; ++ax) b[ax] = va ? filt[nlin[ax]] : -1;
+    unsigned long long pk[3];
+    unsigned int mn[3], cntv[3];
+    bool lead[3];
 #pragma unroll
     for (int ax = 0; ax < 3; ++ax) {
-        int nlin = 0;
-        if (live) {
-            if (ax == 0) nlin = (wrap_small(x + 1, R) * R + y) * R + z;
-            else if (ax == 1) nlin = (x * R + wrap_small(y + 1, R)) * R + z;
-            else nlin = (x * R + y) * R + wrap_small(z + 1, R);
-        }
-        int b = va ? filt[nlin] : -1;
-        bool valid = va && b >= 0 && b < n && b != a;
-        unsigned long long pk = 0;
+        const bool valid = va && b[ax] >= 0 && b[ax] < n && b[ax] != a;
+        pk[ax] = 0;
         unsigned int fk = 0;
         if (valid) {
-            int lo = a < b ? a : b, hi = a < b ? b : a;
-            pk = ((unsigned long long)(unsigned int)lo << 32) | (unsigned int)hi;
-            fk = (a < b) ? (unsigned int)l * 6u + (unsigned int)(ax * 2 + 1)
-                         : (unsigned int)nlin * 6u + (unsigned int)(ax * 2);
+            int lo = a < b[ax] ? a : b[ax], hi = a < b[ax] ? b[ax] : a;
+            pk[ax] = ((unsigned long long)(unsigned int)lo << 32) | (unsigned int)hi;
+            fk = (a < b[ax]) ? (unsigned int)l * 6u + (unsigned int)(ax * 2 + 1)
+                             : (unsigned int)nlin[ax] * 6u + (unsigned int)(ax * 2);
         }
+        lead[ax] = false;
+        mn[ax] = 0;
+        cntv[ax] = 0;
         unsigned int m = __ballot_sync(0xffffffffu, valid);
         if (valid) {
-            unsigned int grp = __match_any_sync(m, pk);
-            unsigned int mn = __reduce_min_sync(grp, fk);
-            if (lane == __ffs(grp) - 1) pair_insert(pk, mn, __popc(grp), keys, hmin, hcnt, claimed, ds, mask);
+            unsigned int grp = __match_any_sync(m, pk[ax]);
+            mn[ax] = __reduce_min_sync(grp, fk);
+            cntv[ax] = __popc(grp);
+            lead[ax] = lane == __ffs(grp) - 1;
         }
     }
+    // first probes of the (up to) three inserts together, then each insert
+    unsigned long long h[3], k[3];
+#pragma unroll
+    for (int ax = 0; ax < 3; ++ax) {
+        h[ax] = fmix64(pk[ax]) & mask;
+        k[ax] = lead[ax] ? keys[h[ax]] : 0ull;
+    }
+#pragma unroll
+    for (int ax = 0; ax < 3; ++ax)
+        if (lead[ax])
+            pair_insert_at(pk[ax], mn[ax], cntv[ax], h[ax], k[ax], keys, hmin, hcnt, claimed, ds,
+                           mask);
 }
 
 // Per face slot t = a*32 + s: the normalised score of finalize_faces_kernel
