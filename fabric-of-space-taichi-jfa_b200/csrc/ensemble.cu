@@ -893,7 +893,7 @@ static int ens_finalize_targets(FosEnsemble* e, cudaStream_t s) {
     FOS_LAUNCHED(c);
     int per_sm = 0;
     FOS_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_finalize, FIN_THREADS, 0));
-    int grid = fos_blocks(n, FIN_THREADS), cap = per_sm * c->num_sms;
+    int grid = fos_blocks(32LL * n, FIN_THREADS), cap = per_sm * c->num_sms;
     if (grid > cap) grid = cap;
     if (grid < 1) grid = 1;
     const int max_it = n + 2 < FOS_FIN_MAXIT ? n + 2 : FOS_FIN_MAXIT;

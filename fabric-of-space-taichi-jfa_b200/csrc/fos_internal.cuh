@@ -60,9 +60,12 @@ struct FosSurBufs;  // surrogate.cu
 
 #define FOS_SKIP_BLOCKS 1024
 #define FOS_GRAPH_SLOTS 6
-// block size of the cooperative finalize kernel: small blocks spread its rows
-// (serial chains of dependent loads) over every SM
-#define FIN_THREADS 64
+// block size of the cooperative finalize kernel (one warp per row); 1024
+// threads at <= 32 registers keep two blocks (64 warps) on every SM and only
+// 296 blocks at each grid barrier
+#ifndef FIN_THREADS
+#define FIN_THREADS 1024
+#endif
 
 struct FosCtx {
     int device = 0;

@@ -278,35 +278,65 @@ __global__ void __launch_bounds__(256) k_rev_sort(int n, const int32_t* __restri
 // lower rows (Jacobi).  Row i depends only on rows a < i, so rows are final
 // after (1 + dependency depth) sweeps and a sweep with no change is the unique
 // fixed point, which equals the serial result.
-__device__ __forceinline__ int fin_row(int i, const int32_t* __restrict__ revstart,
-                                       const int32_t* __restrict__ rev,
-                                       const uint8_t* acc_in, uint8_t* acc_out,
-                                       const float* __restrict__ score, const float* __restrict__ prev,
-                                       float t_add, float t_drop) {
-    float app[FOS_S];
+//
+// One warp per row, lane s holding face slot s.  fin_app gathers the first
+// FOS_S accepted entries of row i's reverse list (sorted ascending, the serial
+// append order): lane p receives the score and the source particle of the
+// p-th one.  It returns how many were appended.
+__device__ __forceinline__ int fin_app(int i, int lane, const int32_t* __restrict__ revstart,
+                                       const int32_t* __restrict__ rev, const uint8_t* acc,
+                                       const float* __restrict__ score, float& appv, int& appi) {
+    const int b = revstart[i], e = revstart[i + 1];
     int used = 0;
-    int b = revstart[i], e = revstart[i + 1];
-    for (int k = b; k < e; ++k) {
-        int t = rev[k];
-        if (__ldcg(&acc_in[t]) && used < FOS_S) app[used++] = score[t];
-    }
-    int changed = 0;
-    for (int s = 0; s < FOS_S; ++s) {
-        size_t o = (size_t)i * FOS_S + s;
-        float sc = score[o];
-        uint8_t ok = 0;
-        if (sc >= 0.0f) {
-            float pr = (s < used) ? app[s] : prev[o];
-            ok = (sc >= t_add) || (pr >= t_drop && sc >= t_drop);
-            if (ok && used < FOS_S) app[used++] = sc;
+    for (int k0 = b; k0 < e && used < FOS_S; k0 += 32) {  // warp-uniform
+        const int k = k0 + lane;
+        const int t = k < e ? rev[k] : 0;
+        const bool a = k < e && __ldcg(&acc[t]);
+        const unsigned m = __ballot_sync(0xffffffffu, a);
+        const float st = a ? score[t] : 0.0f;
+        const int cnt = __popc(m), d = lane - used;
+        const bool mine = d >= 0 && d < cnt;
+        const int src = mine ? (int)__fns(m, 0, d + 1) : lane;
+        const float v = __shfl_sync(0xffffffffu, st, src);
+        const int ti = __shfl_sync(0xffffffffu, t, src);
+        if (mine) {
+            appv = v;
+            appi = ti >> 5;
         }
-        if (ok != __ldcg(&acc_in[o])) changed = 1;
-        __stcg(&acc_out[o], ok);
+        used += cnt;
     }
-    return changed;
+    return used < FOS_S ? used : FOS_S;
 }
 
-__global__ void __launch_bounds__(FIN_THREADS) k_finalize(int n, const int32_t* __restrict__ revstart,
+// Decisions of row i's own slots (bit s = slot s accepted) after `used`
+// appended entries.  ok = sc >= t_add, or sc >= t_drop and the score at
+// neighbour-list slot s is >= t_drop: the s-th appended entry while s is
+// below the running count (rev entries first, then this row's accepted slots
+// in slot order), else the previous frame's score.  Slots in the band
+// [t_drop, t_add) depend on the acceptances below them and are decided in
+// slot order; the others are fixed by their score alone.
+__device__ __forceinline__ unsigned fin_decide(int used, float sc, float pv, float appv,
+                                               float t_add, float t_drop) {
+    unsigned okm = __ballot_sync(0xffffffffu, sc >= 0.0f && sc >= t_add);
+    unsigned band = __ballot_sync(0xffffffffu, sc >= 0.0f && !(sc >= t_add) && sc >= t_drop);
+    while (band) {  // warp-uniform
+        const int s = __ffs(band) - 1;
+        band &= band - 1u;
+        const int below = __popc(okm & ((1u << s) - 1u));
+        int src = s;
+        float v = pv;
+        if (s < used) {
+            v = appv;
+        } else if (s < used + below) {
+            src = (int)__fns(okm, 0, s - used + 1);
+            v = sc;
+        }
+        if (__shfl_sync(0xffffffffu, v, src) >= t_drop) okm |= 1u << s;
+    }
+    return okm;
+}
+
+__global__ void __launch_bounds__(FIN_THREADS, 2048 / FIN_THREADS) k_finalize(int n, const int32_t* __restrict__ revstart,
                                                   const int32_t* __restrict__ rev,
                                                   uint8_t* acc0, uint8_t* acc1,
                                                   const float* __restrict__ score,
@@ -316,16 +346,28 @@ __global__ void __launch_bounds__(FIN_THREADS) k_finalize(int n, const int32_t* 
                                                   float t_drop, float alpha, int apply_ema,
                                                   FosDevState* ds, int* fin_changed,
                                                   int max_iters) {
-    int stride = gridDim.x * blockDim.x;
-    int tid = blockIdx.x * blockDim.x + threadIdx.x;
+    const int lane = threadIdx.x & 31;
+    const int wstride = gridDim.x * (blockDim.x >> 5);
+    const int w0 = (threadIdx.x >> 5) * gridDim.x + blockIdx.x;  // rows spread over all SMs
+    const bool lead = blockIdx.x == 0 && threadIdx.x == 0;
     uint8_t* cur = acc0;
     uint8_t* nxt = acc1;
     int it = 0;
     unsigned int epoch = 0;
     for (;;) {
         int ch = 0;
-        for (int i = tid; i < n; i += stride)
-            ch |= fin_row(i, revstart, rev, cur, nxt, score, prev, t_add, t_drop);
+        for (int i = w0; i < n; i += wstride) {
+            const size_t o = (size_t)i * FOS_S + lane;
+            const float sc = score[o];
+            const float pv = prev[o];
+            const uint8_t was = __ldcg(&cur[o]);
+            float appv = 0.0f;
+            int appi = 0;
+            const int used = fin_app(i, lane, revstart, rev, cur, score, appv, appi);
+            const uint8_t ok = (fin_decide(used, sc, pv, appv, t_add, t_drop) >> lane) & 1u;
+            __stcg(&nxt[o], ok);
+            ch |= ok != was;
+        }
         if (__syncthreads_or(ch) && threadIdx.x == 0) atomicOr(&fin_changed[it], 1);
         if (!grid_barrier(ds, epoch)) return;
         int any = *((volatile int*)&fin_changed[it]);
@@ -335,52 +377,50 @@ __global__ void __launch_bounds__(FIN_THREADS) k_finalize(int n, const int32_t* 
         ++it;
         if (!any) break;
         if (it >= max_iters) {
-            if (tid == 0) atomicCAS(&ds->error, 0, (int)FOS_E_TIMEOUT);
+            if (lead) atomicCAS(&ds->error, 0, (int)FOS_E_TIMEOUT);
             return;
         }
     }
-    if (tid == 0) ds->fin_iters = it;
-    // Materialise the serial result from the converged decisions `cur`.
-    for (int i = tid; i < n; i += stride) {
-        float pr[FOS_S];
-        int used = 0;
-        size_t row = (size_t)i * FOS_S;
-#pragma unroll
-        for (int s = 0; s < FOS_S; ++s) pr[s] = prev[row + s];
-        int b = revstart[i], e = revstart[i + 1];
-        for (int k = b; k < e; ++k) {
-            int t = rev[k];
-            if (__ldcg(&cur[t]) && used < FOS_S) {
-                nl[row + used] = t >> 5;
-                pr[used] = score[t];
-                used++;
+    if (lead) ds->fin_iters = it;
+    // Materialise the serial result from the converged decisions `cur`.  For
+    // neighbour-list slot p the serial writes are: the previous score; the
+    // p-th reverse append; then, in slot order, the append of this row's own
+    // accepted slot of rank p - used0 (slot sa) and the zeroing of a rejected
+    // slot p.  The later of the last two wins.
+    for (int i = w0; i < n; i += wstride) {
+        const size_t o = (size_t)i * FOS_S + lane;
+        const float sc = score[o];
+        const float pv = prev[o];
+        const int fid = face_ids[o];
+        const bool ok = sc >= 0.0f && __ldcg(&cur[o]);
+        float appv = 0.0f;
+        int appi = 0;
+        const int used0 = fin_app(i, lane, revstart, rev, cur, score, appv, appi);
+        const unsigned okm = __ballot_sync(0xffffffffu, ok);
+        const int own = __popc(okm);
+        const int used = used0 + own < FOS_S ? used0 + own : FOS_S;
+        const int r = lane - used0;
+        const bool app = r >= 0 && r < own;
+        const int sa = app ? (int)__fns(okm, 0, r + 1) : lane;
+        const float va = __shfl_sync(0xffffffffu, sc, sa);
+        const int ia = __shfl_sync(0xffffffffu, fid, sa);
+        const bool zero = sc >= 0.0f && !ok;
+        float pr = lane < used0 ? appv : pv;
+        if (app) pr = (zero && sa < lane) ? 0.0f : va;
+        else if (zero) pr = 0.0f;
+        prev[o] = pr;
+        nl[o] = lane < used0 ? appi : (app ? ia : -1);
+        if (lane == 0) {
+            used_out[i] = used;
+            fsc[i] = used;
+            if (apply_ema) {  // update_fsc_ema (jfa.py:765-785)
+                float em = ema[i];
+                if (em == 0.0f && used > 0) em = (float)used;
+                else em = fadd(fmul(alpha, (float)used), fmul(fsub(1.0f, alpha), em));
+                ema[i] = em;
             }
+            if (used == 0) atomicAdd(&ds->zero_fsc, 1);
         }
-        for (int s = 0; s < FOS_S; ++s) {
-            float sc = score[row + s];
-            if (sc < 0.0f) continue;
-            if (__ldcg(&cur[row + s])) {
-                if (used < FOS_S) {
-                    nl[row + used] = face_ids[row + s];
-                    pr[used] = sc;
-                    used++;
-                }
-            } else {
-                pr[s] = 0.0f;
-            }
-        }
-        for (int s = used; s < FOS_S; ++s) nl[row + s] = -1;
-#pragma unroll
-        for (int s = 0; s < FOS_S; ++s) prev[row + s] = pr[s];
-        used_out[i] = used;
-        fsc[i] = used;
-        if (apply_ema) {  // update_fsc_ema (jfa.py:765-785)
-            float em = ema[i];
-            if (em == 0.0f && used > 0) em = (float)used;
-            else em = fadd(fmul(alpha, (float)used), fmul(fsub(1.0f, alpha), em));
-            ema[i] = em;
-        }
-        if (used == 0) atomicAdd(&ds->zero_fsc, 1);
     }
 }
 
@@ -569,11 +609,10 @@ static int finalize_impl(FosCtx* c, const float* rad, int n, bool apply_ema, cud
     FOS_LAUNCHED(c);
     k_rev_sort<<<fos_blocks(32LL * n, 256), 256, 0, s>>>(n, c->revstart, c->rev);
     FOS_LAUNCHED(c);
-    // 64-thread blocks spread the rows over every SM (each row is a serial
-    // chain of dependent loads, so more SMs in flight, not more threads per SM)
+    // one warp per row, as many co-resident blocks as the rows fill
     int per_sm = 0;
     FOS_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_finalize, FIN_THREADS, 0));
-    int grid = fos_blocks(n, FIN_THREADS);
+    int grid = fos_blocks(32LL * n, FIN_THREADS);
     int cap = per_sm * c->num_sms;
     if (grid > cap) grid = cap;
     if (grid < 1) grid = 1;
