@@ -95,9 +95,27 @@ struct CoopLayout {
 // full row sets overflow bit par, and the rebuild then takes the CSR form).
 // A phase that produces particle i's new position can run this for the next
 // rebuild right away, so that rebuild needs no P1 phase or barrier of its own.
+// Where a P1 drops its particle: the count buffer, the rows (cfix / spst, or
+// NULL for none), the slot map (slot[i] = the particle's row slot; NULL for
+// none) and the overflow bit that a full row sets.
+struct P1Dst {
+    int32_t* cnt;
+    int32_t* cfix;
+    float4* spst;
+    int32_t* slot;
+    int ovf_bit;
+};
+
+// The alternating form: count buffer `par`, the one set of rows (sorted into
+// a second set by the rebuild), no slot map.
+template <class Args>
+__device__ __forceinline__ P1Dst coop_p1_par(const Args& a, int par) {
+    return P1Dst{par ? a.cnt2 : a.cnt, a.cfix, a.spst, nullptr, 1 << par};
+}
+
 template <class Args, class Geo>
 __device__ __forceinline__ void coop_p1_val(const Args& a, const Geo& geo, int i, float3 v,
-                                            float r, float* dst, int par) {
+                                            float r, float* dst, const P1Dst& t) {
     float wx = grid_wrap(v.x, geo.L, geo.invL);
     float wy = grid_wrap(v.y, geo.L, geo.invL);
     float wz = grid_wrap(v.z, geo.L, geo.invL);
@@ -106,25 +124,26 @@ __device__ __forceinline__ void coop_p1_val(const Args& a, const Geo& geo, int i
     dst[3 * i + 2] = wz;
     int c = geo.cell(i, wx, wy, wz);
     a.cellof[i] = c;
-    int k = atomicAdd(&(par ? a.cnt2 : a.cnt)[c], 1);
+    int k = atomicAdd(&t.cnt[c], 1);
     a.rank[i] = k;
-    if (a.cfix) {
+    if (t.cfix) {
         if (k < COOP_CAP) {
             const size_t slot = (size_t)c * COOP_CAP + k;
-            a.cfix[slot] = i;
-            a.spst[slot] = make_float4(wx, wy, wz, r);
+            t.cfix[slot] = i;
+            t.spst[slot] = make_float4(wx, wy, wz, r);
+            if (t.slot) t.slot[i] = (int)slot;
         } else {
-            atomicOr(&a.ds->grid_ovf, 1 << par);
+            atomicOr(&a.ds->grid_ovf, t.ovf_bit);
         }
     }
 }
 
 template <class Args, class Geo>
 __device__ __forceinline__ void coop_p1_one(const Args& a, const Geo& geo, int i, const float* src,
-                                            const float* rad, float* dst, int par) {
+                                            const float* rad, float* dst, const P1Dst& t) {
     float3 v = make_float3(__ldcg(&src[3 * i + 0]), __ldcg(&src[3 * i + 1]),
                            __ldcg(&src[3 * i + 2]));
-    coop_p1_val(a, geo, i, v, rad ? __ldcg(&rad[i]) : 0.f, dst, par);
+    coop_p1_val(a, geo, i, v, rad ? __ldcg(&rad[i]) : 0.f, dst, t);
 }
 
 // With ou != NULL each deferred particle first takes the frame's OU jitter
@@ -139,13 +158,21 @@ struct OuStep {
     int ctr_base;         // Philox counter = i - ctr_base (index within the foam)
 };
 
+// A P1 target given directly.
+template <class Args>
+__device__ __forceinline__ const P1Dst& p1_target(const Args&, const P1Dst& t) {
+    return t;
+}
+
+// Tgt: a P1Dst, or any type with a p1_target(args, tgt) overload that builds
+// one when the deferred particles are flushed (fewer live registers).
 struct P1Defer {
     int i = -1;
     float4 v;  // new position, radius
     int q = 0;
-    template <class Args, class Geo>
+    template <class Args, class Geo, class Tgt>
     __device__ __forceinline__ void put(const Args& a, const Geo& geo, int lane, int pi, float4 pv,
-                                        float* dst, int par, const OuStep* ou = nullptr) {
+                                        float* dst, const Tgt& t, const OuStep* ou = nullptr) {
         const int slot = q & 31;
         const int si = __shfl_sync(0xffffffffu, pi, 0);
         const float sx = __shfl_sync(0xffffffffu, pv.x, 0);
@@ -157,93 +184,33 @@ struct P1Defer {
             v = make_float4(sx, sy, sz, sr);
         }
         ++q;
-        if (slot == 31) flush(a, geo, dst, par, ou);
+        if (slot == 31) flush(a, geo, dst, t, ou);
     }
-    template <class Args, class Geo>
-    __device__ __forceinline__ void flush(const Args& a, const Geo& geo, float* dst, int par,
+    template <class Args, class Geo, class Tgt>
+    __device__ __forceinline__ void flush(const Args& a, const Geo& geo, float* dst, const Tgt& t,
                                           const OuStep* ou = nullptr) {
         if (i >= 0) {
             float3 p = make_float3(v.x, v.y, v.z);
             if (ou)
                 p = ou_one(i, (unsigned int)(i - ou->ctr_base), p, ou->vjit, v.w, ou->kick, ou->o,
                            ou->frame);
-            coop_p1_val(a, geo, i, p, v.w, dst, par);
+            coop_p1_val(a, geo, i, p, v.w, dst, p1_target(a, t));
         }
         i = -1;
     }
 };
 
-// Rebuild of the hash grid from src into dst (wrapped) with count buffer
-// `par` (rebuilds alternate buffers, so the next rebuild's P1 can run while
-// this grid is still being read).  Ends with a grid barrier unless last;
-// returns false if a barrier timed out; *out receives the layout.
-//   P1        histogram + arrival rank + fixed-capacity row slot (skipped
-//             when p1_done: the previous phase ran coop_p1_* for every
-//             particle with the same src, dst and par);
-//   fixed     when the rows did not overflow, want_csr is false and rad is
-//             given: one phase, one warp per cell sorts its row by particle
-//             index and writes the (pos, rad) copy;
-//   CSR       otherwise (the user-visible final rebuild always): small tables
-//             (G3 <= COOP_SMALL_G3) scan the whole table in every block's
-//             shared memory (block 0 writes cell_count/cell_start) and scatter
-//             ranks, then place stably; large tables use a chunked four-phase
-//             form.  CSR ci/sp/cc/cs are written.
-// The second phase also clears the other count buffer and overflow bit for
-// the rebuild after this one.
+// The CSR form of a rebuild whose P1 filled count buffer `cnt` (cellof and
+// rank written): small tables (G3 <= COOP_SMALL_G3) scan the whole table in
+// every block's shared memory (block 0 writes cell_count/cell_start) and
+// scatter ranks, then place stably; large tables use a chunked four-phase
+// form.  CSR ci/cc/cs and slot_of are written, and sp when rad is given.
+// Ends with a grid barrier unless last; false if a barrier timed out.
 template <class Args, class Geo>
-__device__ bool coop_grid(const Args& a, const Geo& geo, const float* src, float* dst,
-                          const float* rad, bool last, int& tk, unsigned int& ep, bool p1_done,
-                          int par, bool want_csr, CoopLayout* out) {
+__device__ bool coop_csr(const Args& a, const Geo& geo, const int32_t* cnt, const float* dst,
+                         const float* rad, bool last, int& tk, unsigned int& ep) {
     extern __shared__ int s_tab[];  // small form: G3 + 1 exclusive starts
     const int T = gridDim.x * blockDim.x;
-    const int tid = blockIdx.x * blockDim.x + threadIdx.x;
-    int32_t* cnt = par ? a.cnt2 : a.cnt;
-    int32_t* cnt_next = par ? a.cnt : a.cnt2;
-    if (!p1_done) {
-        for (int i = spread_tid(); i < a.n; i += T) coop_p1_one(a, geo, i, src, rad, dst, par);
-        if (!grid_barrier(a.ds, ep)) return false;
-        trace_mark(a, tk);
-    }
-    const bool ovf = ((*((volatile int*)&a.ds->grid_ovf)) >> par) & 1;
-    for (int c = tid; c < a.G3; c += T) cnt_next[c] = 0;
-    if (tid == 0) atomicAnd(&a.ds->grid_ovf, ~(1 << (par ^ 1)));
-    if (a.cfix && !want_csr && !ovf && rad) {
-        // fixed-capacity rows: sort each cell's (<= COOP_CAP) arrivals by
-        // index.  A warp takes two cells per round and loads both rows whole
-        // (slots past the count hold stale entries and are ignored) together
-        // with the counts, so a round waits for one load latency.
-        const int lane = threadIdx.x & 31, W = T >> 5, wid = tid >> 5;
-        for (int c0 = wid; c0 < a.G3; c0 += 2 * W) {
-            const int cc2[2] = {c0, c0 + W};
-            int m[2], id[2];
-            float4 pr[2];
-#pragma unroll
-            for (int h = 0; h < 2; ++h) {
-                const bool ok = cc2[h] < a.G3;  // warp-uniform
-                const size_t base = (size_t)(ok ? cc2[h] : 0) * COOP_CAP;
-                m[h] = ok ? __ldcg(&cnt[cc2[h]]) : 0;  // <= COOP_CAP
-                id[h] = ok ? __ldcg(&a.cfix[base + lane]) : 0;
-                pr[h] = ok ? __ldcg(&a.spst[base + lane]) : make_float4(0.f, 0.f, 0.f, 0.f);
-            }
-#pragma unroll
-            for (int h = 0; h < 2; ++h) {
-                const int key = lane < m[h] ? id[h] : 0x7fffffff;
-                int r = 0;
-                for (int k = 0; k < m[h]; ++k) r += __shfl_sync(0xffffffffu, key, k) < key;
-                if (lane < m[h]) {
-                    const size_t base = (size_t)cc2[h] * COOP_CAP;
-                    a.idsort[base + r] = key;
-                    a.spfix[base + r] = pr[h];
-                    a.slot_of[key] = (int)(base + r);
-                }
-            }
-        }
-        if (out) *out = CoopLayout{a.idsort, a.spfix, nullptr, cnt, COOP_CAP};
-        if (!last && !grid_barrier(a.ds, ep)) return false;
-        trace_mark(a, tk);
-        return true;
-    }
-    if (out) *out = CoopLayout{a.ci, a.sp, a.cs, a.cc, 0};
     if (a.small_grid) {
         // P2: whole-table scan per block, then the rank scatter
         const int per = (a.G3 + blockDim.x - 1) / blockDim.x;
@@ -343,5 +310,75 @@ __device__ bool coop_grid(const Args& a, const Geo& geo, const float* src, float
     if (!last && !grid_barrier(a.ds, ep)) return false;
     trace_mark(a, tk);
     return true;
+}
+
+// Rebuild of the hash grid from src into dst (wrapped) with count buffer
+// `par` (rebuilds alternate buffers, so the next rebuild's P1 can run while
+// this grid is still being read).  Ends with a grid barrier unless last;
+// returns false if a barrier timed out; *out receives the layout.
+//   P1        histogram + arrival rank + fixed-capacity row slot (skipped
+//             when p1_done: the previous phase ran coop_p1_* for every
+//             particle with the same src, dst and par);
+//   fixed     when the rows did not overflow, want_csr is false and rad is
+//             given: one phase, one warp per cell sorts its row by particle
+//             index and writes the (pos, rad) copy;
+//   CSR       otherwise (the user-visible final rebuild always): coop_csr.
+// The second phase also clears the other count buffer and overflow bit for
+// the rebuild after this one.
+template <class Args, class Geo>
+__device__ bool coop_grid(const Args& a, const Geo& geo, const float* src, float* dst,
+                          const float* rad, bool last, int& tk, unsigned int& ep, bool p1_done,
+                          int par, bool want_csr, CoopLayout* out) {
+    const int T = gridDim.x * blockDim.x;
+    const int tid = blockIdx.x * blockDim.x + threadIdx.x;
+    int32_t* cnt = par ? a.cnt2 : a.cnt;
+    int32_t* cnt_next = par ? a.cnt : a.cnt2;
+    if (!p1_done) {
+        const P1Dst t = coop_p1_par(a, par);
+        for (int i = spread_tid(); i < a.n; i += T) coop_p1_one(a, geo, i, src, rad, dst, t);
+        if (!grid_barrier(a.ds, ep)) return false;
+        trace_mark(a, tk);
+    }
+    const bool ovf = ((*((volatile int*)&a.ds->grid_ovf)) >> par) & 1;
+    for (int c = tid; c < a.G3; c += T) cnt_next[c] = 0;
+    if (tid == 0) atomicAnd(&a.ds->grid_ovf, ~(1 << (par ^ 1)));
+    if (a.cfix && !want_csr && !ovf && rad) {
+        // fixed-capacity rows: sort each cell's (<= COOP_CAP) arrivals by
+        // index.  A warp takes two cells per round and loads both rows whole
+        // (slots past the count hold stale entries and are ignored) together
+        // with the counts, so a round waits for one load latency.
+        const int lane = threadIdx.x & 31, W = T >> 5, wid = tid >> 5;
+        for (int c0 = wid; c0 < a.G3; c0 += 2 * W) {
+            const int cc2[2] = {c0, c0 + W};
+            int m[2], id[2];
+            float4 pr[2];
+#pragma unroll
+            for (int h = 0; h < 2; ++h) {
+                const bool ok = cc2[h] < a.G3;  // warp-uniform
+                const size_t base = (size_t)(ok ? cc2[h] : 0) * COOP_CAP;
+                m[h] = ok ? __ldcg(&cnt[cc2[h]]) : 0;  // <= COOP_CAP
+                id[h] = ok ? __ldcg(&a.cfix[base + lane]) : 0;
+                pr[h] = ok ? __ldcg(&a.spst[base + lane]) : make_float4(0.f, 0.f, 0.f, 0.f);
+            }
+#pragma unroll
+            for (int h = 0; h < 2; ++h) {
+                const int key = lane < m[h] ? id[h] : 0x7fffffff;
+                int r = 0;
+                for (int k = 0; k < m[h]; ++k) r += __shfl_sync(0xffffffffu, key, k) < key;
+                if (lane < m[h]) {
+                    const size_t base = (size_t)cc2[h] * COOP_CAP;
+                    a.idsort[base + r] = key;
+                    a.spfix[base + r] = pr[h];
+                    a.slot_of[key] = (int)(base + r);
+                }
+            }
+        }
+        if (out) *out = CoopLayout{a.idsort, a.spfix, nullptr, cnt, COOP_CAP};
+        if (!last && !grid_barrier(a.ds, ep)) return false;
+        trace_mark(a, tk);
+        return true;
+    }
+    if (out) *out = CoopLayout{a.ci, a.sp, a.cs, a.cc, 0};
+    return coop_csr(a, geo, cnt, dst, rad, last, tk, ep);
 }
 

@@ -327,10 +327,10 @@ __device__ __forceinline__ void ens_pbd(const EnsArgs& a, const EnsGeo& geo, con
             int pi = pbd_warp<LdL2>(kk, lane, lay.sp, lay.ci, a.pos_tmp, g,
                                     lay.cs ? lay.cs + d.cell_off : nullptr, lay.cc + d.cell_off,
                                     a.gap1, a.mdf, a.dmul, &nv, lay.cap, d.cell_off);
-            if (p1) d1.put(a, geo, lane, pi, nv, a.pos, par);
+            if (p1) d1.put(a, geo, lane, pi, nv, a.pos, coop_p1_par(a, par));
         }
     }
-    if (p1) d1.flush(a, geo, a.pos, par);
+    if (p1) d1.flush(a, geo, a.pos, coop_p1_par(a, par));
 }
 
 template <int THREADS>
@@ -430,7 +430,7 @@ __global__ void __launch_bounds__(THREADS) k_ens_coop(EnsArgs a) {
         const EnsFoamDev& d = a.F[a.foam_of[i]];
         brownian_one<LdL2>(i, (unsigned int)(i - d.part_off), a.pos, a.strength, a.domain, a.halfL,
                            d.k0, d.k1, (unsigned int)frame);
-        coop_p1_one(a, geo, i, a.pos, a.rad, a.pos, gk & 1);
+        coop_p1_one(a, geo, i, a.pos, a.rad, a.pos, coop_p1_par(a, gk & 1));
     }
     for (int f = tid; f < a.nf; f += T)
         if (a.W[f].settle > 0) a.W[f].settle -= 1;

@@ -104,8 +104,10 @@ static int alloc_cells(FosCtx* c) {
     c->coop_cfix = c->coop_idsort = nullptr;
     c->coop_spfix = c->coop_spst = nullptr;
     c->coop_fixed = 0;
-    for (int32_t** b : bufs) FOS_CUDA(cudaMalloc((void**)b, need * sizeof(int32_t)));
-    FOS_CUDA(cudaMemset(c->coop_cnt, 0, need * sizeof(int32_t)));
+    // coop_cnt holds three count buffers: the single-foam kernel rotates them
+    for (int32_t** b : bufs)
+        FOS_CUDA(cudaMalloc((void**)b, (b == &c->coop_cnt ? 3 : 1) * need * sizeof(int32_t)));
+    FOS_CUDA(cudaMemset(c->coop_cnt, 0, 3 * need * sizeof(int32_t)));
     FOS_CUDA(cudaMemset(c->coop_cnt2, 0, need * sizeof(int32_t)));
     const size_t slots = need * 32;
     if (slots * (4 + 4 + 2 * sizeof(float4)) <= FOS_COOP_FIXED_MAX_BYTES) {

@@ -35,12 +35,9 @@ struct CoopArgs {
     int32_t* cellof;
     int32_t* rank;
     int32_t* ci_tmp;
-    int32_t* cnt;
-    int32_t* cnt2;
-    int32_t* cfix;
-    int32_t* idsort;
-    float4* spfix;
-    float4* spst;
+    int32_t* cnt;               // 3 x G3 count buffers (rebuild r uses buffer r % 3)
+    int32_t* rows_ci[2];        // fixed-capacity rows of rebuild r: set r & 1 (NULL: CSR only)
+    float4* rows_sp[2];
     int32_t* slot_of;
     float* vol0;                // [n] r^P ping-pong of the pressure sweeps
     float* vol1;
@@ -61,6 +58,48 @@ struct CoopArgs {
     int trace_cap;
 };
 
+// Rebuild r of a frame (r = 0 before max overlap, 1..pbd_iters before each PBD
+// sweep, pbd_iters + 1 the final CSR one) drops its particles into count
+// buffer r % 3, row set r & 1 and overflow bit r % 3; its P1 runs in the phase
+// before its first reader.  The rows stay in arrival order: max overlap does
+// not depend on the order, and the PBD sweeps put their hits in index order
+// themselves (pbd_warp_rows), so no phase sorts the rows.
+__device__ __forceinline__ P1Dst coop_p1_dst(const CoopArgs& a, int r) {
+    return P1Dst{a.cnt + (size_t)(r % 3) * a.G3, a.rows_ci[r & 1], a.rows_sp[r & 1], a.slot_of,
+                 1 << (r % 3)};
+}
+
+// Rebuild index as a deferred P1 target.
+struct RebuildIdx {
+    int r;
+};
+__device__ __forceinline__ P1Dst p1_target(const CoopArgs& a, RebuildIdx t) {
+    return coop_p1_dst(a, t.r);
+}
+
+// Layout of rebuild r for the phase that reads it: the rows when none
+// overflowed, else the CSR form, whose phases run first.  Also clears count
+// buffer and overflow bit (r + 2) % 3 for rebuild r + 2, whose P1 comes one
+// phase later (their last reader, of rebuild r - 1, is done).
+__device__ __forceinline__ bool coop_layout(const CoopArgs& a, const UniGeo& geo, int r,
+                                            int& tk, unsigned int& ep, CoopLayout& lay,
+                                            bool& rows) {
+    const int T = gridDim.x * blockDim.x;
+    const int tid = blockIdx.x * blockDim.x + threadIdx.x;
+    int32_t* zc = a.cnt + (size_t)((r + 2) % 3) * a.G3;
+    for (int c = tid; c < a.G3; c += T) zc[c] = 0;
+    if (tid == 0) atomicAnd(&a.ds->grid_ovf, ~(1 << ((r + 2) % 3)));
+    const bool ovf = ((*((volatile int*)&a.ds->grid_ovf)) >> (r % 3)) & 1;
+    const int32_t* cnt = a.cnt + (size_t)(r % 3) * a.G3;
+    rows = a.rows_ci[0] != nullptr && !ovf;
+    if (rows) {
+        lay = CoopLayout{a.rows_ci[r & 1], a.rows_sp[r & 1], nullptr, cnt, COOP_CAP};
+        return true;
+    }
+    lay = CoopLayout{a.ci, a.sp, a.cs, a.cc, 0};
+    return coop_csr(a, geo, cnt, a.pos, a.rad, false, tk, ep);
+}
+
 __global__ void __launch_bounds__(COOP_THREADS) k_frame_coop(CoopArgs a) {
     const int T = gridDim.x * blockDim.x;
     const int tid = blockIdx.x * blockDim.x + threadIdx.x;
@@ -73,23 +112,32 @@ __global__ void __launch_bounds__(COOP_THREADS) k_frame_coop(CoopArgs a) {
     unsigned int ep = 0;
     trace_mark(a, tk);
 
-    // (1) rebuild_grid (run.py:704); rebuild gk uses count buffer gk & 1
+    // (1) rebuild_grid (run.py:704): rebuild 0's P1, then its layout
     const UniGeo geo{a.g.G, a.g.L, a.g.invL, a.g.halfL};
     CoopLayout lay;
-    int gk = 0;
-    if (!coop_grid(a, geo, a.pos, a.pos, a.rad, false, tk, ep, false, gk & 1, false, &lay)) return;
-    ++gk;
+    bool rows = false;
+    {
+        const P1Dst t = coop_p1_dst(a, 0);
+        for (int i = spread_tid(); i < a.n; i += T) coop_p1_one(a, geo, i, a.pos, a.rad, a.pos, t);
+    }
+    if (!grid_barrier(a.ds, ep)) return;
+    trace_mark(a, tk);
     // (2) compute_max_overlap (run.py:709): particle i's slot comes from
-    // slot_of, prefetched one round ahead
+    // slot_of, prefetched one round ahead.  The first prefetch is issued with
+    // the layout's overflow read (the rows' slots come from P1) and repeated
+    // only when the CSR form rewrote slot_of.
+    int kk0 = wid < a.n ? __ldcg(&a.slot_of[wid]) : 0;
+    if (!coop_layout(a, geo, 0, tk, ep, lay, rows)) return;
+    if (!rows) kk0 = wid < a.n ? __ldcg(&a.slot_of[wid]) : 0;
     {
         unsigned int wmax = 0u;
-        int kk_next = wid < a.n ? __ldcg(&a.slot_of[wid]) : 0;
+        int kk_next = kk0;
         for (int r = 0; r < warp_rounds; ++r) {
             const int i = r * W + wid;
             const int kk = kk_next;
             kk_next = i + W < a.n ? __ldcg(&a.slot_of[i + W]) : 0;
             if (i < a.n) {
-                unsigned int b = maxov_warp<LdL2>(kk, lane, lay.sp, lay.ci, a.g, lay.cs, lay.cc,
+                unsigned int b = maxov_warp<LdL1>(kk, lane, lay.sp, lay.ci, a.g, lay.cs, lay.cc,
                                                   a.eps, a.lmd, lay.cap);
                 wmax = b > wmax ? b : wmax;
             }
@@ -167,7 +215,7 @@ __global__ void __launch_bounds__(COOP_THREADS) k_frame_coop(CoopArgs a) {
             if (a.ou) rq += rad_fixed(__ldcg(&a.rad[i]));
             brownian_one<LdL2>(i, (unsigned int)i, a.pos, a.strength, a.domain, a.halfL, a.k0,
                                a.k1, frame);
-            coop_p1_one(a, geo, i, a.pos, a.rad, a.pos, gk & 1);
+            coop_p1_one(a, geo, i, a.pos, a.rad, a.pos, coop_p1_dst(a, 1));
         }
         if (a.ou) {
 #pragma unroll
@@ -182,11 +230,11 @@ __global__ void __launch_bounds__(COOP_THREADS) k_frame_coop(CoopArgs a) {
     // Every rebuild here has its P1 done by the phase that produced the
     // positions (Brownian, then each PBD sweep's lane 0).
     // The OU jitter step (run.py:855-867) runs inside the last sweep's P1.
-    const float* src = a.pos;
     for (int k = 0; k < a.pbd_iters; ++k) {
-        if (!coop_grid(a, geo, src, a.pos, a.rad, false, tk, ep, true, gk & 1, false, &lay))
-            return;
-        ++gk;
+        kk0 = wid < a.n ? __ldcg(&a.slot_of[wid]) : 0;  // as in (2)
+        if (!coop_layout(a, geo, k + 1, tk, ep, lay, rows)) return;
+        if (!rows) kk0 = wid < a.n ? __ldcg(&a.slot_of[wid]) : 0;
+        const RebuildIdx next{k + 2};
         OuStep ous;
         const bool ou_here = a.ou && k == a.pbd_iters - 1;
         if (ou_here) {
@@ -195,24 +243,27 @@ __global__ void __launch_bounds__(COOP_THREADS) k_frame_coop(CoopArgs a) {
                          (unsigned int)pa.frame, 0};
         }
         P1Defer p1;
-        int kk_next = wid < a.n ? __ldcg(&a.slot_of[wid]) : 0;
+        int kk_next = kk0;
         for (int r = 0; r < warp_rounds; ++r) {
             const int i = r * W + wid;
             const int kk = kk_next;
             kk_next = i + W < a.n ? __ldcg(&a.slot_of[i + W]) : 0;
             if (i < a.n) {  // warp-uniform
                 float4 nv = make_float4(0.f, 0.f, 0.f, 0.f);
-                int pi = pbd_warp<LdL2>(kk, lane, lay.sp, lay.ci, a.pos_tmp, a.g, lay.cs, lay.cc,
-                                        a.gap1, a.mdf, a.dmul, &nv, lay.cap);
-                p1.put(a, geo, lane, pi, nv, a.pos, gk & 1, ou_here ? &ous : nullptr);
+                const int pi =
+                    rows ? pbd_warp_rows<LdL1>(kk, lane, lay.sp, lay.ci, a.pos_tmp, a.g, lay.cc,
+                                               COOP_CAP, a.gap1, a.mdf, a.dmul, &nv)
+                         : pbd_warp<LdL1>(kk, lane, lay.sp, lay.ci, a.pos_tmp, a.g, lay.cs,
+                                          lay.cc, a.gap1, a.mdf, a.dmul, &nv, lay.cap);
+                p1.put(a, geo, lane, pi, nv, a.pos, next, ou_here ? &ous : nullptr);
             }
         }
-        p1.flush(a, geo, a.pos, gk & 1, ou_here ? &ous : nullptr);
+        p1.flush(a, geo, a.pos, next, ou_here ? &ous : nullptr);
         if (!grid_barrier(a.ds, ep)) return;
         trace_mark(a, tk);
-        src = a.pos_tmp;
     }
-    coop_grid(a, geo, src, a.pos, nullptr, true, tk, ep, true, gk & 1, true, nullptr);
+    coop_csr(a, geo, a.cnt + (size_t)((a.pbd_iters + 1) % 3) * a.G3, a.pos, nullptr, true, tk,
+             ep);
 }
 
 __global__ void k_coop_prep(FosDevState* ds) {
@@ -277,11 +328,12 @@ int fos_frame_coop_dynamics(FosCtx* c, const FosState* st, const FosFrameParams*
     a.rank = c->rank;
     a.ci_tmp = c->ci_tmp;
     a.cnt = c->coop_cnt;
-    a.cnt2 = c->coop_cnt2;
-    a.cfix = c->coop_fixed ? c->coop_cfix : nullptr;
-    a.idsort = c->coop_idsort;
-    a.spfix = c->coop_spfix;
-    a.spst = c->coop_spst;
+    if (c->coop_fixed) {  // the two row sets
+        a.rows_ci[0] = c->coop_cfix;
+        a.rows_ci[1] = c->coop_idsort;
+        a.rows_sp[0] = c->coop_spst;
+        a.rows_sp[1] = c->coop_spfix;
+    }
     a.slot_of = c->coop_slot;
     a.vol0 = c->pvol;
     a.vol1 = c->pvol + c->max_n;
@@ -323,11 +375,13 @@ int fos_frame_coop_dynamics(FosCtx* c, const FosState* st, const FosFrameParams*
     a.trace_cap = trace_cap;
 
     FOS_REQUIRE(fp->max_eq_nei <= 16, FOS_E_ARG, "cooperative frame needs max_eq_nei <= 16");
+    FOS_REQUIRE(n <= (1 << 26), FOS_E_ARG, "cooperative frame supports up to 2^26 particles");
     FOS_REQUIRE(!a.ou || fp->pbd_iters >= 1, FOS_E_ARG,
                 "cooperative frame runs the OU jitter inside a PBD sweep: pbd_iters >= 1");
     k_coop_prep<<<1, 1, 0, s>>>(c->ds);
     FOS_LAUNCHED(c);
-    FOS_CUDA(cudaMemsetAsync(c->coop_cnt, 0, (size_t)G3 * sizeof(int32_t), s));
+    // count buffers 0 and 1 start empty (the frame clears buffer 2 itself)
+    FOS_CUDA(cudaMemsetAsync(c->coop_cnt, 0, 2 * (size_t)G3 * sizeof(int32_t), s));
     cudaLaunchConfig_t cfg = {};
     cfg.gridDim = dim3(blocks);
     cfg.blockDim = dim3(COOP_THREADS);

@@ -24,6 +24,15 @@ struct LdL2 {
     template <class T>
     __device__ __forceinline__ static T ld(const T* p) { return __ldcg(p); }
 };
+// Plain, L1-allocating loads, for the cooperative kernel's data that no thread
+// writes during the current phase.  Each phase starts after a grid barrier:
+// thread 0's acquire load, then the block barrier, orders every later load of
+// the block after all writes released before the barrier (PTX memory model),
+// so no line cached in an earlier phase is read.
+struct LdL1 {
+    template <class T>
+    __device__ __forceinline__ static T ld(const T* p) { return *p; }
+};
 
 // ------------------------------------------------------------------ grid
 // Cell of an already wrapped position (grid.py:204-222):
@@ -104,15 +113,20 @@ __device__ __forceinline__ Stencil stencil_ranges(float px, float py, float pz, 
     return r;
 }
 
-// Sorted-array position of candidate t (t < total).
-__device__ __forceinline__ int stencil_locate(const Stencil& r, int t) {
+// Stencil cell (lane index) holding candidate t (t < total).
+__device__ __forceinline__ int stencil_cell(const Stencil& r, int t) {
     int c = 0;
 #pragma unroll
     for (int step = 16; step >= 1; step >>= 1) {
         int v = __shfl_sync(0xffffffffu, r.incl, c + step - 1);
         if (v <= t) c += step;
     }
-    int src = c & 31;
+    return c & 31;
+}
+
+// Sorted-array position of candidate t (t < total).
+__device__ __forceinline__ int stencil_locate(const Stencil& r, int t) {
+    const int src = stencil_cell(r, t);
     int st = __shfl_sync(0xffffffffu, r.st, src);
     int ex = __shfl_sync(0xffffffffu, r.excl, src);
     return st + (t - ex);
@@ -151,6 +165,38 @@ __device__ __forceinline__ void warp_ordered_add3(bool hit, float vx, float vy, 
     while (m) {
         int b = __ffs(m) - 1;
         m &= m - 1;
+        cx = fadd(cx, __shfl_sync(0xffffffffu, vx, b));
+        cy = fadd(cy, __shfl_sync(0xffffffffu, vy, b));
+        cz = fadd(cz, __shfl_sync(0xffffffffu, vz, b));
+    }
+}
+
+// Adds the hits' corrections in ascending key order (keys distinct).  When
+// every hit's key exceeds the previous hit's (lane order) they already are in
+// order and are added as warp_ordered_add3 does; otherwise each hit takes its
+// rank among the hits.  All 32 lanes.
+__device__ __forceinline__ void warp_keyed_add3(bool hit, int key, float vx, float vy, float vz,
+                                                float& cx, float& cy, float& cz) {
+    const unsigned int m = __ballot_sync(0xffffffffu, hit);
+    if (!m) return;
+    const int lane = threadIdx.x & 31;
+    const unsigned int before = m & ((1u << lane) - 1u);
+    const int prev = 31 - __clz(before);  // -1: no earlier hit
+    const int kp = __shfl_sync(0xffffffffu, key, prev & 31);
+    if (!__ballot_sync(0xffffffffu, hit && prev >= 0 && kp > key)) {
+        for (unsigned int mm = m; mm; mm &= mm - 1) {
+            const int b = __ffs(mm) - 1;
+            cx = fadd(cx, __shfl_sync(0xffffffffu, vx, b));
+            cy = fadd(cy, __shfl_sync(0xffffffffu, vy, b));
+            cz = fadd(cz, __shfl_sync(0xffffffffu, vz, b));
+        }
+        return;
+    }
+    int rank = 0;
+    for (unsigned int mm = m; mm; mm &= mm - 1) rank += __shfl_sync(0xffffffffu, key, __ffs(mm) - 1) < key;
+    const int h = __popc(m);
+    for (int q = 0; q < h; ++q) {
+        const int b = __ffs(__ballot_sync(0xffffffffu, hit && rank == q)) - 1;
         cx = fadd(cx, __shfl_sync(0xffffffffu, vx, b));
         cy = fadd(cy, __shfl_sync(0xffffffffu, vy, b));
         cz = fadd(cz, __shfl_sync(0xffffffffu, vz, b));
@@ -202,6 +248,54 @@ __device__ __forceinline__ int pbd_warp(int kk, int lane, const float4* sp, cons
         if (t < r.total && k != kk)
             hit = pbd_term(LD::ld(&sp[k]), px, py, pz, ri, md, gap1, g, vx, vy, vz);
         warp_ordered_add3(hit, vx, vy, vz, cx, cy, cz);
+    }
+    if (lane == 0) {
+        int i = LD::ld(&ci[kk]);
+        const float3 n3 = pbd_move(px, py, pz, ri, cx, cy, cz, mdf, dmul, g);
+        pout[3 * i + 0] = n3.x;
+        pout[3 * i + 1] = n3.y;
+        pout[3 * i + 2] = n3.z;
+        if (np) *np = make_float4(n3.x, n3.y, n3.z, ri);
+        return i;
+    }
+    return -1;
+}
+
+// pbd_warp on fixed-capacity rows (cap <= 32 slots a cell, cell c at c * cap)
+// whose particles sit in arrival order, not index order.  Each chunk of
+// candidates covers whole stencil cells (a row holds at most 32), and
+// a chunk's hits are added in the key order (stencil cell, particle index):
+// the reference's loop order, so the sum is pbd_warp's bit for bit.  The
+// candidates' particle indices come with their (pos, rad); requires
+// n <= 2^26 (the key packs the cell above bit 26).
+template <class LD>
+__device__ __forceinline__ int pbd_warp_rows(int kk, int lane, const float4* sp, const int32_t* ci,
+                                             float* pout, const GridGeom g, const int32_t* cc,
+                                             int cap, float gap1, float mdf, float dmul,
+                                             float4* np) {
+    float4 me = LD::ld(&sp[kk]);
+    float px = me.x, py = me.y, pz = me.z, ri = me.w;
+    Stencil r = stencil_ranges<LD>(px, py, pz, g.L, g.invL, g.halfL, g.G, nullptr, cc, lane, cap,
+                                   0);
+    float md = fmul(mdf, ri);
+    float cx = 0.f, cy = 0.f, cz = 0.f;
+    for (int base = 0; base < r.total;) {  // warp-uniform
+        // the chunk ends with the last stencil cell that ends within base + 32
+        const unsigned int fit = __ballot_sync(0xffffffffu, lane < 27 && r.incl <= base + 32);
+        const int end = __shfl_sync(0xffffffffu, r.incl, 31 - __clz(fit));
+        const int t = base + lane;
+        const int c = stencil_cell(r, t < r.total ? t : r.total - 1);  // same cell for t < end
+        const int k = __shfl_sync(0xffffffffu, r.st, c) + (t - __shfl_sync(0xffffffffu, r.excl, c));
+        bool hit = false;
+        int key = 0;
+        float vx = 0.f, vy = 0.f, vz = 0.f;
+        if (t < end && k != kk) {
+            const float4 q = LD::ld(&sp[k]);
+            key = (c << 26) | LD::ld(&ci[k]);
+            hit = pbd_term(q, px, py, pz, ri, md, gap1, g, vx, vy, vz);
+        }
+        warp_keyed_add3(hit, key, vx, vy, vz, cx, cy, cz);
+        base = end;
     }
     if (lane == 0) {
         int i = LD::ld(&ci[kk]);

@@ -110,3 +110,29 @@ def test_cooperative_frame_matches_stage_kernels(name):
     assert np.array_equal(a.local_max_depth.cpu().numpy(), b.local_max_depth.cpu().numpy())
     assert a.counters() == b.counters()
     assert a.ctx.device_error() == 0
+
+
+def test_cooperative_frame_with_crowded_cells():
+    """Cells of more than 32 particles overflow the cooperative kernel's
+    fixed-capacity rows, and those rebuilds take the CSR form; the frames still
+    equal the one-kernel-per-stage path bit for bit.  300 particles start in a
+    0.02 cube (hash cells 0.04 wide), so the first frames overflow."""
+    from fos.inputs import Foam
+    rng = np.random.default_rng(9)
+    n = 2000
+    pos = rng.random((n, 3), dtype=np.float32)
+    pos[:300] = (0.3 + 0.02 * rng.random((300, 3))).astype(np.float32)
+    rad = rng.uniform(0.01, 0.02, n).astype(np.float32)
+    foam = Foam("crowd-2k-64", pos, rad, 64, 0.01, 0.02, 10, 16, 4, 10, 2, 2, 6, 5)
+    a = FoamSim.from_foam(foam, use_graph=True)
+    b = FoamSim.from_foam(foam, use_graph=False)
+    a.initialize()
+    b.initialize()
+    for _ in range(4):
+        a.step()
+        b.step_profiled()
+    torch.cuda.synchronize()
+    for key in ("pos", "rad", "fsc", "cell_indices", "cell_start", "local_max_depth"):
+        assert torch.equal(getattr(a, key), getattr(b, key)), key
+    assert a.counters() == b.counters()
+    assert a.ctx.device_error() == 0
