@@ -91,7 +91,7 @@ struct CoopLayout {
 // wrap v into dst[i], find its cell, take an arrival rank in the count
 // buffer `par` (all-zero before the first arrival) and drop the particle into
 // slot rank of the cell's fixed-capacity rows: its index into cfix and its
-// (wrapped position, radius) into spst, so the row sort needs no gather (a
+// (wrapped position, radius) into spst, so a row sort needs no gather (a
 // full row sets overflow bit par, and the rebuild then takes the CSR form).
 // A phase that produces particle i's new position can run this for the next
 // rebuild right away, so that rebuild needs no P1 phase or barrier of its own.

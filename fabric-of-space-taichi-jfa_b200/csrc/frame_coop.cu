@@ -10,11 +10,12 @@
 // barriers; each phase calls the same per-element device functions as the
 // standalone kernels (phases.cuh), so the results are identical.
 //
-// Grid rebuilds inside the kernel (grid.py:145-309 / run.py:476-504): see
-// coop_grid (coop.cuh).  The rebuilds the frame's own stages read use
-// fixed-capacity cell rows (one phase after the histogram, which itself runs
-// inside the phase that produced the positions); the final rebuild, whose
-// cell arrays the caller sees, is the CSR form.
+// Grid rebuilds inside the kernel (grid.py:145-309 / run.py:476-504): the
+// histogram of a rebuild runs inside the phase that produced the positions
+// and drops each particle into a fixed-capacity cell row; the frame's own
+// stages read those rows as they are (coop_p1_dst, coop_layout below).  A row
+// that overflows sends its rebuild to the CSR form (coop_csr, coop.cuh); the
+// final rebuild, whose cell arrays the caller sees, is always the CSR form.
 #include <string.h>
 
 #include "coop.cuh"
