@@ -97,20 +97,22 @@ struct CoopLayout {
 // rebuild right away, so that rebuild needs no P1 phase or barrier of its own.
 // Where a P1 drops its particle: the count buffer, the rows (cfix / spst, or
 // NULL for none), the slot map (slot[i] = the particle's row slot; NULL for
-// none) and the overflow bit that a full row sets.
+// none) and the overflow bit that a full row sets in *ovf_word.
 struct P1Dst {
     int32_t* cnt;
     int32_t* cfix;
     float4* spst;
     int32_t* slot;
-    int ovf_bit;
+    unsigned int* ovf_word;
+    unsigned int ovf_bit;
 };
 
 // The alternating form: count buffer `par`, the one set of rows (sorted into
 // a second set by the rebuild), no slot map.
 template <class Args>
 __device__ __forceinline__ P1Dst coop_p1_par(const Args& a, int par) {
-    return P1Dst{par ? a.cnt2 : a.cnt, a.cfix, a.spst, nullptr, 1 << par};
+    return P1Dst{par ? a.cnt2 : a.cnt, a.cfix, a.spst, nullptr, (unsigned int*)&a.ds->grid_ovf,
+                 1u << par};
 }
 
 template <class Args, class Geo>
@@ -133,7 +135,7 @@ __device__ __forceinline__ void coop_p1_val(const Args& a, const Geo& geo, int i
             t.spst[slot] = make_float4(wx, wy, wz, r);
             if (t.slot) t.slot[i] = (int)slot;
         } else {
-            atomicOr(&a.ds->grid_ovf, t.ovf_bit);
+            atomicOr(t.ovf_word, t.ovf_bit);
         }
     }
 }

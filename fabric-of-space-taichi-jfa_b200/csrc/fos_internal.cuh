@@ -325,8 +325,19 @@ __device__ __forceinline__ void red_release_gpu_add(unsigned int* p, unsigned in
     asm volatile("red.release.gpu.global.add.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
 }
 
-__device__ __forceinline__ bool grid_barrier(FosDevState* ds, unsigned int& epoch) {
+//
+// The counter takes the low FOS_BAR_FLAG_SHIFT bits of ds->bar_count; the
+// bits above are flags that a phase raises (atomicOr before its block arrives)
+// for the phase after the barrier.  The poll that ends the barrier reads them
+// with the count and hands them to the block in *flags, so no thread has to
+// load a shared flag word of its own.
+#define FOS_BAR_FLAG_SHIFT 26
+#define FOS_BAR_COUNT_MASK ((1u << FOS_BAR_FLAG_SHIFT) - 1u)
+
+__device__ __forceinline__ bool grid_barrier(FosDevState* ds, unsigned int& epoch,
+                                             unsigned int* flags = nullptr) {
     __shared__ int s_ok;
+    __shared__ unsigned int s_flags;
     __syncthreads();
     if (threadIdx.x == 0) {
         epoch += 1u;
@@ -335,7 +346,8 @@ __device__ __forceinline__ bool grid_barrier(FosDevState* ds, unsigned int& epoc
         red_release_gpu_add(&ds->bar_count, 1u);
         long long t0 = clock64();
         unsigned int polls = 0;
-        while (ld_acquire_gpu(&ds->bar_count) < target) {
+        unsigned int v;
+        while (((v = ld_acquire_gpu(&ds->bar_count)) & FOS_BAR_COUNT_MASK) < target) {
             // the error word and the clock are checked every 32 polls, so a
             // poll is one L2 round trip and the release is seen sooner
             if ((++polls & 31u) == 0u) {
@@ -348,7 +360,9 @@ __device__ __forceinline__ bool grid_barrier(FosDevState* ds, unsigned int& epoc
             }
         }
         s_ok = ok ? 1 : 0;
+        s_flags = v >> FOS_BAR_FLAG_SHIFT;
     }
     __syncthreads();
+    if (flags) *flags = s_flags;
     return s_ok != 0;
 }

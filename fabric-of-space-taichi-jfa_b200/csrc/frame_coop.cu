@@ -61,13 +61,14 @@ struct CoopArgs {
 
 // Rebuild r of a frame (r = 0 before max overlap, 1..pbd_iters before each PBD
 // sweep, pbd_iters + 1 the final CSR one) drops its particles into count
-// buffer r % 3, row set r & 1 and overflow bit r % 3; its P1 runs in the phase
-// before its first reader.  The rows stay in arrival order: max overlap does
+// buffer r % 3, row set r & 1 and overflow flag r % 3 of the barrier word; its
+// P1 runs in the phase before its first reader, which gets the flags from the
+// barrier between them.  The rows stay in arrival order: max overlap does
 // not depend on the order, and the PBD sweeps put their hits in index order
 // themselves (pbd_warp_rows), so no phase sorts the rows.
 __device__ __forceinline__ P1Dst coop_p1_dst(const CoopArgs& a, int r) {
     return P1Dst{a.cnt + (size_t)(r % 3) * a.G3, a.rows_ci[r & 1], a.rows_sp[r & 1], a.slot_of,
-                 1 << (r % 3)};
+                 &a.ds->bar_count, 1u << (FOS_BAR_FLAG_SHIFT + r % 3)};
 }
 
 // Rebuild index as a deferred P1 target.
@@ -78,19 +79,20 @@ __device__ __forceinline__ P1Dst p1_target(const CoopArgs& a, RebuildIdx t) {
     return coop_p1_dst(a, t.r);
 }
 
-// Layout of rebuild r for the phase that reads it: the rows when none
-// overflowed, else the CSR form, whose phases run first.  Also clears count
-// buffer and overflow bit (r + 2) % 3 for rebuild r + 2, whose P1 comes one
-// phase later (their last reader, of rebuild r - 1, is done).
+// Layout of rebuild r for the phase that reads it (flags: from the barrier
+// after its P1): the rows when none overflowed, else the CSR form, whose
+// phases run first.  Also clears count buffer and overflow flag (r + 2) % 3
+// for rebuild r + 2, whose P1 comes one phase later (their last reader, of
+// rebuild r - 1, is done).
 __device__ __forceinline__ bool coop_layout(const CoopArgs& a, const UniGeo& geo, int r,
-                                            int& tk, unsigned int& ep, CoopLayout& lay,
-                                            bool& rows) {
+                                            unsigned int flags, int& tk, unsigned int& ep,
+                                            CoopLayout& lay, bool& rows) {
     const int T = gridDim.x * blockDim.x;
     const int tid = blockIdx.x * blockDim.x + threadIdx.x;
     int32_t* zc = a.cnt + (size_t)((r + 2) % 3) * a.G3;
     for (int c = tid; c < a.G3; c += T) zc[c] = 0;
-    if (tid == 0) atomicAnd(&a.ds->grid_ovf, ~(1 << ((r + 2) % 3)));
-    const bool ovf = ((*((volatile int*)&a.ds->grid_ovf)) >> (r % 3)) & 1;
+    if (tid == 0) atomicAnd(&a.ds->bar_count, ~(1u << (FOS_BAR_FLAG_SHIFT + (r + 2) % 3)));
+    const bool ovf = (flags >> (r % 3)) & 1u;
     const int32_t* cnt = a.cnt + (size_t)(r % 3) * a.G3;
     rows = a.rows_ci[0] != nullptr && !ovf;
     if (rows) {
@@ -121,14 +123,14 @@ __global__ void __launch_bounds__(COOP_THREADS) k_frame_coop(CoopArgs a) {
         const P1Dst t = coop_p1_dst(a, 0);
         for (int i = spread_tid(); i < a.n; i += T) coop_p1_one(a, geo, i, a.pos, a.rad, a.pos, t);
     }
-    if (!grid_barrier(a.ds, ep)) return;
+    unsigned int gfl = 0u;  // overflow flags from the barrier after the last P1
+    if (!grid_barrier(a.ds, ep, &gfl)) return;
     trace_mark(a, tk);
     // (2) compute_max_overlap (run.py:709): particle i's slot comes from
-    // slot_of, prefetched one round ahead.  The first prefetch is issued with
-    // the layout's overflow read (the rows' slots come from P1) and repeated
-    // only when the CSR form rewrote slot_of.
+    // slot_of, prefetched one round ahead (the rows' slots come from P1; the
+    // CSR form rewrites slot_of, and the first prefetch is then repeated).
     int kk0 = wid < a.n ? __ldcg(&a.slot_of[wid]) : 0;
-    if (!coop_layout(a, geo, 0, tk, ep, lay, rows)) return;
+    if (!coop_layout(a, geo, 0, gfl, tk, ep, lay, rows)) return;
     if (!rows) kk0 = wid < a.n ? __ldcg(&a.slot_of[wid]) : 0;
     {
         unsigned int wmax = 0u;
@@ -225,7 +227,7 @@ __global__ void __launch_bounds__(COOP_THREADS) k_frame_coop(CoopArgs a) {
         }
         if (tid == 0 && a.ds->settle > 0) a.ds->settle -= 1;
     }
-    if (!grid_barrier(a.ds, ep)) return;
+    if (!grid_barrier(a.ds, ep, &gfl)) return;
     trace_mark(a, tk);
     // (6) PBD passes, each on a fresh grid (run.py:829-846); (7) rebuild (run.py:874)
     // Every rebuild here has its P1 done by the phase that produced the
@@ -233,7 +235,7 @@ __global__ void __launch_bounds__(COOP_THREADS) k_frame_coop(CoopArgs a) {
     // The OU jitter step (run.py:855-867) runs inside the last sweep's P1.
     for (int k = 0; k < a.pbd_iters; ++k) {
         kk0 = wid < a.n ? __ldcg(&a.slot_of[wid]) : 0;  // as in (2)
-        if (!coop_layout(a, geo, k + 1, tk, ep, lay, rows)) return;
+        if (!coop_layout(a, geo, k + 1, gfl, tk, ep, lay, rows)) return;
         if (!rows) kk0 = wid < a.n ? __ldcg(&a.slot_of[wid]) : 0;
         const RebuildIdx next{k + 2};
         OuStep ous;
@@ -260,7 +262,7 @@ __global__ void __launch_bounds__(COOP_THREADS) k_frame_coop(CoopArgs a) {
             }
         }
         p1.flush(a, geo, a.pos, next, ou_here ? &ous : nullptr);
-        if (!grid_barrier(a.ds, ep)) return;
+        if (!grid_barrier(a.ds, ep, &gfl)) return;
         trace_mark(a, tk);
     }
     coop_csr(a, geo, a.cnt + (size_t)((a.pbd_iters + 1) % 3) * a.G3, a.pos, nullptr, true, tk,
