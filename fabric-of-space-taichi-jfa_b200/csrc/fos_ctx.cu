@@ -208,6 +208,15 @@ extern "C" int fos_ctx_create(const FosParams* p, int max_n, int max_res, int de
     ALLOC(c->rank, (size_t)max_n * 4);
     ALLOC(c->coop_slot, (size_t)max_n * 4);
     ALLOC(c->pvol, (size_t)max_n * 8);
+    c->ptag_n = max_n < FOS_PTAG_MAX_N ? max_n : FOS_PTAG_MAX_N;
+    ALLOC(c->ptag, (size_t)(FOS_PTAG_SWEEPS + 1) * c->ptag_n * 8);
+    {
+        cudaError_t e_ = cudaMemset(c->ptag, 0, (size_t)(FOS_PTAG_SWEEPS + 1) * c->ptag_n * 8);
+        if (e_ != cudaSuccess) {
+            fos_ctx_destroy(c);
+            return fos_cuda_fail(e_, "cudaMemset ptag", __FILE__, __LINE__);
+        }
+    }
     ALLOC(c->stats_f, 64 * 4);
     ALLOC(c->stats_i, 64 * 4);
     ALLOC(c->ds, sizeof(FosDevState));
@@ -267,7 +276,7 @@ extern "C" int fos_ctx_destroy(FosCtx* c) {
                     c->fin_changed, c->sorted, c->ci_tmp, c->coop_bsum, c->coop_cnt,
                     c->coop_part, c->coop_cnt2, c->coop_cfix, c->coop_idsort, c->coop_spfix,
                     c->coop_spst,
-                    c->coop_slot, c->skip_part, c->pvol};
+                    c->coop_slot, c->skip_part, c->pvol, c->ptag};
     for (void* q : ptrs)
         if (q) cudaFree(q);
     if (c->pinned) cudaFreeHost(c->pinned);

@@ -42,7 +42,7 @@ struct FosDevState {
     int grid_ovf;                 // bit p: a fixed-capacity cell row of count buffer p overflowed
     unsigned long long rad_sum;   // OU jitter: sum of the radii, 2^-40 fixed point
     int tile_count;               // fos_dirty_count: marked tiles
-    int pad_tc;
+    unsigned int coop_epoch;      // cooperative frame launches (tags of the pressure words)
     unsigned long long changes[FOS_MAX_PASSES];
 };
 
@@ -59,6 +59,8 @@ struct FosGraphKey {
 struct FosSurBufs;  // surrogate.cu
 
 #define FOS_SKIP_BLOCKS 1024
+#define FOS_PTAG_MAX_N 32768  // particles the tagged pressure words are allocated for
+#define FOS_PTAG_SWEEPS 64    // most sweeps they hold (one word per particle and sweep)
 #define FOS_GRAPH_SLOTS 6
 // block size of the cooperative finalize kernel (one warp per row); 1024
 // threads at <= 32 registers keep two blocks (64 warps) on every SM and only
@@ -113,6 +115,10 @@ struct FosCtx {
     int coop_fixed = 0;               // the fixed-capacity rows are allocated
     int32_t* coop_slot = nullptr;     // [max_n] slot of each particle in the last rebuild
     float* pvol = nullptr;            // [2 * max_n] r^P ping-pong of the pressure sweeps
+    // tagged r^P words of the cooperative frame's barrier-free pressure sweeps:
+    // [(FOS_PTAG_SWEEPS + 1) * ptag_n], zeroed at creation
+    unsigned long long* ptag = nullptr;
+    int ptag_n = 0;
     int32_t* coop_bsum = nullptr;     // [1024]
     int32_t* ci_tmp = nullptr;        // [max_n]
     int use_coop = 1;                 // plain-frame dynamics as one cooperative kernel
@@ -334,10 +340,18 @@ __device__ __forceinline__ void red_release_gpu_add(unsigned int* p, unsigned in
 #define FOS_BAR_FLAG_SHIFT 26
 #define FOS_BAR_COUNT_MASK ((1u << FOS_BAR_FLAG_SHIFT) - 1u)
 
+//
+// With nf > 0, thread 0 also loads the words *fetch[0..nf) (nf <= 4) after
+// the barrier and the block gets them in fetched[]: one load per block of a
+// word that every block wrote or reads, instead of one per warp of the same
+// address.
 __device__ __forceinline__ bool grid_barrier(FosDevState* ds, unsigned int& epoch,
-                                             unsigned int* flags = nullptr) {
+                                             unsigned int* flags = nullptr,
+                                             const unsigned int* const* fetch = nullptr,
+                                             int nf = 0, unsigned int* fetched = nullptr) {
     __shared__ int s_ok;
     __shared__ unsigned int s_flags;
+    __shared__ unsigned int s_fetch[4];
     __syncthreads();
     if (threadIdx.x == 0) {
         epoch += 1u;
@@ -361,8 +375,10 @@ __device__ __forceinline__ bool grid_barrier(FosDevState* ds, unsigned int& epoc
         }
         s_ok = ok ? 1 : 0;
         s_flags = v >> FOS_BAR_FLAG_SHIFT;
+        for (int k = 0; k < nf; ++k) s_fetch[k] = *((const volatile unsigned int*)fetch[k]);
     }
     __syncthreads();
     if (flags) *flags = s_flags;
+    for (int k = 0; k < nf; ++k) fetched[k] = s_fetch[k];
     return s_ok != 0;
 }

@@ -42,6 +42,7 @@ struct CoopArgs {
     int32_t* slot_of;
     float* vol0;                // [n] r^P ping-pong of the pressure sweeps
     float* vol1;
+    unsigned long long* ptag;   // non-NULL: barrier-free pressure sweeps on tagged words
     int32_t* part;
     int32_t* bsum;
     float4* sp;
@@ -58,6 +59,56 @@ struct CoopArgs {
     unsigned long long* trace;  // optional: %globaltimer after every phase (block 0)
     int trace_cap;
 };
+
+// Tagged pressure words: (tag << 32) | float bits, written and read whole, so
+// a reader that sees the tag it waits for also sees that sweep's value.
+__device__ __forceinline__ void st_tagged(unsigned long long* p, unsigned int tag, float v) {
+    const unsigned long long w = ((unsigned long long)tag << 32) | __float_as_uint(v);
+    asm volatile("st.relaxed.gpu.global.u64 [%0], %1;" ::"l"(p), "l"(w) : "memory");
+}
+
+__device__ __forceinline__ unsigned long long ld_tagged(const unsigned long long* p) {
+    unsigned long long w;
+    asm volatile("ld.relaxed.gpu.global.u64 %0, [%1];" : "=l"(w) : "l"(p) : "memory");
+    return w;
+}
+
+// Every lane waits for the words at p0 / p1 (where need0 / need1) to carry
+// `tag` and gets their values; the whole warp polls together, so the warp's
+// groups never diverge.  Bounded like the grid barrier: after ~1 s, or once
+// the error word is set, it records FOS_E_TIMEOUT, clears ok and returns
+// (the next grid barrier then ends the kernel).
+__device__ __forceinline__ void wait_tagged2(const unsigned long long* p0,
+                                             const unsigned long long* p1, bool need0,
+                                             bool need1, unsigned int tag, FosDevState* ds,
+                                             bool& ok, float& v0, float& v1) {
+    const long long t0 = clock64();
+    unsigned int polls = 0;
+    for (;;) {
+        if (need0) {
+            const unsigned long long w = ld_tagged(p0);
+            if ((unsigned int)(w >> 32) == tag) {
+                v0 = __uint_as_float((unsigned int)w);
+                need0 = false;
+            }
+        }
+        if (need1) {
+            const unsigned long long w = ld_tagged(p1);
+            if ((unsigned int)(w >> 32) == tag) {
+                v1 = __uint_as_float((unsigned int)w);
+                need1 = false;
+            }
+        }
+        if (!__any_sync(0xffffffffu, need0 || need1) || !ok) return;
+        if ((++polls & 31u) == 0u &&
+            __any_sync(0xffffffffu, *((volatile int*)&ds->error) != 0 ||
+                                        clock64() - t0 > FOS_BAR_CYCLE_LIMIT)) {
+            atomicCAS(&ds->error, 0, (int)FOS_E_TIMEOUT);
+            ok = false;
+            return;
+        }
+    }
+}
 
 // Rebuild r of a frame (r = 0 before max overlap, 1..pbd_iters before each PBD
 // sweep, pbd_iters + 1 the final CSR one) drops its particles into count
@@ -147,14 +198,78 @@ __global__ void __launch_bounds__(COOP_THREADS) k_frame_coop(CoopArgs a) {
         }
         block_max_atomic(wmax, &a.ds->omax_bits);
     }
-    if (!grid_barrier(a.ds, ep)) return;
+    // settle, the deepest overlap, the frame number and the launch epoch,
+    // fetched once per block
+    const unsigned int* const fw[4] = {(const unsigned int*)&a.ds->settle, &a.ds->omax_bits,
+                                       (const unsigned int*)&a.ds->frame, &a.ds->coop_epoch};
+    unsigned int fv[4];
+    if (!grid_barrier(a.ds, ep, nullptr, fw, 4, fv)) return;
     trace_mark(a, tk);
+    const bool nudge = (int)fv[0] > 0;
+    const float bg = back_global_from_bits(fv[1], a.contact_tol_d);
+    PressureArgs pa = a.pa;
+    pa.frame = (int)fv[2];
+    // four consecutive particles per warp (one sector of each per-particle
+    // array), consecutive warps of particles on consecutive blocks
+    const int i_one =
+        (int)((((threadIdx.x >> 5) * gridDim.x + blockIdx.x) << 2) + ((threadIdx.x >> 3) & 3));
+    if (a.ptag) {
+        // (3) + (4) without grid barriers (n <= T/8, 1 <= sweeps <= FOS_PTAG_SWEEPS):
+        // each 8-lane group nudges its particle and runs every pressure sweep
+        // on it.  The power r^P that starts sweep w is published as the word
+        // ptag[w * n + i] tagged (epoch << 7) | (w + 1), and a sweep waits for
+        // its neighbours' words of the same sweep, so it reads exactly the
+        // values a barrier between the sweeps would give.  Every sweep has its
+        // own words: a particle may run ahead of the particles that read it.
+        const int i = i_one, gl = lane & 7;
+        const bool live = i < a.n;
+        const unsigned int tbase = fv[3] << 7;
+        float ri = 0.f;
+        if (live) {
+            ri = __ldcg(&a.rad[i]);
+            if (nudge)
+                ri = nudge_one(ri, __ldcg(&a.rad_target[i]), __ldcg(&a.lmd[i]), a.alpha,
+                               a.max_step, a.rmin, a.rmax, bg, a.bp_mode, a.contact_tol);
+        }
+        float Vi = live ? powf(ri, pa.P) : 0.f;
+        if (live && gl == 0) {
+            if (nudge) a.rad[i] = ri;
+            st_tagged(&a.ptag[i], tbase | 1u, Vi);
+        }
+        const PressureNbr nb = pressure_nbr8x2<LdL2>(i, lane, pa);
+        bool ok = true;
+        float d = 0.f;
+        for (int w = 0; w < a.sweeps; ++w) {
+            const unsigned int tag = tbase | (unsigned int)(w + 1);
+            const unsigned long long* words = a.ptag + (size_t)w * a.n;
+            d = 0.f;
+            float vj0 = 0.f, vj1 = 0.f;
+            wait_tagged2(&words[nb.j[0]], &words[nb.j[1]], nb.fc > 0 && nb.ok[0],
+                         nb.fc > 0 && nb.ok[1], tag, a.ds, ok, vj0, vj1);
+            if (nb.fc > 0) d = pressure_sum8x2(pa, nb, lane, ri, Vi, vj0, vj1);
+            ri = fmaxf(pa.rmin, fminf(pa.rmax, fadd(ri, d)));
+            if (w + 1 < a.sweeps) {
+                Vi = powf(ri, pa.P);
+                if (live && gl == 0) st_tagged(&a.ptag[(size_t)(w + 1) * a.n + i], tag + 1u, Vi);
+            }
+        }
+        if (live && gl == 0) {
+            a.delta_r[i] = d;
+            a.rad[i] = ri;
+        }
+        // the last sweep's stats
+        const float ad = fabsf(d);
+        const int ch = (live && gl == 0) && ad > 1e-12f;
+        const int cnt = __syncthreads_count(ch);
+        const unsigned int bm = __reduce_max_sync(0xffffffffu, ch ? __float_as_uint(ad) : 0u);
+        block_max_atomic(bm, &a.ds->maxabs_dr_bits);
+        if (threadIdx.x == 0 && cnt) atomicAdd(&a.ds->changed, cnt);
+        if (!grid_barrier(a.ds, ep)) return;
+        trace_mark(a, tk);
+    } else {
     // (3) nudge_radii_adaptive_ema while settle_frames_left > 0 (run.py:744-750);
     // each final radius's power r^P seeds the pressure sweeps
     {
-        const bool nudge = *((volatile int*)&a.ds->settle) > 0;
-        const float bg = back_global_from_bits(*((volatile unsigned int*)&a.ds->omax_bits),
-                                               a.contact_tol_d);
         for (int i = spread_tid(); i < a.n; i += T) {
             float r = __ldcg(&a.rad[i]);
             if (nudge) {
@@ -168,8 +283,6 @@ __global__ void __launch_bounds__(COOP_THREADS) k_frame_coop(CoopArgs a) {
     if (!grid_barrier(a.ds, ep)) return;
     trace_mark(a, tk);
     // (4) pressure sweeps (run.py:755-771); the last sweep reports its stats
-    PressureArgs pa = a.pa;
-    pa.frame = *((volatile int*)&a.ds->frame);
     // 8-lane groups, two neighbours per lane: every particle in one round
     const int groups_per_round = T / 8;
     const int p_rounds = (a.n + groups_per_round - 1) / groups_per_round;
@@ -177,10 +290,6 @@ __global__ void __launch_bounds__(COOP_THREADS) k_frame_coop(CoopArgs a) {
     // for all sweeps, and the particles are spread over every block, so every
     // SM issues the same share of the sweep
     const bool keep_nbr = p_rounds == 1;
-    // four consecutive particles per warp (one sector of each per-particle
-    // array), consecutive warps of particles on consecutive blocks
-    const int i_one =
-        (int)((((threadIdx.x >> 5) * gridDim.x + blockIdx.x) << 2) + ((threadIdx.x >> 3) & 3));
     const PressureNbr nb0 = pressure_nbr8x2<LdL2>(i_one, lane, pa);
     for (int w = 0; w < a.sweeps; ++w) {
         const float* rin = (w & 1) ? a.rad_tmp : a.rad;
@@ -205,6 +314,7 @@ __global__ void __launch_bounds__(COOP_THREADS) k_frame_coop(CoopArgs a) {
         if (!grid_barrier(a.ds, ep)) return;
         trace_mark(a, tk);
     }
+    }
     // (5) apply_brownian_motion (run.py:807-813); the odd-sweep result is copied
     // back into rad, and settle_frames_left -= 1 (run.py:750).  Each new
     // position enters the next rebuild's histogram right away (its P1).
@@ -214,7 +324,7 @@ __global__ void __launch_bounds__(COOP_THREADS) k_frame_coop(CoopArgs a) {
         unsigned int frame = (unsigned int)pa.frame;
         long long rq = 0;
         for (int i = spread_tid(); i < a.n; i += T) {
-            if (a.sweeps & 1) a.rad[i] = __ldcg(&a.rad_tmp[i]);
+            if ((a.sweeps & 1) && !a.ptag) a.rad[i] = __ldcg(&a.rad_tmp[i]);
             if (a.ou) rq += rad_fixed(__ldcg(&a.rad[i]));
             brownian_one<LdL2>(i, (unsigned int)i, a.pos, a.strength, a.domain, a.halfL, a.k0,
                                a.k1, frame);
@@ -270,6 +380,7 @@ __global__ void __launch_bounds__(COOP_THREADS) k_frame_coop(CoopArgs a) {
 }
 
 __global__ void k_coop_prep(FosDevState* ds) {
+    ds->coop_epoch += 1u;
     ds->grid_ovf = 0;
     ds->rad_sum = 0ull;
     ds->omax_bits = 0u;
@@ -340,6 +451,10 @@ int fos_frame_coop_dynamics(FosCtx* c, const FosState* st, const FosFrameParams*
     a.slot_of = c->coop_slot;
     a.vol0 = c->pvol;
     a.vol1 = c->pvol + c->max_n;
+    // barrier-free pressure sweeps: every particle in one 8-lane group
+    if (c->ptag && n <= c->ptag_n && (long long)n * 8 <= (long long)blocks * COOP_THREADS &&
+        fp->pressure_iters >= 1 && fp->pressure_iters <= FOS_PTAG_SWEEPS)
+        a.ptag = c->ptag;
     a.part = c->coop_part;
     a.bsum = c->coop_bsum;
     a.sp = c->sorted;

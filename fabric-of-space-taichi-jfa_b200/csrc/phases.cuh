@@ -496,14 +496,49 @@ __device__ __forceinline__ float pressure_sweep8x2(int i, int lane, const Pressu
 // new-radius term) instead of two, and lane 0 also writes vout[i] =
 // powf(rout[i], P) for the next sweep (vout may be NULL).  The result is
 // pressure_sweep8x2's bit for bit: the same powf of the same values.
+// The radius delta of one 8-lane group's particle (radius ri, power Vi = ri^P)
+// from its neighbours' powers vj0 / vj1 (lane t: neighbours t and t + 8 of
+// the hashed rotation), summed in neighbour order; every lane of the group
+// gets it.  Only called when nb.fc > 0 (uniform over the group).
+__device__ __forceinline__ float pressure_sum8x2(const PressureArgs& a, const PressureNbr& nb,
+                                                 int lane, float ri, float Vi, float vj0,
+                                                 float vj1) {
+    const int base_lane = lane & 24;
+    const unsigned int gmask = 0xffu << base_lane;
+    const float invP = fdiv(1.0f, a.P);
+    float term[2] = {0.f, 0.f};
+#pragma unroll
+    for (int h = 0; h < 2; ++h) {
+        if (nb.ok[h]) {
+            const float Vj = h == 0 ? vj0 : vj1;
+            const float dvr = fmul(a.k, fsub(Vi, Vj));
+            const float vmin = fminf(Vi, Vj);
+            const float dv = fmaxf(fmul(-a.cap, vmin), fminf(fmul(a.cap, vmin), dvr));
+            term[h] = fsub(powf(fsub(Vi, dv), invP), ri);
+        }
+    }
+    // neighbour order: lanes 0..7 of the group for h = 0, then for h = 1; the
+    // eight shuffles of each h are issued before the adds that consume them
+    float d = 0.f;
+#pragma unroll
+    for (int h = 0; h < 2; ++h) {
+        const unsigned int m = (__ballot_sync(gmask, nb.ok[h]) & gmask) >> base_lane;
+        float v[8];
+#pragma unroll
+        for (int t = 0; t < 8; ++t) v[t] = __shfl_sync(gmask, term[h], t, 8);
+#pragma unroll
+        for (int t = 0; t < 8; ++t)
+            if ((m >> t) & 1u) d = fadd(d, v[t]);
+    }
+    return d;
+}
+
 template <class LD>
 __device__ __forceinline__ float pressure_sweep8x2v(int i, int lane, const PressureArgs a,
                                                     const PressureNbr& nb, const float* rin,
                                                     const float* vin, float* rout, float* vout,
                                                     float* delta_r) {
     const int gl = lane & 7;
-    const int base_lane = lane & 24;
-    const unsigned int gmask = 0xffu << base_lane;
     const bool live = i < a.n;
     const float ri = live ? LD::ld(&rin[i]) : 0.f;
     float d = 0.f;
@@ -511,27 +546,7 @@ __device__ __forceinline__ float pressure_sweep8x2v(int i, int lane, const Press
         const float Vi = LD::ld(&vin[i]);
         const float vj0 = nb.ok[0] ? LD::ld(&vin[nb.j[0]]) : 0.f;
         const float vj1 = nb.ok[1] ? LD::ld(&vin[nb.j[1]]) : 0.f;
-        const float invP = fdiv(1.0f, a.P);
-        float term[2] = {0.f, 0.f};
-#pragma unroll
-        for (int h = 0; h < 2; ++h) {
-            if (nb.ok[h]) {
-                const float Vj = h == 0 ? vj0 : vj1;
-                const float dvr = fmul(a.k, fsub(Vi, Vj));
-                const float vmin = fminf(Vi, Vj);
-                const float dv = fmaxf(fmul(-a.cap, vmin), fminf(fmul(a.cap, vmin), dvr));
-                term[h] = fsub(powf(fsub(Vi, dv), invP), ri);
-            }
-        }
-#pragma unroll
-        for (int h = 0; h < 2; ++h) {
-            unsigned int m = (__ballot_sync(gmask, nb.ok[h]) & gmask) >> base_lane;
-            while (m) {
-                const int b = __ffs(m) - 1;
-                m &= m - 1;
-                d = fadd(d, __shfl_sync(gmask, term[h], b, 8));
-            }
-        }
+        d = pressure_sum8x2(a, nb, lane, ri, Vi, vj0, vj1);
     }
     if (live && gl == 0) {
         delta_r[i] = d;
