@@ -214,28 +214,30 @@ __device__ bool coop_csr(const Args& a, const Geo& geo, const int32_t* cnt, cons
     extern __shared__ int s_tab[];  // small form: G3 + 1 exclusive starts
     const int T = gridDim.x * blockDim.x;
     if (a.small_grid) {
-        // P2: whole-table scan per block, then the rank scatter
+        // P2: the whole count table into shared memory with coalesced loads
+        // (each block reads each line once), a scan per block (each thread
+        // takes `per` consecutive cells), then the rank scatter
+        for (int c = threadIdx.x; c < a.G3; c += blockDim.x) s_tab[c] = __ldcg(&cnt[c]);
+        __syncthreads();
         const int per = (a.G3 + blockDim.x - 1) / blockDim.x;
         const int b0 = threadIdx.x * per, b1 = min(a.G3, b0 + per);
         int sum = 0;
-        for (int c = b0; c < b1; ++c) {
-            int v = __ldcg(&cnt[c]);
-            s_tab[c] = v;
-            sum += v;
-        }
+        for (int c = b0; c < b1; ++c) sum += s_tab[c];
         int tot;
         int run = coop_block_scan(sum, &tot);
         for (int c = b0; c < b1; ++c) {
             int v = s_tab[c];
             s_tab[c] = run;
-            if (blockIdx.x == 0) {
-                a.cc[c] = v;
-                a.cs[c] = run;
-            }
             run += v;
         }
         if (threadIdx.x == 0) s_tab[a.G3] = tot;
         __syncthreads();
+        if (blockIdx.x == 0) {
+            for (int c = threadIdx.x; c < a.G3; c += blockDim.x) {
+                a.cs[c] = s_tab[c];
+                a.cc[c] = s_tab[c + 1] - s_tab[c];
+            }
+        }
         for (int i = spread_tid(); i < a.n; i += T)
             a.ci_tmp[s_tab[__ldcg(&a.cellof[i])] + __ldcg(&a.rank[i])] = i;
         if (!grid_barrier(a.ds, ep)) return false;
