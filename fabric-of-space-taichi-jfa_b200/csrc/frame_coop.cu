@@ -159,7 +159,9 @@ __global__ void __launch_bounds__(COOP_THREADS) k_frame_coop(CoopArgs a) {
     const int tid = blockIdx.x * blockDim.x + threadIdx.x;
     const int lane = threadIdx.x & 31;
     const int W = T >> 5;
-    const int wid = tid >> 5;
+    // warp index for one-warp-per-particle loops: consecutive warps on
+    // consecutive blocks, so a last partial round spreads over every SM
+    const int wid = (threadIdx.x >> 5) * gridDim.x + blockIdx.x;
     // rounds of work with block-uniform trip counts (block reductions inside)
     const int warp_rounds = (a.n + W - 1) / W;
     int tk = 0;
