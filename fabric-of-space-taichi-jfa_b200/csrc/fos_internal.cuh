@@ -43,6 +43,8 @@ struct FosDevState {
     unsigned long long rad_sum;   // OU jitter: sum of the radii, 2^-40 fixed point
     int tile_count;               // fos_dirty_count: marked tiles
     unsigned int coop_epoch;      // cooperative frame launches (tags of the pressure words)
+    unsigned int rmax_bits;       // cooperative frame: largest radius before the PBD sweeps
+    unsigned int pad_rm;
     unsigned long long changes[FOS_MAX_PASSES];
 };
 

@@ -325,9 +325,12 @@ __global__ void __launch_bounds__(COOP_THREADS) k_frame_coop(CoopArgs a) {
     {
         unsigned int frame = (unsigned int)pa.frame;
         long long rq = 0;
+        unsigned int rmx = 0u;  // the largest radius (positive floats order as their bits)
         for (int i = spread_tid(); i < a.n; i += T) {
             if ((a.sweeps & 1) && !a.ptag) a.rad[i] = __ldcg(&a.rad_tmp[i]);
-            if (a.ou) rq += rad_fixed(__ldcg(&a.rad[i]));
+            const float r_i = __ldcg(&a.rad[i]);
+            if (a.ou) rq += rad_fixed(r_i);
+            rmx = max(rmx, __float_as_uint(r_i));
             brownian_one<LdL2>(i, (unsigned int)i, a.pos, a.strength, a.domain, a.halfL, a.k0,
                                a.k1, frame);
             coop_p1_one(a, geo, i, a.pos, a.rad, a.pos, coop_p1_dst(a, 1));
@@ -337,10 +340,18 @@ __global__ void __launch_bounds__(COOP_THREADS) k_frame_coop(CoopArgs a) {
             for (int o = 16; o >= 1; o >>= 1) rq += __shfl_xor_sync(0xffffffffu, rq, o);
             if (lane == 0 && rq) atomicAdd(&a.ds->rad_sum, (unsigned long long)rq);
         }
+        block_max_atomic(__reduce_max_sync(0xffffffffu, rmx), &a.ds->rmax_bits);
         if (tid == 0 && a.ds->settle > 0) a.ds->settle -= 1;
     }
-    if (!grid_barrier(a.ds, ep, &gfl)) return;
+    const unsigned int* const fwr[1] = {&a.ds->rmax_bits};
+    unsigned int fvr[1];
+    if (!grid_barrier(a.ds, ep, &gfl, fwr, 1, fvr)) return;
     trace_mark(a, tk);
+    // The PBD sweeps' stencils skip the cells that cannot hold an overlap
+    // (radii are fixed during the sweeps; see stencil_ranges_near).  A radius
+    // that is not a positive number leaves the full stencil.
+    const float rmax_all = a.g.G >= 5 ? __uint_as_float(fvr[0]) : 0.f;
+    const float cell_w = a.g.L / (float)a.g.G;
     // (6) PBD passes, each on a fresh grid (run.py:829-846); (7) rebuild (run.py:874)
     // Every rebuild here has its P1 done by the phase that produced the
     // positions (Brownian, then each PBD sweep's lane 0).
@@ -367,7 +378,8 @@ __global__ void __launch_bounds__(COOP_THREADS) k_frame_coop(CoopArgs a) {
                 float4 nv = make_float4(0.f, 0.f, 0.f, 0.f);
                 const int pi =
                     rows ? pbd_warp_rows<LdL1>(kk, lane, lay.sp, lay.ci, a.pos_tmp, a.g, lay.cc,
-                                               COOP_CAP, a.gap1, a.mdf, a.dmul, &nv)
+                                               COOP_CAP, a.gap1, a.mdf, a.dmul, &nv, rmax_all,
+                                               cell_w)
                          : pbd_warp<LdL1>(kk, lane, lay.sp, lay.ci, a.pos_tmp, a.g, lay.cs,
                                           lay.cc, a.gap1, a.mdf, a.dmul, &nv, lay.cap);
                 p1.put(a, geo, lane, pi, nv, a.pos, next, ou_here ? &ous : nullptr);
@@ -383,6 +395,7 @@ __global__ void __launch_bounds__(COOP_THREADS) k_frame_coop(CoopArgs a) {
 
 __global__ void k_coop_prep(FosDevState* ds) {
     ds->coop_epoch += 1u;
+    ds->rmax_bits = 0u;
     ds->grid_ovf = 0;
     ds->rad_sum = 0ull;
     ds->omax_bits = 0u;

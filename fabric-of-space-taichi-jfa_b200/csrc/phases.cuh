@@ -137,6 +137,59 @@ struct GridGeom {
     float L, invL, halfL;
 };
 
+// stencil_ranges on fixed-capacity rows (cap slots a cell) with the cells that
+// cannot hold a particle within `reach` of p dropped (their count taken as 0).
+// Per axis, the nearest point of a neighbour cell is at least as far from p
+// as the home cell's face on that side (rel: p's offset from the home cell's
+// lower face, cs: the cell width), less `margin`, which covers float error and
+// the 1e-7 offset of the cell assignment; a cell whose squared bound exceeds
+// reach2 is skipped.  The other candidates keep their stencil order, so any
+// pair within reach is enumerated exactly as by stencil_ranges.  Needs G >= 5,
+// so that the adjacent cells are the nearest periodic images.
+template <class LD>
+__device__ __forceinline__ Stencil stencil_ranges_near(float px, float py, float pz,
+                                                       const GridGeom& g, float cs,
+                                                       const int32_t* cc, int lane, int cap,
+                                                       float reach2, float margin) {
+    const float p3[3] = {px, py, pz};
+    int h[3];
+    float rel[3];
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {  // home_coord, keeping the wrapped position
+        const float w = grid_wrap(p3[a], g.L, g.invL);
+        h[a] = (int)fmul(fmul(fadd(w, g.halfL), g.invL), (float)g.G);
+        rel[a] = w - ((float)h[a] * cs - g.halfL);
+    }
+    int st = 0, ct = 0;
+    if (lane < 27) {
+        const int o[3] = {lane / 9 - 1, (lane / 3) % 3 - 1, lane % 3 - 1};
+        const int nx = wrap_near(h[0] + o[0], g.G);
+        const int ny = wrap_near(h[1] + o[1], g.G);
+        const int nz = wrap_near(h[2] + o[2], g.G);
+        const int cid = (nx * g.G + ny) * g.G + nz;
+        st = cid * cap;
+        float b2 = 0.f;
+#pragma unroll
+        for (int a = 0; a < 3; ++a) {
+            const float b = o[a] == 0 ? 0.f : fmaxf(0.f, (o[a] < 0 ? rel[a] : cs - rel[a]) - margin);
+            b2 += b * b;
+        }
+        ct = b2 > reach2 ? 0 : LD::ld(&cc[cid]);
+    }
+    int incl = ct;
+#pragma unroll
+    for (int k = 1; k < 32; k <<= 1) {
+        int y = __shfl_up_sync(0xffffffffu, incl, k);
+        if (lane >= k) incl += y;
+    }
+    Stencil r;
+    r.st = st;
+    r.incl = incl;
+    r.excl = incl - ct;
+    r.total = __shfl_sync(0xffffffffu, incl, 31);
+    return r;
+}
+
 // Correction of project_overlaps (dynamics.py:120-160) from candidate q on a
 // particle at p with radius ri (md = mdf * ri); false when they do not overlap.
 __device__ __forceinline__ bool pbd_term(float4 q, float px, float py, float pz, float ri,
@@ -268,15 +321,25 @@ __device__ __forceinline__ int pbd_warp(int kk, int lane, const float4* sp, cons
 // the reference's loop order, so the sum is pbd_warp's bit for bit.  The
 // candidates' particle indices come with their (pos, rad); requires
 // n <= 2^26 (the key packs the cell above bit 26).
+//
+// rmax > 0 (the largest radius of any particle; G >= 5): the stencil keeps only
+// the cells that can hold a particle within (ri + rmax) * gap1 of p
+// (stencil_ranges_near), which is every cell that can hold an overlap.
 template <class LD>
 __device__ __forceinline__ int pbd_warp_rows(int kk, int lane, const float4* sp, const int32_t* ci,
                                              float* pout, const GridGeom g, const int32_t* cc,
                                              int cap, float gap1, float mdf, float dmul,
-                                             float4* np) {
+                                             float4* np, float rmax = 0.f, float cs = 0.f) {
     float4 me = LD::ld(&sp[kk]);
     float px = me.x, py = me.y, pz = me.z, ri = me.w;
-    Stencil r = stencil_ranges<LD>(px, py, pz, g.L, g.invL, g.halfL, g.G, nullptr, cc, lane, cap,
-                                   0);
+    Stencil r;
+    if (rmax > 0.f) {
+        const float reach = (ri + rmax) * gap1 * 1.0001f;
+        r = stencil_ranges_near<LD>(px, py, pz, g, cs, cc, lane, cap, reach * reach,
+                                    1e-5f * g.L + 1e-6f);
+    } else {
+        r = stencil_ranges<LD>(px, py, pz, g.L, g.invL, g.halfL, g.G, nullptr, cc, lane, cap, 0);
+    }
     float md = fmul(mdf, ri);
     float cx = 0.f, cy = 0.f, cz = 0.f;
     for (int base = 0; base < r.total;) {  // warp-uniform
