@@ -44,7 +44,7 @@ struct FosDevState {
     int tile_count;               // fos_dirty_count: marked tiles
     unsigned int coop_epoch;      // cooperative frame launches (tags of the pressure words)
     unsigned int rmax_bits;       // cooperative frame: largest radius before the PBD sweeps
-    unsigned int pad_rm;
+    unsigned int rmax0_bits;      // cooperative frame: largest radius at the frame's start
     unsigned long long changes[FOS_MAX_PASSES];
 };
 
@@ -184,9 +184,11 @@ int fos_sur_frame_before_jfa(FosCtx* c, const FosSurrogate* m, const FosState* s
 int fos_sur_frame_judge(FosCtx* c, int n, cudaStream_t s);
 int fos_sur_frame_between(FosCtx* c, const FosSurrogate* m, const FosState* st,
                           const FosFrameParams* fp, cudaStream_t s);
+// end_frame: the kernel is the frame's last one and advances the frame counter
+// itself (k_frame_end's job).
 int fos_frame_coop_dynamics(FosCtx* c, const FosState* st, const FosFrameParams* fp,
                             cudaStream_t s, unsigned long long* trace = nullptr,
-                            int trace_cap = 0);
+                            int trace_cap = 0, int end_frame = 0);
 
 // ------------------------------------------------------------ device math
 __device__ __forceinline__ float fadd(float a, float b) { return __fadd_rn(a, b); }

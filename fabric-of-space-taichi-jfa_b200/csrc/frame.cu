@@ -199,12 +199,15 @@ static int frame_impl(FosCtx* c, const FosState* st, const FosFrameParams* fp, i
 #define MARK(id) \
     if (prof) prof->mark(id)
     const int* dframe = &c->ds->frame;
+    bool coop_ends = false;
     if (!(part & FRAME_DYNAMICS)) {
         // measurement part only
     } else if (c->use_coop && !prof && fp->max_eq_nei <= 16 && !(fp->ou_jitter && fp->pbd_iters == 0) &&
         fos_coop_supported(c)) {
-        // (1)-(7) as one persistent cooperative kernel (frame_coop.cu)
-        rc = fos_frame_coop_dynamics(c, st, fp, s);
+        // (1)-(7) as one persistent cooperative kernel (frame_coop.cu); a plain
+        // frame ends there, and the kernel advances the frame counter itself
+        coop_ends = (part & FRAME_MEASURE) && !jfa_frame && !sur;
+        rc = fos_frame_coop_dynamics(c, st, fp, s, nullptr, 0, coop_ends ? 1 : 0);
         if (rc) return rc;
     } else {
         // (1) rebuild_grid (run.py:704)
@@ -300,8 +303,10 @@ static int frame_impl(FosCtx* c, const FosState* st, const FosFrameParams* fp, i
             if (rc) return rc;
         }
     }
-    k_frame_end<<<1, 1, 0, s>>>(c->ds);
-    FOS_LAUNCHED(c);
+    if (!coop_ends) {
+        k_frame_end<<<1, 1, 0, s>>>(c->ds);
+        FOS_LAUNCHED(c);
+    }
     MARK(9);
 #undef MARK
     return FOS_OK;

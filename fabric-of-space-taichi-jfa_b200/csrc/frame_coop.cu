@@ -58,6 +58,7 @@ struct CoopArgs {
     OuParams ou_p;
     unsigned long long* trace;  // optional: %globaltimer after every phase (block 0)
     int trace_cap;
+    int end_frame;              // advance the frame counter at the end (k_frame_end)
 };
 
 // Tagged pressure words: (tag << 32) | float bits, written and read whole, so
@@ -174,16 +175,30 @@ __global__ void __launch_bounds__(COOP_THREADS) k_frame_coop(CoopArgs a) {
     bool rows = false;
     {
         const P1Dst t = coop_p1_dst(a, 0);
-        for (int i = spread_tid(); i < a.n; i += T) coop_p1_one(a, geo, i, a.pos, a.rad, a.pos, t);
+        unsigned int rmx = 0u;  // the largest radius (positive floats order as their bits)
+        for (int i = spread_tid(); i < a.n; i += T) {
+            const float r_i = __ldcg(&a.rad[i]);
+            rmx = max(rmx, __float_as_uint(r_i));
+            coop_p1_val(a, geo, i,
+                        make_float3(__ldcg(&a.pos[3 * i + 0]), __ldcg(&a.pos[3 * i + 1]),
+                                    __ldcg(&a.pos[3 * i + 2])),
+                        r_i, a.pos, t);
+        }
+        block_max_atomic(__reduce_max_sync(0xffffffffu, rmx), &a.ds->rmax0_bits);
     }
     unsigned int gfl = 0u;  // overflow flags from the barrier after the last P1
-    if (!grid_barrier(a.ds, ep, &gfl)) return;
+    const unsigned int* const fw0[1] = {&a.ds->rmax0_bits};
+    unsigned int fv0[1];
+    if (!grid_barrier(a.ds, ep, &gfl, fw0, 1, fv0)) return;
     trace_mark(a, tk);
+    const float cell_w = a.g.L / (float)a.g.G;
     // (2) compute_max_overlap (run.py:709): particle i's slot comes from
     // slot_of, prefetched one round ahead (the rows' slots come from P1; the
     // CSR form rewrites slot_of, and the first prefetch is then repeated).
     int kk0 = wid < a.n ? __ldcg(&a.slot_of[wid]) : 0;
     if (!coop_layout(a, geo, 0, gfl, tk, ep, lay, rows)) return;
+    // max overlap visits only the cells that can hold a positive depth (rows only)
+    const float rmax0 = rows && a.g.G >= 5 ? __uint_as_float(fv0[0]) : 0.f;
     if (!rows) kk0 = wid < a.n ? __ldcg(&a.slot_of[wid]) : 0;
     {
         unsigned int wmax = 0u;
@@ -194,7 +209,7 @@ __global__ void __launch_bounds__(COOP_THREADS) k_frame_coop(CoopArgs a) {
             kk_next = i + W < a.n ? __ldcg(&a.slot_of[i + W]) : 0;
             if (i < a.n) {
                 unsigned int b = maxov_warp<LdL1>(kk, lane, lay.sp, lay.ci, a.g, lay.cs, lay.cc,
-                                                  a.eps, a.lmd, lay.cap);
+                                                  a.eps, a.lmd, lay.cap, 0, rmax0, cell_w);
                 wmax = b > wmax ? b : wmax;
             }
         }
@@ -351,7 +366,6 @@ __global__ void __launch_bounds__(COOP_THREADS) k_frame_coop(CoopArgs a) {
     // (radii are fixed during the sweeps; see stencil_ranges_near).  A radius
     // that is not a positive number leaves the full stencil.
     const float rmax_all = a.g.G >= 5 ? __uint_as_float(fvr[0]) : 0.f;
-    const float cell_w = a.g.L / (float)a.g.G;
     // (6) PBD passes, each on a fresh grid (run.py:829-846); (7) rebuild (run.py:874)
     // Every rebuild here has its P1 done by the phase that produced the
     // positions (Brownian, then each PBD sweep's lane 0).
@@ -389,19 +403,29 @@ __global__ void __launch_bounds__(COOP_THREADS) k_frame_coop(CoopArgs a) {
         if (!grid_barrier(a.ds, ep, &gfl)) return;
         trace_mark(a, tk);
     }
-    coop_csr(a, geo, a.cnt + (size_t)((a.pbd_iters + 1) % 3) * a.G3, a.pos, nullptr, true, tk,
-             ep);
+    if (!coop_csr(a, geo, a.cnt + (size_t)((a.pbd_iters + 1) % 3) * a.G3, a.pos, nullptr, true,
+                  tk, ep))
+        return;
+    // every block has read the frame counter (it was fetched after max overlap)
+    if (a.end_frame && blockIdx.x == 0 && threadIdx.x == 0) a.ds->frame += 1;
 }
 
-__global__ void k_coop_prep(FosDevState* ds) {
-    ds->coop_epoch += 1u;
-    ds->rmax_bits = 0u;
-    ds->grid_ovf = 0;
-    ds->rad_sum = 0ull;
-    ds->omax_bits = 0u;
-    ds->maxabs_dr_bits = 0u;
-    ds->changed = 0;
-    ds->bar_count = 0u;
+// Per-launch state of the cooperative frame, and count buffers 0 and 1 of
+// its rebuilds cleared (the frame clears buffer 2 itself).
+__global__ void k_coop_prep(FosDevState* ds, int32_t* cnt01, int m) {
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    for (int k = t; k < m; k += gridDim.x * blockDim.x) cnt01[k] = 0;
+    if (t == 0) {
+        ds->coop_epoch += 1u;
+        ds->rmax_bits = 0u;
+        ds->rmax0_bits = 0u;
+        ds->grid_ovf = 0;
+        ds->rad_sum = 0ull;
+        ds->omax_bits = 0u;
+        ds->maxabs_dr_bits = 0u;
+        ds->changed = 0;
+        ds->bar_count = 0u;
+    }
 }
 
 // Host side ---------------------------------------------------------------
@@ -428,7 +452,8 @@ bool fos_coop_supported(FosCtx* c) {
 }
 
 int fos_frame_coop_dynamics(FosCtx* c, const FosState* st, const FosFrameParams* fp,
-                            cudaStream_t s, unsigned long long* trace, int trace_cap) {
+                            cudaStream_t s, unsigned long long* trace, int trace_cap,
+                            int end_frame) {
     int blocks = coop_grid_size(c);
     FOS_REQUIRE(blocks > 0, FOS_E_CUDA, "cooperative frame kernel cannot be resident");
     const int n = st->n;
@@ -506,15 +531,15 @@ int fos_frame_coop_dynamics(FosCtx* c, const FosState* st, const FosFrameParams*
                        (float)fp->dt, c->L, c->invL, fp->seed);
     a.trace = trace;
     a.trace_cap = trace_cap;
+    a.end_frame = end_frame;
 
     FOS_REQUIRE(fp->max_eq_nei <= 16, FOS_E_ARG, "cooperative frame needs max_eq_nei <= 16");
     FOS_REQUIRE(n <= (1 << 26), FOS_E_ARG, "cooperative frame supports up to 2^26 particles");
     FOS_REQUIRE(!a.ou || fp->pbd_iters >= 1, FOS_E_ARG,
                 "cooperative frame runs the OU jitter inside a PBD sweep: pbd_iters >= 1");
-    k_coop_prep<<<1, 1, 0, s>>>(c->ds);
+    k_coop_prep<<<fos_blocks(2LL * G3, 256) < 64 ? fos_blocks(2LL * G3, 256) : 64, 256, 0, s>>>(
+        c->ds, c->coop_cnt, 2 * G3);
     FOS_LAUNCHED(c);
-    // count buffers 0 and 1 start empty (the frame clears buffer 2 itself)
-    FOS_CUDA(cudaMemsetAsync(c->coop_cnt, 0, 2 * (size_t)G3 * sizeof(int32_t), s));
     cudaLaunchConfig_t cfg = {};
     cfg.gridDim = dim3(blocks);
     cfg.blockDim = dim3(COOP_THREADS);

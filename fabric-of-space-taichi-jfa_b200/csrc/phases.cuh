@@ -386,15 +386,26 @@ __device__ __forceinline__ float maxov_term(float4 q, float4 me, float eps, cons
 // compute_local_max_overlaps (dynamics.py:304-352) for the particle at
 // sorted position kk (pairs i < j only); writes lmd[i] and returns the depth's
 // float bits (non-negative floats order as their bits).  All 32 lanes.
+// rmax > 0 (fixed-capacity rows, cell_base 0, G >= 5; rmax the largest
+// radius): only the cells that can hold a particle within ri + rmax, the
+// only ones with a positive depth, are visited (stencil_ranges_near).
 template <class LD>
 __device__ __forceinline__ unsigned int maxov_warp(int kk, int lane, const float4* sp,
                                                    const int32_t* ci, const GridGeom g,
                                                    const int32_t* cs, const int32_t* cc, float eps,
-                                                   float* lmd, int cap = 0, int cell_base = 0) {
+                                                   float* lmd, int cap = 0, int cell_base = 0,
+                                                   float rmax = 0.f, float cell_w = 0.f) {
     float4 me = LD::ld(&sp[kk]);
     int i = LD::ld(&ci[kk]);
-    Stencil r = stencil_ranges<LD>(me.x, me.y, me.z, g.L, g.invL, g.halfL, g.G, cs, cc, lane, cap,
-                                   cell_base);
+    Stencil r;
+    if (rmax > 0.f) {
+        const float reach = (me.w + rmax) * 1.0001f;
+        r = stencil_ranges_near<LD>(me.x, me.y, me.z, g, cell_w, cc, lane, cap, reach * reach,
+                                    1e-5f * g.L + 1e-6f);
+    } else {
+        r = stencil_ranges<LD>(me.x, me.y, me.z, g.L, g.invL, g.halfL, g.G, cs, cc, lane, cap,
+                               cell_base);
+    }
     float lm = 0.f;
     for (int base = 0; base < r.total; base += 32) {
         int t = base + lane;
