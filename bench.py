@@ -379,7 +379,7 @@ def run_fos(args):
                                     "fallback 6650 GB/s",
                      "traffic": traffic.get("k_frame_coop"),
                      "alg_bytes_per_launch": coop_bytes, "launch_us": round(coop_s * 1e6, 2),
-                     "note": "latency/barrier bound: 34 phases (33 grid barriers) over L2-resident "
+                     "note": "latency/barrier bound: 14 phases (13 grid barriers) over L2-resident "
                              "data; HBM is not the limiting roof"},
         "roofline_jfa_pass": {"bound": "hbm", "kernel": "k_jfa_pass (128^3, one pass)",
                               "achieved": round(achieved, 2), "peak": peak, "unit": "GB/s",
