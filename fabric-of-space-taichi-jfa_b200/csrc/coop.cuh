@@ -29,7 +29,7 @@ __device__ __forceinline__ unsigned long long global_ns() {
 // Records a timestamp in trace[k++] from block 0, thread 0 (tracing only).
 template <class Args>
 __device__ __forceinline__ void trace_mark(const Args& a, int& k) {
-    if (a.trace && blockIdx.x == 0 && threadIdx.x == 0 && k < a.trace_cap) a.trace[k] = global_ns();
+    if (a.trace && blockIdx.x == 0 && threadIdx.x == 0 && k < a.trace_cap - 2) a.trace[k] = global_ns();
     ++k;
 }
 

@@ -56,8 +56,8 @@ struct CoopArgs {
     int ou;                     // OU jitter fused into the last PBD sweep (pbd_iters >= 1)
     float* vjit;
     OuParams ou_p;
-    unsigned long long* trace;  // optional: %globaltimer after every phase (block 0)
-    int trace_cap;
+    unsigned long long* trace;  // optional: %globaltimer after every phase (block 0); the
+    int trace_cap;              // last two slots: ~(earliest block start), latest block end
     int end_frame;              // advance the frame counter at the end (k_frame_end)
 };
 
@@ -74,33 +74,37 @@ __device__ __forceinline__ unsigned long long ld_tagged(const unsigned long long
     return w;
 }
 
-// Every lane waits for the words at p0 / p1 (where need0 / need1) to carry
-// `tag` and gets their values; the whole warp polls together, so the warp's
+// Lanes per particle of the barrier-free pressure sweeps (a power of two
+// dividing 16: each lane takes 16 / COOP_PLANES neighbours).
+#ifndef COOP_PLANES
+#define COOP_PLANES 8
+#endif
+
+// Every lane waits for the words base[j[h]] (where need[h]) to carry `tag`
+// and gets their values in v[h]; the whole warp polls together, so the warp's
 // groups never diverge.  Bounded like the grid barrier: after ~1 s, or once
 // the error word is set, it records FOS_E_TIMEOUT, clears ok and returns
 // (the next grid barrier then ends the kernel).
-__device__ __forceinline__ void wait_tagged2(const unsigned long long* p0,
-                                             const unsigned long long* p1, bool need0,
-                                             bool need1, unsigned int tag, FosDevState* ds,
-                                             bool& ok, float& v0, float& v1) {
+template <int H>
+__device__ __forceinline__ void wait_tagged_n(const unsigned long long* base, const int* j,
+                                              bool* need, unsigned int tag, FosDevState* ds,
+                                              bool& ok, float* v) {
     const long long t0 = clock64();
     unsigned int polls = 0;
     for (;;) {
-        if (need0) {
-            const unsigned long long w = ld_tagged(p0);
-            if ((unsigned int)(w >> 32) == tag) {
-                v0 = __uint_as_float((unsigned int)w);
-                need0 = false;
+        bool any = false;
+#pragma unroll
+        for (int h = 0; h < H; ++h) {
+            if (need[h]) {
+                const unsigned long long w = ld_tagged(&base[j[h]]);
+                if ((unsigned int)(w >> 32) == tag) {
+                    v[h] = __uint_as_float((unsigned int)w);
+                    need[h] = false;
+                }
             }
+            any |= need[h];
         }
-        if (need1) {
-            const unsigned long long w = ld_tagged(p1);
-            if ((unsigned int)(w >> 32) == tag) {
-                v1 = __uint_as_float((unsigned int)w);
-                need1 = false;
-            }
-        }
-        if (!__any_sync(0xffffffffu, need0 || need1) || !ok) return;
+        if (!__any_sync(0xffffffffu, any) || !ok) return;
         if ((++polls & 31u) == 0u &&
             __any_sync(0xffffffffu, *((volatile int*)&ds->error) != 0 ||
                                         clock64() - t0 > FOS_BAR_CYCLE_LIMIT)) {
@@ -167,6 +171,7 @@ __global__ void __launch_bounds__(COOP_THREADS) k_frame_coop(CoopArgs a) {
     const int warp_rounds = (a.n + W - 1) / W;
     int tk = 0;
     unsigned int ep = 0;
+    if (a.trace && threadIdx.x == 0) atomicMax(&a.trace[a.trace_cap - 2], ~global_ns());
     trace_mark(a, tk);
 
     // (1) rebuild_grid (run.py:704): rebuild 0's P1, then its layout
@@ -231,14 +236,17 @@ __global__ void __launch_bounds__(COOP_THREADS) k_frame_coop(CoopArgs a) {
     const int i_one =
         (int)((((threadIdx.x >> 5) * gridDim.x + blockIdx.x) << 2) + ((threadIdx.x >> 3) & 3));
     if (a.ptag) {
-        // (3) + (4) without grid barriers (n <= T/8, 1 <= sweeps <= FOS_PTAG_SWEEPS):
-        // each 8-lane group nudges its particle and runs every pressure sweep
-        // on it.  The power r^P that starts sweep w is published as the word
-        // ptag[w * n + i] tagged (epoch << 7) | (w + 1), and a sweep waits for
-        // its neighbours' words of the same sweep, so it reads exactly the
-        // values a barrier between the sweeps would give.  Every sweep has its
-        // own words: a particle may run ahead of the particles that read it.
-        const int i = i_one, gl = lane & 7;
+        // (3) + (4) without grid barriers (n * COOP_PLANES <= T,
+        // 1 <= sweeps <= FOS_PTAG_SWEEPS): each group of COOP_PLANES lanes
+        // nudges its particle and runs every pressure sweep on it.  The power
+        // r^P that starts sweep w is published as the word ptag[w * n + i]
+        // tagged (epoch << 7) | (w + 1), and a sweep waits for its neighbours'
+        // words of the same sweep, so it reads exactly the values a barrier
+        // between the sweeps would give.  Every sweep has its own words: a
+        // particle may run ahead of the particles that read it.
+        constexpr int NL = COOP_PLANES, H = 16 / COOP_PLANES;
+        const int i = (((threadIdx.x >> 5) * gridDim.x + blockIdx.x) * (32 / NL)) + (lane / NL);
+        const int gl = lane & (NL - 1);
         const bool live = i < a.n;
         const unsigned int tbase = fv[3] << 7;
         float ri = 0.f;
@@ -253,17 +261,21 @@ __global__ void __launch_bounds__(COOP_THREADS) k_frame_coop(CoopArgs a) {
             if (nudge) a.rad[i] = ri;
             st_tagged(&a.ptag[i], tbase | 1u, Vi);
         }
-        const PressureNbr nb = pressure_nbr8x2<LdL2>(i, lane, pa);
+        const PressureNbrN<NL> nb = pressure_nbr_n<NL, LdL2>(i, lane, pa);
         bool ok = true;
         float d = 0.f;
         for (int w = 0; w < a.sweeps; ++w) {
             const unsigned int tag = tbase | (unsigned int)(w + 1);
-            const unsigned long long* words = a.ptag + (size_t)w * a.n;
             d = 0.f;
-            float vj0 = 0.f, vj1 = 0.f;
-            wait_tagged2(&words[nb.j[0]], &words[nb.j[1]], nb.fc > 0 && nb.ok[0],
-                         nb.fc > 0 && nb.ok[1], tag, a.ds, ok, vj0, vj1);
-            if (nb.fc > 0) d = pressure_sum8x2(pa, nb, lane, ri, Vi, vj0, vj1);
+            float vj[H];
+            bool need[H];
+#pragma unroll
+            for (int h = 0; h < H; ++h) {
+                vj[h] = 0.f;
+                need[h] = nb.fc > 0 && nb.ok[h];
+            }
+            wait_tagged_n<H>(a.ptag + (size_t)w * a.n, nb.j, need, tag, a.ds, ok, vj);
+            if (nb.fc > 0) d = pressure_sum_n<NL>(pa, nb, lane, ri, Vi, vj);
             ri = fmaxf(pa.rmin, fminf(pa.rmax, fadd(ri, d)));
             if (w + 1 < a.sweeps) {
                 Vi = powf(ri, pa.P);
@@ -408,6 +420,10 @@ __global__ void __launch_bounds__(COOP_THREADS) k_frame_coop(CoopArgs a) {
         return;
     // every block has read the frame counter (it was fetched after max overlap)
     if (a.end_frame && blockIdx.x == 0 && threadIdx.x == 0) a.ds->frame += 1;
+    if (a.trace) {
+        __syncthreads();
+        if (threadIdx.x == 0) atomicMax(&a.trace[a.trace_cap - 1], global_ns());
+    }
 }
 
 // Per-launch state of the cooperative frame, and count buffers 0 and 1 of
@@ -492,7 +508,7 @@ int fos_frame_coop_dynamics(FosCtx* c, const FosState* st, const FosFrameParams*
     a.vol0 = c->pvol;
     a.vol1 = c->pvol + c->max_n;
     // barrier-free pressure sweeps: every particle in one 8-lane group
-    if (c->ptag && n <= c->ptag_n && (long long)n * 8 <= (long long)blocks * COOP_THREADS &&
+    if (c->ptag && n <= c->ptag_n && (long long)n * COOP_PLANES <= (long long)blocks * COOP_THREADS &&
         fp->pressure_iters >= 1 && fp->pressure_iters <= FOS_PTAG_SWEEPS)
         a.ptag = c->ptag;
     a.part = c->coop_part;
@@ -559,7 +575,7 @@ int fos_frame_coop_dynamics(FosCtx* c, const FosState* st, const FosFrameParams*
 // (block 0's view): stamp 0 at kernel entry, then one per grid barrier.
 extern "C" int fos_frame_trace(FosCtx* c, const FosState* st, const FosFrameParams* fp,
                                long long* ns_host, int cap, int* count, fos_stream_t s) {
-    FOS_REQUIRE(c && st && fp && ns_host && count && cap > 0, FOS_E_ARG, "NULL argument");
+    FOS_REQUIRE(c && st && fp && ns_host && count && cap >= 3, FOS_E_ARG, "NULL argument or cap < 3");
     FOS_REQUIRE(fos_coop_supported(c), FOS_E_STATE, "cooperative launch unsupported");
     unsigned long long* d = nullptr;
     FOS_CUDA(cudaMalloc(&d, (size_t)cap * 8));
@@ -572,7 +588,7 @@ extern "C" int fos_frame_trace(FosCtx* c, const FosState* st, const FosFramePara
     }
     cudaFree(d);
     int k = 0;
-    while (k < cap && ns_host[k] != 0) ++k;
+    while (k < cap - 2 && ns_host[k] != 0) ++k;
     *count = k;
     return rc;
 }

@@ -522,6 +522,77 @@ __device__ __forceinline__ PressureNbr pressure_nbr8x2(int i, int lane, const Pr
     return nb;
 }
 
+// The same for a group of NL lanes (NL divides 16): lane t of the group takes
+// neighbours t, t + NL, t + 2 NL, ... of the hashed rotation.
+template <int NL>
+struct PressureNbrN {
+    int fc;
+    int j[16 / NL];
+    bool ok[16 / NL];
+};
+
+template <int NL, class LD>
+__device__ __forceinline__ PressureNbrN<NL> pressure_nbr_n(int i, int lane, const PressureArgs a) {
+    PressureNbrN<NL> nb;
+    const int gl = lane & (NL - 1);
+    nb.fc = i < a.n ? LD::ld(&a.fsc[i]) : 0;
+#pragma unroll
+    for (int h = 0; h < 16 / NL; ++h) {
+        nb.j[h] = 0;
+        nb.ok[h] = false;
+    }
+    if (nb.fc > 0) {
+        const int an = nb.fc < a.max_nei ? nb.fc : a.max_nei;
+        const int st = hash_func(i - a.hoff, a.frame) % nb.fc;
+#pragma unroll
+        for (int h = 0; h < 16 / NL; ++h) {
+            const int kk = gl + NL * h;
+            if (kk < an) {
+                const int ni = (st + kk) % nb.fc;
+                const int j = LD::ld(&a.face_ids[(size_t)i * FOS_S + ni]);
+                nb.j[h] = j;
+                nb.ok[h] = !(j < 0 || j >= a.n || j == i);
+            }
+        }
+    }
+    return nb;
+}
+
+// pressure_sum8x2 for NL-lane groups (vj[h]: the power of neighbour h of this
+// lane); the terms are added in neighbour order, so the sum is the same float.
+template <int NL>
+__device__ __forceinline__ float pressure_sum_n(const PressureArgs& a, const PressureNbrN<NL>& nb,
+                                                int lane, float ri, float Vi, const float* vj) {
+    constexpr int H = 16 / NL;
+    const int base_lane = lane & (32 - NL);
+    const unsigned int gmask = ((1u << NL) - 1u) << base_lane;
+    const float invP = fdiv(1.0f, a.P);
+    float term[H];
+#pragma unroll
+    for (int h = 0; h < H; ++h) {
+        term[h] = 0.f;
+        if (nb.ok[h]) {
+            const float Vj = vj[h];
+            const float dvr = fmul(a.k, fsub(Vi, Vj));
+            const float vmin = fminf(Vi, Vj);
+            const float dv = fmaxf(fmul(-a.cap, vmin), fminf(fmul(a.cap, vmin), dvr));
+            term[h] = fsub(powf(fsub(Vi, dv), invP), ri);
+        }
+    }
+    float d = 0.f;
+#pragma unroll
+    for (int h = 0; h < H; ++h) {
+        const unsigned int m = (__ballot_sync(gmask, nb.ok[h]) & gmask) >> base_lane;
+        float v[NL];
+#pragma unroll
+        for (int t = 0; t < NL; ++t) v[t] = __shfl_sync(gmask, term[h], t, NL);
+#pragma unroll
+        for (int t = 0; t < NL; ++t)
+            if ((m >> t) & 1u) d = fadd(d, v[t]);
+    }
+    return d;
+}
+
 template <class LD>
 __device__ __forceinline__ float pressure_sweep8x2(int i, int lane, const PressureArgs a,
                                                    const PressureNbr& nb, const float* rin,

@@ -319,7 +319,9 @@ int fos_frame_profile(FosCtx* ctx, const FosState* st, const FosFrameParams* fp,
  * kernel) with a %globaltimer stamp, in ns, at kernel entry and after every
  * grid barrier (block 0's view).  Allocates a scratch buffer and
  * synchronises; for profiling, not for the frame loop.  *count gets the
- * number of stamps written (<= cap). */
+ * number of stamps written (<= cap - 2); ns_host[cap - 2] holds the bitwise
+ * NOT of the earliest block's start and ns_host[cap - 1] the latest block's
+ * end (cap >= 3). */
 int fos_frame_trace(FosCtx* ctx, const FosState* st, const FosFrameParams* fp, long long* ns_host,
                     int cap, int* count, fos_stream_t s);
 /* The frame in two parts, for hosts that decide on the JFA after the
