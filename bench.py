@@ -12,7 +12,8 @@ timed steps is bracketed by CUDA events on the launching stream, with a
 256 MiB L2 flush between steps outside the events; barrier + synchronize
 around the timed region; max over ranks.  e2e repeats the step through the
 public API with host buffers: pinned H2D of pos/rad before and D2H of
-pos/rad/fsc after the 5 frames, inside the timed region.
+pos/rad/fsc after the 5 frames, inside the timed region.  The resident and the
+e2e steps alternate, so both cover the same stretch of the trajectory.
 
 --impl reference times the CPU restatement of the reference (oracle/, the
 reference itself is Python+Taichi and Taichi is not installable here) with all
@@ -243,18 +244,48 @@ def run_fos(args):
     torch_kernels_before = 1 + 8  # flush buffer fill + state tensor fills
     s = torch.cuda.current_stream()
     times = []
+    # e2e through the public API with host buffers, interleaved with the
+    # resident steps so that both numbers cover the same stretch of the
+    # trajectory (the foam packs over the run and frames slow down with it):
+    # each iteration times one resident step, then refreshes the pinned host
+    # copy of the particle state (outside the events) and times one step that
+    # uploads it, runs and reads the state and the FSC back
+    n = foam.n
+    h_pos = torch.empty((n, 3), dtype=torch.float32).pin_memory()
+    h_rad = torch.empty((n,), dtype=torch.float32).pin_memory()
+    h_fsc = torch.empty((n,), dtype=torch.int32).pin_memory()
+    e2e_ms = 0.0
+    launches = 0
     barrier()
     for _ in range(args.steps):
         flush.fill_(1.0)
         e0 = torch.cuda.Event(enable_timing=True)
         e1 = torch.cuda.Event(enable_timing=True)
+        l0 = sim.ctx.launch_count()
         e0.record(s)
         one_step()
         e1.record(s)
+        launches += sim.ctx.launch_count() - l0
         times.append((e0, e1))
+        h_pos.copy_(sim.pos)
+        h_rad.copy_(sim.rad)
+        flush.fill_(1.0)
+        f0 = torch.cuda.Event(enable_timing=True)
+        f1 = torch.cuda.Event(enable_timing=True)
+        l0 = sim.ctx.launch_count()
+        f0.record(s)
+        sim.pos.copy_(h_pos, non_blocking=True)
+        sim.rad.copy_(h_rad, non_blocking=True)
+        one_step()
+        h_pos.copy_(sim.pos, non_blocking=True)
+        h_rad.copy_(sim.rad, non_blocking=True)
+        h_fsc.copy_(sim.fsc, non_blocking=True)
+        f1.record(s)
+        launches += sim.ctx.launch_count() - l0
+        f1.synchronize()
+        e2e_ms += f0.elapsed_time(f1)
     barrier()
     clk = clocks.stop()
-    launches = sim.ctx.launch_count() - launches0
     total_ms = sum(a.elapsed_time(b) for a, b in times)
     t = torch.tensor([total_ms], dtype=torch.float64, device=dev)
     if world > 1:
@@ -262,29 +293,6 @@ def run_fos(args):
     total_ms = float(t.item())
     value = world * FRAMES_PER_STEP * args.steps / (total_ms / 1000.0)
 
-    # ---- e2e through the public API with host buffers
-    n = foam.n
-    h_pos = torch.empty((n, 3), dtype=torch.float32).pin_memory()
-    h_rad = torch.empty((n,), dtype=torch.float32).pin_memory()
-    h_fsc = torch.empty((n,), dtype=torch.int32).pin_memory()
-    h_pos.copy_(sim.pos.cpu())
-    h_rad.copy_(sim.rad.cpu())
-    barrier()
-    e2e_ms = 0.0
-    for _ in range(args.steps):
-        flush.fill_(1.0)
-        e0 = torch.cuda.Event(enable_timing=True)
-        e1 = torch.cuda.Event(enable_timing=True)
-        e0.record(s)
-        sim.pos.copy_(h_pos, non_blocking=True)
-        sim.rad.copy_(h_rad, non_blocking=True)
-        one_step()
-        h_pos.copy_(sim.pos, non_blocking=True)
-        h_rad.copy_(sim.rad, non_blocking=True)
-        h_fsc.copy_(sim.fsc, non_blocking=True)
-        e1.record(s)
-        e1.synchronize()
-        e2e_ms += e0.elapsed_time(e1)
     t = torch.tensor([e2e_ms], dtype=torch.float64, device=dev)
     if world > 1:
         dist.all_reduce(t, op=dist.ReduceOp.MAX)

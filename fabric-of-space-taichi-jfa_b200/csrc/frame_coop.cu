@@ -79,6 +79,11 @@ __device__ __forceinline__ unsigned long long ld_tagged(const unsigned long long
 #ifndef COOP_PLANES
 #define COOP_PLANES 8
 #endif
+// Pause between two polls of a word that is not ready yet, in ns (fewer L2
+// requests from waiting warps).
+#ifndef COOP_POLL_NS
+#define COOP_POLL_NS 0
+#endif
 
 // Every lane waits for the words base[j[h]] (where need[h]) to carry `tag`
 // and gets their values in v[h]; the whole warp polls together, so the warp's
@@ -105,6 +110,7 @@ __device__ __forceinline__ void wait_tagged_n(const unsigned long long* base, co
             any |= need[h];
         }
         if (!__any_sync(0xffffffffu, any) || !ok) return;
+        if (COOP_POLL_NS > 0) __nanosleep(COOP_POLL_NS);
         if ((++polls & 31u) == 0u &&
             __any_sync(0xffffffffu, *((volatile int*)&ds->error) != 0 ||
                                         clock64() - t0 > FOS_BAR_CYCLE_LIMIT)) {
