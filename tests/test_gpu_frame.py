@@ -157,3 +157,30 @@ def test_cooperative_pressure_sweep_counts(sweeps):
         assert torch.equal(getattr(a, key), getattr(b, key)), key
     assert a.counters() == b.counters()
     assert a.ctx.device_error() == 0
+
+
+@pytest.mark.parametrize("r_max,G", [(0.2, 3), (0.13, 4), (0.11, 5)])
+def test_cooperative_frame_on_coarse_grids(r_max, G):
+    """Hash grids of 3 to 5 cells a side: the stencil wraps onto itself below 3
+    distinct neighbours, and the stencil pruning of PBD / max overlap is off
+    below 5 cells (on at 5); the cooperative frame still equals the stage
+    kernels bit for bit."""
+    from fos.inputs import Foam
+    rng = np.random.default_rng(G)
+    n = 150
+    pos = rng.random((n, 3), dtype=np.float32)
+    rad = rng.uniform(0.4 * r_max, r_max, n).astype(np.float32)
+    foam = Foam(f"coarse-{G}", pos, rad, 32, 0.3 * r_max, r_max, 6, 14, 4, 10, 2, 2, 6, G)
+    a = FoamSim.from_foam(foam, use_graph=True)
+    b = FoamSim.from_foam(foam, use_graph=False)
+    assert a.cfg.grid_res() == G
+    a.initialize()
+    b.initialize()
+    for _ in range(4):
+        a.step()
+        b.step_profiled()
+    torch.cuda.synchronize()
+    for key in ("pos", "rad", "fsc", "cell_indices", "local_max_depth"):
+        assert torch.equal(getattr(a, key), getattr(b, key)), key
+    assert a.counters() == b.counters()
+    assert a.ctx.device_error() == 0
