@@ -184,3 +184,33 @@ def test_cooperative_frame_on_coarse_grids(r_max, G):
         assert torch.equal(getattr(a, key), getattr(b, key)), key
     assert a.counters() == b.counters()
     assert a.ctx.device_error() == 0
+
+
+def test_dynamics_trace_and_span():
+    """fos_frame_trace: block 0's stamps after every phase, in order, inside the
+    kernel's span (earliest block start .. latest block end); the frame counter
+    does not move; cap < 3 is an argument error."""
+    import ctypes as C
+    from fos import _lib
+    from fos._lib import call
+    from fos.context import stream
+    s = FoamSim.from_foam(inputs.small())
+    s.initialize()
+    s.run(3)
+    before = s.counters()
+    cap = 64
+    buf = (C.c_longlong * cap)()
+    cnt = C.c_int()
+    call("fos_frame_trace", s.ctx.h, C.byref(s.state), C.byref(s.fp), buf, cap, C.byref(cnt),
+         stream())
+    t = [buf[i] for i in range(cnt.value)]
+    assert 8 <= len(t) <= cap - 2
+    assert all(b >= a for a, b in zip(t, t[1:]))
+    start = (~buf[cap - 2]) & 0xFFFFFFFFFFFFFFFF
+    end = buf[cap - 1]
+    assert start <= t[0] and t[-1] <= end
+    assert 0 < end - start < 50_000_000  # ns
+    assert s.counters() == before
+    with pytest.raises(_lib.FosError):
+        call("fos_frame_trace", s.ctx.h, C.byref(s.state), C.byref(s.fp), buf, 2, C.byref(cnt),
+             stream())
