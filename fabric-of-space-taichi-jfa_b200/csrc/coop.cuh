@@ -9,7 +9,13 @@
 
 #include "phases.cuh"
 
+// block size and resident blocks per SM of the single-foam cooperative kernel
+#ifndef COOP_THREADS
 #define COOP_THREADS 1024
+#endif
+#ifndef COOP_BLOCKS_PER_SM
+#define COOP_BLOCKS_PER_SM 1
+#endif
 #define COOP_SMALL_G3 12288  // cell tables up to this size are scanned per block in smem
 
 struct UniGeo {

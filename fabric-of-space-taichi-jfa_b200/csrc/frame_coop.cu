@@ -165,7 +165,7 @@ __device__ __forceinline__ bool coop_layout(const CoopArgs& a, const UniGeo& geo
     return coop_csr(a, geo, cnt, a.pos, a.rad, false, tk, ep);
 }
 
-__global__ void __launch_bounds__(COOP_THREADS) k_frame_coop(CoopArgs a) {
+__global__ void __launch_bounds__(COOP_THREADS, COOP_BLOCKS_PER_SM) k_frame_coop(CoopArgs a) {
     const int T = gridDim.x * blockDim.x;
     const int tid = blockIdx.x * blockDim.x + threadIdx.x;
     const int lane = threadIdx.x & 31;
@@ -460,7 +460,7 @@ static int coop_grid_size(FosCtx* c) {
     if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_frame_coop, COOP_THREADS,
                                                       (COOP_SMALL_G3 + 1) * 4) != cudaSuccess)
         return -1;
-    if (per_sm > 1) per_sm = 1;  // one full block per SM: fewest barrier arrivals
+    if (per_sm > COOP_BLOCKS_PER_SM) per_sm = COOP_BLOCKS_PER_SM;  // fewest barrier arrivals
     int blocks = per_sm * c->num_sms;
     if (blocks > 1024) blocks = 1024;
     c->coop_blocks = blocks;
