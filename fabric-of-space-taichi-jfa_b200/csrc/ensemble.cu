@@ -204,10 +204,16 @@ __global__ void __launch_bounds__(512) k_ens_faces(const long long* __restrict__
                                                    unsigned long long* keys, unsigned int* hmin,
                                                    unsigned int* hcnt, unsigned int* claimed,
                                                    FosDevState* ds, unsigned long long mask) {
+    __shared__ unsigned int s_slot[3 * 512];
+    __shared__ int s_n;
+    if (threadIdx.x == 0) s_n = 0;
+    __syncthreads();
+    const ClaimBuf cb{s_slot, &s_n, claimed};
     const long long v0 = (long long)blockIdx.x * blockDim.x;
     const EnsFoamDev d = F[ens_vox_foam(vo, nf, v0)];
-    faces_body(filt + d.vox_off, d.R, ntot, keys, hmin, hcnt, claimed, ds, mask,
+    faces_body(filt + d.vox_off, d.R, ntot, keys, hmin, hcnt, cb, ds, mask,
                v0 + threadIdx.x - d.vox_off);
+    faces_claims_flush(cb, claimed, ds);
 }
 
 __global__ void k_ens_scores(int ntot, const EnsFoamDev* __restrict__ F,

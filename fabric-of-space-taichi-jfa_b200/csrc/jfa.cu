@@ -129,7 +129,8 @@ __global__ void __launch_bounds__(256) k_faces(const int32_t* __restrict__ filt,
                                                unsigned long long* keys, unsigned int* hmin,
                                                unsigned int* hcnt, unsigned int* claimed,
                                                FosDevState* ds, unsigned long long mask) {
-    faces_body(filt, R, n, keys, hmin, hcnt, claimed, ds, mask,
+    const ClaimBuf cb{nullptr, nullptr, claimed};
+    faces_body(filt, R, n, keys, hmin, hcnt, cb, ds, mask,
                (long long)blockIdx.x * blockDim.x + threadIdx.x);
 }
 

@@ -208,6 +208,17 @@ __device__ __forceinline__ unsigned long long fmix64(unsigned long long k) {
     return k;
 }
 
+// Where a claimed pair-table slot goes.  slot != NULL: gathered in shared
+// memory and appended to the table's claimed list with one atomic per block
+// (faces_claims_flush) -- with millions of pairs (the ensembles) one counter
+// shared by every claim serialises; slot == NULL: appended directly (cheaper
+// at one foam's tens of thousands of pairs).
+struct ClaimBuf {
+    unsigned int* slot;  // >= 3 * blockDim.x entries, or NULL
+    int* n;
+    unsigned int* claimed;
+};
+
 // Insert (or find) pair key pk in the open-addressed table and add its
 // count c and first-touch key fk.  h is the pair's home slot and k the key
 // already loaded from it (the caller issues the first probes of a warp's
@@ -216,15 +227,15 @@ __device__ __forceinline__ void pair_insert_at(unsigned long long pk, unsigned i
                                                unsigned int c, unsigned long long h,
                                                unsigned long long k, unsigned long long* keys,
                                                unsigned int* hmin, unsigned int* hcnt,
-                                               unsigned int* claimed, FosDevState* ds,
+                                               const ClaimBuf& cb, FosDevState* ds,
                                                unsigned long long mask) {
     for (unsigned long long probe = 0; probe <= mask; ++probe) {
         bool hit = (k == pk);
         if (!hit && k == EMPTY_KEY) {
             unsigned long long prev = atomicCAS(&keys[h], EMPTY_KEY, pk);
             if (prev == EMPTY_KEY) {
-                int idx = atomicAdd(&ds->pair_count, 1);
-                claimed[idx] = (unsigned int)h;
+                if (cb.slot) cb.slot[atomicAdd(cb.n, 1)] = (unsigned int)h;
+                else cb.claimed[atomicAdd(&ds->pair_count, 1)] = (unsigned int)h;
                 hit = true;
             } else {
                 hit = (prev == pk);
@@ -250,7 +261,7 @@ __device__ __forceinline__ void pair_insert_at(unsigned long long pk, unsigned i
 // the pair's count and minimum first-touch key.
 __device__ __forceinline__ void faces_body(const int32_t* __restrict__ filt, int R, int n,
                                            unsigned long long* keys, unsigned int* hmin,
-                                           unsigned int* hcnt, unsigned int* claimed,
+                                           unsigned int* hcnt, const ClaimBuf& cb,
                                            FosDevState* ds, unsigned long long mask,
                                            long long lin) {
     const int V = R * R * R;
@@ -305,8 +316,21 @@ __device__ __forceinline__ void faces_body(const int32_t* __restrict__ filt, int
 #pragma unroll
     for (int ax = 0; ax < 3; ++ax)
         if (lead[ax])
-            pair_insert_at(pk[ax], mn[ax], cntv[ax], h[ax], k[ax], keys, hmin, hcnt, claimed, ds,
+            pair_insert_at(pk[ax], mn[ax], cntv[ax], h[ax], k[ax], keys, hmin, hcnt, cb, ds,
                            mask);
+}
+
+// A faces kernel block's gathered claims (cb.slot != NULL): call with every
+// thread of the block after faces_body; cb.n was zeroed (and synchronised)
+// before it.
+__device__ __forceinline__ void faces_claims_flush(const ClaimBuf& cb, unsigned int* claimed,
+                                                   FosDevState* ds) {
+    __shared__ int s_base;
+    __syncthreads();
+    const int m = *cb.n;
+    if (threadIdx.x == 0) s_base = m ? atomicAdd(&ds->pair_count, m) : 0;
+    __syncthreads();
+    for (int t = threadIdx.x; t < m; t += blockDim.x) claimed[s_base + t] = cb.slot[t];
 }
 
 // Per face slot t = a*32 + s: the normalised score of finalize_faces_kernel
