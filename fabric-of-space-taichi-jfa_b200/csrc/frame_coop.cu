@@ -237,10 +237,6 @@ __global__ void __launch_bounds__(COOP_THREADS, COOP_BLOCKS_PER_SM) k_frame_coop
     const float bg = back_global_from_bits(fv[1], a.contact_tol_d);
     PressureArgs pa = a.pa;
     pa.frame = (int)fv[2];
-    // four consecutive particles per warp (one sector of each per-particle
-    // array), consecutive warps of particles on consecutive blocks
-    const int i_one =
-        (int)((((threadIdx.x >> 5) * gridDim.x + blockIdx.x) << 2) + ((threadIdx.x >> 3) & 3));
     if (a.ptag) {
         // (3) + (4) without grid barriers (n * COOP_PLANES <= T,
         // 1 <= sweeps <= FOS_PTAG_SWEEPS): each group of COOP_PLANES lanes
@@ -325,6 +321,10 @@ __global__ void __launch_bounds__(COOP_THREADS, COOP_BLOCKS_PER_SM) k_frame_coop
     // for all sweeps, and the particles are spread over every block, so every
     // SM issues the same share of the sweep
     const bool keep_nbr = p_rounds == 1;
+    // four consecutive particles per warp (one sector of each per-particle
+    // array), consecutive warps of particles on consecutive blocks
+    const int i_one =
+        (int)((((threadIdx.x >> 5) * gridDim.x + blockIdx.x) << 2) + ((threadIdx.x >> 3) & 3));
     const PressureNbr nb0 = pressure_nbr8x2<LdL2>(i_one, lane, pa);
     for (int w = 0; w < a.sweeps; ++w) {
         const float* rin = (w & 1) ? a.rad_tmp : a.rad;
