@@ -410,9 +410,10 @@ __device__ __forceinline__ unsigned int maxov_warp(int kk, int lane, const float
     for (int base = 0; base < r.total; base += 32) {
         int t = base + lane;
         int k = stencil_locate(r, t < r.total ? t : r.total - 1);
-        if (t < r.total) {
-            int j = LD::ld(&ci[k]);
-            if (i < j) lm = fmaxf(lm, maxov_term(LD::ld(&sp[k]), me, eps, g));
+        if (t < r.total) {  // both loads before the test: one round trip
+            const int j = LD::ld(&ci[k]);
+            const float4 q = LD::ld(&sp[k]);
+            if (i < j) lm = fmaxf(lm, maxov_term(q, me, eps, g));
         }
     }
     unsigned int b = __reduce_max_sync(0xffffffffu, __float_as_uint(lm));
