@@ -129,9 +129,14 @@ __global__ void __launch_bounds__(256) k_faces(const int32_t* __restrict__ filt,
                                                unsigned long long* keys, unsigned int* hmin,
                                                unsigned int* hcnt, unsigned int* claimed,
                                                FosDevState* ds, unsigned long long mask) {
-    const ClaimBuf cb{nullptr, nullptr, claimed};
+    __shared__ unsigned int s_slot[3 * 256];
+    __shared__ int s_n;
+    if (threadIdx.x == 0) s_n = 0;
+    __syncthreads();
+    const ClaimBuf cb{s_slot, &s_n, claimed};
     faces_body(filt, R, n, keys, hmin, hcnt, cb, ds, mask,
                (long long)blockIdx.x * blockDim.x + threadIdx.x);
+    faces_claims_flush(cb, claimed, ds);
 }
 
 // Moves every claimed pair into its lower particle's candidate row and resets

@@ -208,13 +208,13 @@ __device__ __forceinline__ unsigned long long fmix64(unsigned long long k) {
     return k;
 }
 
-// Where a claimed pair-table slot goes.  slot != NULL: gathered in shared
-// memory and appended to the table's claimed list with one atomic per block
-// (faces_claims_flush) -- with millions of pairs (the ensembles) one counter
-// shared by every claim serialises; slot == NULL: appended directly (cheaper
-// at one foam's tens of thousands of pairs).
+// Where a claimed pair-table slot goes: gathered in shared memory and appended
+// to the table's claimed list with one atomic per block (faces_claims_flush).
+// One counter shared by every claim serialises in L2: at 200,000 particles
+// (1.4 M pairs) the face kernel took 1.73 ms with an atomic per claim and
+// 0.99 ms with one per block.
 struct ClaimBuf {
-    unsigned int* slot;  // >= 3 * blockDim.x entries, or NULL
+    unsigned int* slot;  // >= 3 * blockDim.x entries
     int* n;
     unsigned int* claimed;
 };
@@ -234,8 +234,7 @@ __device__ __forceinline__ void pair_insert_at(unsigned long long pk, unsigned i
         if (!hit && k == EMPTY_KEY) {
             unsigned long long prev = atomicCAS(&keys[h], EMPTY_KEY, pk);
             if (prev == EMPTY_KEY) {
-                if (cb.slot) cb.slot[atomicAdd(cb.n, 1)] = (unsigned int)h;
-                else cb.claimed[atomicAdd(&ds->pair_count, 1)] = (unsigned int)h;
+                cb.slot[atomicAdd(cb.n, 1)] = (unsigned int)h;
                 hit = true;
             } else {
                 hit = (prev == pk);
@@ -259,6 +258,13 @@ __device__ __forceinline__ void pair_insert_at(unsigned long long pk, unsigned i
 // (that voxel's linear index)*6 + axis*2 + (dir == +1).  Lanes of a warp that
 // hit the same pair are merged (__match_any_sync) before one atomic update of
 // the pair's count and minimum first-touch key.
+//
+// Element lin is a thread slot, not a voxel: when R is a multiple of 8 each
+// warp (32 consecutive slots) takes a 2 (x) x 2 (y) x 8 (z) voxel tile, whose
+// four z-rows are whole 32-byte sectors.  A tile meets fewer distinct pairs
+// per axis than a 32-voxel z-run (cells are a few voxels across), so fewer
+// merged groups reach the table.  The count and the minimum key of a pair do
+// not depend on which thread visits which face, so the result is the same.
 __device__ __forceinline__ void faces_body(const int32_t* __restrict__ filt, int R, int n,
                                            unsigned long long* keys, unsigned int* hmin,
                                            unsigned int* hcnt, const ClaimBuf& cb,
@@ -266,21 +272,29 @@ __device__ __forceinline__ void faces_body(const int32_t* __restrict__ filt, int
                                            long long lin) {
     const int V = R * R * R;
     bool live = lin < V;
-    const int l = live ? (int)lin : 0;
+    const int s = live ? (int)lin : 0;
     int lane = threadIdx.x & 31;
-    int a = live ? filt[l] : -1;
-    bool va = a >= 0 && a < n;
-    int z = 0, y = 0, x = 0;
-    if (live) vox_xyz(l, R, x, y, z);
-    // the three neighbour labels first, so their loads are in flight together
-    int nlin[3] = {0, 0, 0}, b[3];
-    if (live) {
-        nlin[0] = (wrap_small(x + 1, R) * R + y) * R + z;
-        nlin[1] = (x * R + wrap_small(y + 1, R)) * R + z;
-        nlin[2] = (x * R + y) * R + wrap_small(z + 1, R);
+    int z, y, x;
+    if ((R & 7) == 0) {  // V is then a multiple of 32: whole tiles only
+        const int w = s >> 5, tz = R >> 3, ty = R >> 1;
+        const int t = w / tz;
+        z = ((w - t * tz) << 3) + (s & 7);
+        y = ((t % ty) << 1) + ((s >> 3) & 1);
+        x = ((t / ty) << 1) + ((s >> 4) & 1);
+    } else {
+        vox_xyz(s, R, x, y, z);
     }
+    const int l = (x * R + y) * R + z;
+    // the voxel's label and its three +1 neighbours' labels are loaded
+    // together (every index is in range, live or not)
+    int nlin[3], b[3];
+    nlin[0] = (wrap_small(x + 1, R) * R + y) * R + z;
+    nlin[1] = (x * R + wrap_small(y + 1, R)) * R + z;
+    nlin[2] = (x * R + y) * R + wrap_small(z + 1, R);
+    const int a = live ? filt[l] : -1;
 #pragma unroll
-    for (int ax = 0; ax < 3; ++ax) b[ax] = va ? filt[nlin[ax]] : -1;
+    for (int ax = 0; ax < 3; ++ax) b[ax] = filt[nlin[ax]];
+    bool va = a >= 0 && a < n;
     unsigned long long pk[3];
     unsigned int mn[3], cntv[3];
     bool lead[3];
@@ -320,9 +334,8 @@ __device__ __forceinline__ void faces_body(const int32_t* __restrict__ filt, int
                            mask);
 }
 
-// A faces kernel block's gathered claims (cb.slot != NULL): call with every
-// thread of the block after faces_body; cb.n was zeroed (and synchronised)
-// before it.
+// A faces kernel block's gathered claims: call with every thread of the block
+// after faces_body; cb.n was zeroed (and synchronised) before it.
 __device__ __forceinline__ void faces_claims_flush(const ClaimBuf& cb, unsigned int* claimed,
                                                    FosDevState* ds) {
     __shared__ int s_base;
