@@ -151,10 +151,13 @@ def test_coincident_seeds_tie_to_lowest_index():
     assert np.array_equal(ctx.labels().cpu().numpy().reshape(-1), full)
 
 
-def test_stage_by_stage_with_loaded_labels():
-    """FSC stages on a given owner grid (stripes + noise) match the oracle."""
+@pytest.mark.parametrize("R", [32, 27, 20])
+def test_stage_by_stage_with_loaded_labels(R):
+    """FSC stages on a given owner grid (stripes + noise) match the oracle; R a
+    multiple of 8 takes the face kernel's 2x2x8 warp tiles, 27 and 20 its
+    linear voxel order."""
     rng = np.random.default_rng(2)
-    R, n = 32, 40
+    n = 40
     lab = rng.integers(-1, n, (R, R, R)).astype(np.int32)
     lab[:, :, :16] = rng.integers(0, 5, (R, R, 16))
     lab = lab.reshape(-1)
