@@ -60,6 +60,13 @@ __global__ void __launch_bounds__(256) k_jfa_pass(const int32_t* __restrict__ in
                                                   float vs, float halfL, float L, int step,
                                                   FosDevState* ds, int pass, int early_exit,
                                                   int min_passes, double th) {
+    // Programmatic dependent launch (passes after the first): the next pass's
+    // blocks may be scheduled once every block of this one has started, and
+    // each block waits here until the previous pass has completed and its
+    // labels and change counts are visible.  Without the launch attribute both
+    // instructions return at once.
+    asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
+    asm volatile("griddepcontrol.wait;" ::: "memory");
     const long long V = (long long)R * R * R;
     if (early_exit && jfa_exited_before(ds, pass, (double)V, min_passes, th)) return;
     jfa_pass_body<UNIT_L, POW2, TIE_LOWER>(in, out, seeds, R, lgR, vs, halfL, L, step, ds->changes,
@@ -479,13 +486,23 @@ extern "C" int fos_jfa_init(FosCtx* c, const float* pos, const float* rad, int n
 }
 
 template <bool UL, bool P2, bool TIE>
-static void launch_pass(FosCtx* c, const int32_t* in, int32_t* out, int step, int pass,
-                        int early_exit, cudaStream_t s) {
+static cudaError_t launch_pass(FosCtx* c, const int32_t* in, int32_t* out, int step,
+                               int pass, int early_exit, cudaStream_t s) {
     const int R = c->res;
     long long V = (long long)R * R * R;
-    k_jfa_pass<UL, P2, TIE><<<fos_blocks(V, 256), 256, 0, s>>>(
-        in, out, c->seeds, R, ilog2(R), c->vs, c->halfL, c->L, step, c->ds, pass, early_exit,
-        c->p.min_jfa_passes, c->p.th_pass_delta);
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3((unsigned)fos_blocks(V, 256));
+    cfg.blockDim = dim3(256);
+    cfg.stream = s;
+    // a pass that follows a pass overlaps its launch with that pass's tail
+    cudaLaunchAttribute at[1];
+    at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    at[0].val.programmaticStreamSerializationAllowed = 1;
+    cfg.attrs = at;
+    cfg.numAttrs = pass > 0 ? 1 : 0;
+    return cudaLaunchKernelEx(&cfg, k_jfa_pass<UL, P2, TIE>, in, out, (const float4*)c->seeds,
+                              R, ilog2(R), c->vs, c->halfL, c->L, step, c->ds, pass,
+                              early_exit, c->p.min_jfa_passes, c->p.th_pass_delta);
 }
 
 // `npass` passes from labA, steps first_step, first_step/2, ... (never below 1).
@@ -500,14 +517,16 @@ static int run_passes(FosCtx* c, int first_step, int npass, int early_exit, cuda
         const int32_t* in = (p & 1) ? c->labB : c->labA;
         int32_t* out = (p & 1) ? c->labA : c->labB;
         const int ee = early_exit;
-        if (ul && p2 && !tie) launch_pass<true, true, false>(c, in, out, step, p, ee, s);
-        else if (ul && p2 && tie) launch_pass<true, true, true>(c, in, out, step, p, ee, s);
-        else if (ul && !p2 && !tie) launch_pass<true, false, false>(c, in, out, step, p, ee, s);
-        else if (ul && !p2 && tie) launch_pass<true, false, true>(c, in, out, step, p, ee, s);
-        else if (!ul && p2 && !tie) launch_pass<false, true, false>(c, in, out, step, p, ee, s);
-        else if (!ul && p2 && tie) launch_pass<false, true, true>(c, in, out, step, p, ee, s);
-        else if (!ul && !p2 && !tie) launch_pass<false, false, false>(c, in, out, step, p, ee, s);
-        else launch_pass<false, false, true>(c, in, out, step, p, ee, s);
+        cudaError_t le;
+        if (ul && p2 && !tie) le = launch_pass<true, true, false>(c, in, out, step, p, ee, s);
+        else if (ul && p2 && tie) le = launch_pass<true, true, true>(c, in, out, step, p, ee, s);
+        else if (ul && !p2 && !tie) le = launch_pass<true, false, false>(c, in, out, step, p, ee, s);
+        else if (ul && !p2 && tie) le = launch_pass<true, false, true>(c, in, out, step, p, ee, s);
+        else if (!ul && p2 && !tie) le = launch_pass<false, true, false>(c, in, out, step, p, ee, s);
+        else if (!ul && p2 && tie) le = launch_pass<false, true, true>(c, in, out, step, p, ee, s);
+        else if (!ul && !p2 && !tie) le = launch_pass<false, false, false>(c, in, out, step, p, ee, s);
+        else le = launch_pass<false, false, true>(c, in, out, step, p, ee, s);
+        if (le != cudaSuccess) return fos_cuda_fail(le, "kernel launch", __FILE__, __LINE__);
         FOS_LAUNCHED(c);
         step /= 2;
     }
