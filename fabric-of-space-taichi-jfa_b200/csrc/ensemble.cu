@@ -870,7 +870,7 @@ static int ens_filter_faces(FosEnsemble* e, cudaStream_t s) {
     k_ens_faces<<<vgrid, vb, 0, s>>>(e->dvo, e->nf, e->df, e->filt, n, c->hkeys, c->hmin, c->hcnt,
                                      c->claimed, c->ds, (unsigned long long)(c->H - 1));
     FOS_LAUNCHED(c);
-    k_compact<<<c->num_sms * 4, 256, 0, s>>>(c->hkeys, c->hmin, c->hcnt, c->claimed, c->ds,
+    k_compact<<<c->num_sms * 8, 256, 0, s>>>(c->hkeys, c->hmin, c->hcnt, c->claimed, c->ds,
                                              c->rowcnt, c->rowbuf);
     FOS_LAUNCHED(c);
     return FOS_OK;

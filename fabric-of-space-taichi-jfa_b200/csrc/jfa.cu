@@ -147,7 +147,10 @@ __global__ void __launch_bounds__(256) k_faces(const int32_t* __restrict__ filt,
 }
 
 // Moves every claimed pair into its lower particle's candidate row and resets
-// the table slot for the next run.
+// the table slot for the next run.  Launched with 8 blocks of 256 per SM (the
+// full 2,048 threads at 32 registers): each pair is a chain of dependent
+// loads and a returning atomic, so the number of chains in flight sets the
+// time at a million pairs.
 __global__ void k_compact(unsigned long long* keys, unsigned int* hmin, unsigned int* hcnt,
                           const unsigned int* __restrict__ claimed, FosDevState* ds,
                           int32_t* rowcnt, uint4* rowbuf) {
@@ -609,7 +612,7 @@ extern "C" int fos_jfa_accumulate_faces(FosCtx* c, int n, fos_stream_t s) {
     k_faces<<<fos_blocks(V, 256), 256, 0, s>>>(c->filt, c->res, n, c->hkeys, c->hmin, c->hcnt,
                                                c->claimed, c->ds, (unsigned long long)(c->H - 1));
     FOS_LAUNCHED(c);
-    k_compact<<<c->num_sms * 4, 256, 0, s>>>(c->hkeys, c->hmin, c->hcnt, c->claimed, c->ds,
+    k_compact<<<c->num_sms * 8, 256, 0, s>>>(c->hkeys, c->hmin, c->hcnt, c->claimed, c->ds,
                                              c->rowcnt, c->rowbuf);
     FOS_LAUNCHED(c);
     k_rows<<<fos_blocks(32LL * n, 256), 256, 0, s>>>(n, c->rowcnt, c->rowbuf, c->face_ids,
