@@ -132,11 +132,17 @@ __global__ void __launch_bounds__(256) k_majority(const int32_t* __restrict__ la
                   (long long)blockIdx.x * blockDim.x + threadIdx.x);
 }
 
-__global__ void __launch_bounds__(256) k_faces(const int32_t* __restrict__ filt, int R, int n,
+// Threads per face-extraction block: a block appends its claimed table slots
+// once, after a block barrier, so smaller blocks wait on fewer warps.
+#ifndef FACES_THREADS
+#define FACES_THREADS 128
+#endif
+
+__global__ void __launch_bounds__(FACES_THREADS) k_faces(const int32_t* __restrict__ filt, int R, int n,
                                                unsigned long long* keys, unsigned int* hmin,
                                                unsigned int* hcnt, unsigned int* claimed,
                                                FosDevState* ds, unsigned long long mask) {
-    __shared__ unsigned int s_slot[3 * 256];
+    __shared__ unsigned int s_slot[3 * FACES_THREADS];
     __shared__ int s_n;
     if (threadIdx.x == 0) s_n = 0;
     __syncthreads();
@@ -609,7 +615,7 @@ extern "C" int fos_jfa_accumulate_faces(FosCtx* c, int n, fos_stream_t s) {
     long long V = (long long)c->res * c->res * c->res;
     k_faces_reset<<<fos_blocks(n, 256), 256, 0, s>>>(c->ds, c->rowcnt, n);
     FOS_LAUNCHED(c);
-    k_faces<<<fos_blocks(V, 256), 256, 0, s>>>(c->filt, c->res, n, c->hkeys, c->hmin, c->hcnt,
+    k_faces<<<fos_blocks(V, FACES_THREADS), FACES_THREADS, 0, s>>>(c->filt, c->res, n, c->hkeys, c->hmin, c->hcnt,
                                                c->claimed, c->ds, (unsigned long long)(c->H - 1));
     FOS_LAUNCHED(c);
     k_compact<<<c->num_sms * 8, 256, 0, s>>>(c->hkeys, c->hmin, c->hcnt, c->claimed, c->ds,
