@@ -44,10 +44,15 @@ static __device__ __align__(256) int32_t g_noalloc_scratch[2 * FOS_NOALLOC_MAX_P
 
 #define FOS_NOALLOC_MAX_DEVICES 64
 
-// Device address of g_noalloc_scratch, resolved once per device.  In host code
-// the symbol's name is only a host-side handle, never a device address, so it
-// must go through cudaGetSymbolAddress with the right device current.
-static int32_t* scratch_for_current_device(int* rc_out) {
+// Device address of g_noalloc_scratch on the current device.  In host code the
+// symbol's name is only a host-side handle, never a device address, so it must
+// go through cudaGetSymbolAddress with the right device current.  Outside
+// stream capture the address is looked up on every call (no allocation, no
+// synchronisation), so a device reset or a reloaded module never leaves a stale
+// pointer behind.  During capture the lookup is not made: the address cached
+// by an earlier call on this device is used, and with none cached the call
+// fails with FOS_E_ARG before anything is launched.
+static int32_t* scratch_for_current_device(fos_stream_t s, int* rc_out) {
     static std::mutex mu;
     static int32_t* addr[FOS_NOALLOC_MAX_DEVICES] = {nullptr};
     int dev = -1;
@@ -60,8 +65,14 @@ static int32_t* scratch_for_current_device(int* rc_out) {
         *rc_out = fos_fail(FOS_E_ARG, "device index above the supported range");
         return nullptr;
     }
+    cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
+    e = cudaStreamIsCapturing(s, &cap);
+    if (e != cudaSuccess) {
+        *rc_out = fos_cuda_fail(e, "cudaStreamIsCapturing", __FILE__, __LINE__);
+        return nullptr;
+    }
     std::lock_guard<std::mutex> lock(mu);
-    if (!addr[dev]) {
+    if (cap == cudaStreamCaptureStatusNone) {
         void* p = nullptr;
         e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
         if (e != cudaSuccess || p == nullptr) {
@@ -70,6 +81,11 @@ static int32_t* scratch_for_current_device(int* rc_out) {
             return nullptr;
         }
         addr[dev] = (int32_t*)p;
+    } else if (!addr[dev]) {
+        *rc_out = fos_fail(FOS_E_ARG,
+                           "fos_grid_build_noalloc: the first call on a device must come before "
+                           "any stream capture (it looks up the scratch array's address)");
+        return nullptr;
     }
     *rc_out = FOS_OK;
     return addr[dev];
@@ -81,12 +97,13 @@ extern "C" int fos_grid_build_noalloc(float* pos, int n, int grid_res, double do
     FOS_REQUIRE(n >= 0, FOS_E_ARG, "n must be >= 0");
     FOS_REQUIRE(n <= FOS_NOALLOC_MAX_PARTICLES, FOS_E_CAPACITY,
                 "n exceeds FOS_NOALLOC_MAX_PARTICLES (65536): use a context and fos_grid_build");
-    FOS_REQUIRE(grid_res >= 3 && grid_res <= 1024, FOS_E_ARG, "grid_res must be in [3, 1024]");
+    FOS_REQUIRE(grid_res >= 3 && grid_res <= FOS_NOALLOC_MAX_GRID_RES, FOS_E_ARG,
+                "grid_res must be in [3, 256]");
     FOS_REQUIRE(domain_size > 0.0, FOS_E_ARG, "domain_size must be > 0");
     FOS_REQUIRE(cell_count && cell_start && cell_indices && (n == 0 || pos), FOS_E_ARG,
                 "NULL argument");
     int rc = FOS_OK;
-    int32_t* scratch = scratch_for_current_device(&rc);
+    int32_t* scratch = scratch_for_current_device(s, &rc);
     if (!scratch) return rc;
     int32_t* cellof = scratch;
     int32_t* rank = scratch + FOS_NOALLOC_MAX_PARTICLES;
@@ -103,7 +120,8 @@ extern "C" int fos_grid_build_noalloc(float* pos, int n, int grid_res, double do
                                                         cellof, rank);
         FOS_CUDA(cudaPeekAtLastError());
     }
-    // single-block scan: it needs no block-sum scratch for any table size
+    // single-block scan: it needs no block-sum scratch, and its time grows with
+    // grid_res^3 (about a millisecond at 128, tens of milliseconds at 256)
     k_scan_single<<<1, 1024, 0, s>>>(cell_count, cell_start, G3, 0);
     FOS_CUDA(cudaPeekAtLastError());
     if (n == 0) return FOS_OK;

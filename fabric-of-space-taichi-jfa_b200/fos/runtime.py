@@ -17,7 +17,7 @@ def configure(cfg: FosConfig):
     """Replace the module configuration (the reference's config.py globals)."""
     global _cfg
     _cfg = cfg
-    if _ctx is not None:
+    if _ctx is not None and getattr(_ctx, "h", None):
         _ctx.set_params(cfg)
 
 
@@ -31,6 +31,7 @@ def init(max_particles: int | None = None, max_res: int | None = None):
     from .context import Context
     if _ctx is not None:
         _ctx.close()
+        _ctx = None  # a failed create below leaves no closed context installed
     _ctx = Context(_cfg, max_n=max_particles or _cfg.MAX_PARTICLES,
                    max_res=max_res or max(_cfg.JFA_RES_MAX, _cfg.JFA_RES))
     return _ctx

@@ -174,14 +174,19 @@ int fos_grid_build(FosCtx* ctx, float* pos, int n, int32_t* cell_count, int32_t*
  * a static device array compiled into the library: 512 KiB on every GPU that
  * loads it, held until the process exits.  That caps n at
  * FOS_NOALLOC_MAX_PARTICLES; a larger n returns FOS_E_CAPACITY and launches
- * nothing.  The first call on each device resolves the array's device address
- * (cudaGetSymbolAddress), so make that first call before any stream capture.
+ * nothing.  Outside stream capture every call looks up the array's device
+ * address (cudaGetSymbolAddress: no allocation, no synchronisation), so a
+ * device reset between calls is harmless.  During capture the address of an
+ * earlier call on the same device is reused; a first call on a device made
+ * during capture returns FOS_E_ARG, so make one call before capturing.
  * All calls share the one array: calls that overlap on the GPU (other streams,
  * other host threads) race and must be serialised.  Outputs equal
  * fos_grid_build's: cell_count and cell_start [grid_res^3], cell_indices
- * ascending inside each cell, pos wrapped in place.  grid_res and domain_size
- * are GRID_RES and DOMAIN_SIZE. */
+ * ascending inside each cell, pos wrapped in place.  grid_res (GRID_RES, at most
+ * FOS_NOALLOC_MAX_GRID_RES: the cell-count scan runs in one thread block) and
+ * domain_size (DOMAIN_SIZE) are the grid's. */
 #define FOS_NOALLOC_MAX_PARTICLES 65536
+#define FOS_NOALLOC_MAX_GRID_RES 256
 int fos_grid_build_noalloc(float* pos, int n, int grid_res, double domain_size,
                            int32_t* cell_count, int32_t* cell_start, int32_t* cell_indices,
                            fos_stream_t s);

@@ -34,7 +34,8 @@ def load(name):
 
 
 def setup(max_n: int, max_res: int = 32, **cfg):
-    runtime.configure(FosConfig(JFA_RES_MIN=8, JFA_RES_MAX=max_res, MAX_PARTICLES=max_n, **cfg))
+    runtime.configure(FosConfig(JFA_RES=max_res, JFA_RES_MIN=8, JFA_RES_MAX=max_res,
+                                MAX_PARTICLES=max_n, **cfg))
     from fos import jfa
     jfa.init_jfa(max_particles=max_n, max_res=max_res)
     return jfa

@@ -78,3 +78,40 @@ def test_noalloc_rejects_more_than_its_capacity():
     assert b"FOS_NOALLOC_MAX_PARTICLES" in _lib.load().fos_last_error()
     torch.cuda.synchronize()
     assert int((cc == -7).sum()) == G ** 3  # nothing was launched
+
+
+@pytest.mark.parametrize("n", [0, MAX_N])
+def test_noalloc_edge_sizes_match_context_build(n):
+    """n = 0 (only the histogram clear and the scan run) and n at the cap (the
+    last scratch entry of the cell half and the first of the rank half), on a
+    17^3 grid, against the context build on the same positions."""
+    G = 17
+    G3 = G ** 3
+    cfg = FosConfig(DOMAIN_SIZE=1.0, GRID_RES=G, JFA_RES=32)
+    ctx = Context(cfg, max_n=max(n, 1), max_res=32)
+    rng = np.random.default_rng(n + 5)
+    pos_np = rng.uniform(-0.7, 0.7, (max(n, 1), 3)).astype(np.float32)
+    a = torch.as_tensor(pos_np).cuda()
+    b = a.clone()
+    ra, rb = _outputs(G3, n), _outputs(G3, n)
+    ctx.grid_build(a, n, *ra)
+    rc = _noalloc(b, n, G, 1.0, *rb)
+    assert rc == 0, _lib.load().fos_last_error()
+    torch.cuda.synchronize()
+    assert torch.equal(ra[0], rb[0]) and torch.equal(ra[1], rb[1])
+    assert torch.equal(ra[2][:n], rb[2][:n])
+    assert torch.equal(a, b)
+    assert int(rb[0].sum()) == n
+    if n == 0:
+        assert int(rb[0].abs().sum()) == 0 and int(rb[1].abs().sum()) == 0
+
+
+def test_noalloc_rejects_a_grid_above_its_cap():
+    G = 257
+    pos = torch.zeros((4, 3), dtype=torch.float32, device="cuda")
+    cc, cs, ci = _outputs(8, 4)
+    rc = _noalloc(pos, 4, G, 1.0, cc, cs, ci)
+    assert rc == 1  # FOS_E_ARG
+    assert b"grid_res" in _lib.load().fos_last_error()
+    torch.cuda.synchronize()
+    assert int((cc == -7).sum()) == 8  # nothing was launched
