@@ -174,6 +174,8 @@ extern "C" int fos_ctx_create(const FosParams* p, int max_n, int max_res, int de
     } while (0)
     ALLOC(c->labA, V * 4);
     ALLOC(c->labB, V * 4);
+    ALLOC(c->recA, V * sizeof(float4));
+    ALLOC(c->recB, V * sizeof(float4));
     ALLOC(c->filt, V * 4);
     ALLOC(c->seedslot, V * 8);
     ALLOC(c->seeds, (size_t)max_n * sizeof(float4));
@@ -268,7 +270,7 @@ extern "C" int fos_ctx_destroy(FosCtx* c) {
     for (int k = 0; k < FOS_GRAPH_SLOTS; ++k)
         if (c->gexec[k]) cudaGraphExecDestroy(c->gexec[k]);
     fos_sur_free(c);
-    void* ptrs[] = {c->labA, c->labB, c->filt, c->seedslot, c->seeds, c->fsc, c->used, c->ema,
+    void* ptrs[] = {c->labA, c->labB, c->recA, c->recB, c->filt, c->seedslot, c->seeds, c->fsc, c->used, c->ema,
                     c->face_ids, c->face_counts, c->nl, c->face_score, c->prev, c->acc0, c->acc1,
                     c->hkeys, c->hmin, c->hcnt, c->claimed, c->rowcnt, c->rowbuf, c->revcnt,
                     c->revstart, c->revfill, c->rev, c->scan_tmp, c->pos_tmp, c->rad_tmp,

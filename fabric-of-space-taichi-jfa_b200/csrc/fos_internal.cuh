@@ -87,6 +87,7 @@ struct FosCtx {
     int G = 3;
     // JFA fields
     int32_t *labA = nullptr, *labB = nullptr, *filt = nullptr;
+    float4 *recA = nullptr, *recB = nullptr;  // seed records mirroring labA / labB
     unsigned long long* seedslot = nullptr;
     float4* seeds = nullptr;
     int32_t *fsc = nullptr, *used = nullptr;

@@ -73,6 +73,38 @@ __global__ void __launch_bounds__(256) k_jfa_pass(const int32_t* __restrict__ in
                                            pass, (long long)blockIdx.x * blockDim.x + threadIdx.x);
 }
 
+// Pass over the record grid (jfa_pass_rec_body); the same launch protocol as
+// k_jfa_pass.
+template <bool UNIT_L, bool POW2>
+__global__ void __launch_bounds__(256) k_jfa_pass_rec(const int32_t* __restrict__ in,
+                                                      const float4* __restrict__ rin,
+                                                      int32_t* __restrict__ out,
+                                                      float4* __restrict__ rout, int R, int lgR,
+                                                      float vs, float halfL, float L, int step,
+                                                      FosDevState* ds, int pass, int early_exit,
+                                                      int min_passes, double th) {
+    asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
+    asm volatile("griddepcontrol.wait;" ::: "memory");
+    const long long V = (long long)R * R * R;
+    if (early_exit && jfa_exited_before(ds, pass, (double)V, min_passes, th)) return;
+    jfa_pass_rec_body<UNIT_L, POW2>(in, rin, out, rout, R, lgR, vs, halfL, L, step, ds->changes,
+                                    pass, (long long)blockIdx.x * blockDim.x + threadIdx.x);
+}
+
+// The record grid of a label grid: record v = seeds[label v], or NaN bits for
+// an unassigned voxel.  Run before every sequence of record passes, so a grid
+// from jfa_init, a warm start or loaded labels all start consistent with the
+// current seed table.
+__global__ void k_rec_from_labels(const int32_t* __restrict__ lab,
+                                  const float4* __restrict__ seeds, float4* __restrict__ rec,
+                                  long long V) {
+    for (long long l = (long long)blockIdx.x * blockDim.x + threadIdx.x; l < V;
+         l += (long long)gridDim.x * blockDim.x) {
+        const int v = lab[l];
+        rec[l] = v >= 0 ? __ldg(&seeds[v]) : rec_none();
+    }
+}
+
 __global__ void k_jfa_finish(FosDevState* ds, int passes, long long V, int early_exit,
                              int min_passes, double th) {
     int done = passes;
@@ -514,13 +546,59 @@ static cudaError_t launch_pass(FosCtx* c, const int32_t* in, int32_t* out, int s
                               early_exit, c->p.min_jfa_passes, c->p.th_pass_delta);
 }
 
+template <bool UL, bool P2>
+static cudaError_t launch_pass_rec(FosCtx* c, int p, int step, int early_exit, cudaStream_t s) {
+    const int R = c->res;
+    long long V = (long long)R * R * R;
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3((unsigned)fos_blocks(V, 256));
+    cfg.blockDim = dim3(256);
+    cfg.stream = s;
+    cudaLaunchAttribute at[1];
+    at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    at[0].val.programmaticStreamSerializationAllowed = 1;
+    cfg.attrs = at;
+    cfg.numAttrs = p > 0 ? 1 : 0;
+    const int32_t* in = (p & 1) ? c->labB : c->labA;
+    int32_t* out = (p & 1) ? c->labA : c->labB;
+    const float4* rin = (p & 1) ? c->recB : c->recA;
+    float4* rout = (p & 1) ? c->recA : c->recB;
+    return cudaLaunchKernelEx(&cfg, k_jfa_pass_rec<UL, P2>, in, rin, out, rout, R, ilog2(R),
+                              c->vs, c->halfL, c->L, step, c->ds, p, early_exit,
+                              c->p.min_jfa_passes, c->p.th_pass_delta);
+}
+
 // `npass` passes from labA, steps first_step, first_step/2, ... (never below 1).
+// The reference's scan-order tie rule runs over the record grid; the
+// lower-index tie rule (which compares labels on equal distances) runs over
+// labels and seed gathers.
 static int run_passes(FosCtx* c, int first_step, int npass, int early_exit, cudaStream_t s) {
     const int R = c->res;
     long long V = (long long)R * R * R;
     FOS_CUDA(cudaMemsetAsync(c->ds->changes, 0, sizeof(c->ds->changes), s));
     bool ul = (c->L == 1.0f), p2 = is_pow2(R), tie = c->p.tie_lower_index != 0;
     int step = first_step;
+    if (!tie) {
+        int blocks = fos_blocks(V, 256);
+        if (blocks > 8 * c->num_sms) blocks = 8 * c->num_sms;
+        k_rec_from_labels<<<blocks, 256, 0, s>>>(c->labA, c->seeds, c->recA, V);
+        FOS_LAUNCHED(c);
+        for (int p = 0; p < npass; ++p) {
+            if (step < 1) step = 1;
+            cudaError_t le;
+            if (ul && p2) le = launch_pass_rec<true, true>(c, p, step, early_exit, s);
+            else if (ul) le = launch_pass_rec<true, false>(c, p, step, early_exit, s);
+            else if (p2) le = launch_pass_rec<false, true>(c, p, step, early_exit, s);
+            else le = launch_pass_rec<false, false>(c, p, step, early_exit, s);
+            if (le != cudaSuccess) return fos_cuda_fail(le, "kernel launch", __FILE__, __LINE__);
+            FOS_LAUNCHED(c);
+            step /= 2;
+        }
+        k_jfa_finish<<<1, 1, 0, s>>>(c->ds, npass, V, early_exit, c->p.min_jfa_passes,
+                                     c->p.th_pass_delta);
+        FOS_LAUNCHED(c);
+        return FOS_OK;
+    }
     for (int p = 0; p < npass; ++p) {
         if (step < 1) step = 1;
         const int32_t* in = (p & 1) ? c->labB : c->labA;

@@ -136,6 +136,107 @@ __device__ __forceinline__ void jfa_pass_body(const int32_t* __restrict__ in,
     if (threadIdx.x == 0 && cnt) atomicAdd(&changes[pass], (unsigned long long)cnt);
 }
 
+// ------------------------------------------------- JFA pass over records
+// The owner grid is mirrored by a record grid: record v = the seed
+// (x, y, z, (beta r)^2) of label v, or all-ones bits (NaN) for an unassigned
+// voxel.  A pass then reads each candidate's seed as part of a coalesced
+// 512-byte row of records instead of a label followed by a 16-byte gather per
+// lane (the gathers were ~12 L1 data-pipe wavefronts each and held the pass on
+// L1 throughput).  A NaN record's distance is NaN, and every comparison with
+// NaN is false, so an unassigned candidate never wins and an unassigned
+// voxel's own distance falls back to 1e10 through fminf, as in the reference.
+__device__ __forceinline__ float4 rec_none() {
+    const float q = __int_as_float(-1);
+    return make_float4(q, q, q, q);
+}
+
+// One pass over records with the reference's rule: own label first (1e10 when
+// unassigned), then the 27 offsets in lexicographic (dx, dy, dz) order, a
+// candidate replacing the best only on a strictly smaller power distance.  The
+// winner is tracked by its voxel index, and its label and record are read once
+// at the end.  The distance of a candidate with the voxel's own label equals
+// the own distance, so it can never replace it and no label is needed per
+// candidate; offset (0, 0, 0) is the voxel itself and is not re-evaluated.
+template <bool UNIT_L, bool POW2>
+__device__ __forceinline__ void jfa_pass_rec_body(const int32_t* __restrict__ in,
+                                                  const float4* __restrict__ rin,
+                                                  int32_t* __restrict__ out,
+                                                  float4* __restrict__ rout, int R, int lgR,
+                                                  float vs, float halfL, float L, int step,
+                                                  unsigned long long* changes, int pass,
+                                                  long long lin) {
+    const int V = R * R * R;  // R <= 512, so V < 2^31
+    const bool live = lin < V;
+    const int l = live ? (int)lin : 0;
+    int x, y, z;
+    if (POW2) {
+        z = l & (R - 1);
+        y = (l >> lgR) & (R - 1);
+        x = l >> (2 * lgR);
+    } else {
+        z = l % R;
+        const int t = l / R;
+        y = t % R;
+        x = t / R;
+    }
+    int xs[3], ys[3], zs[3];
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+        int o = (k - 1) * step;
+        if (POW2) {
+            xs[k] = ((x + o) & (R - 1)) << (2 * lgR);
+            ys[k] = ((y + o) & (R - 1)) << lgR;
+            zs[k] = (z + o) & (R - 1);
+        } else {
+            xs[k] = wrap_small(x + o, R) * R * R;
+            ys[k] = wrap_small(y + o, R) * R;
+            zs[k] = wrap_small(z + o, R);
+        }
+    }
+    const int own = in[l];
+    const float4 orec = __ldg(&rin[l]);
+    const float vx = voxel_centre(x, vs, halfL), vy = voxel_centre(y, vs, halfL),
+                vz = voxel_centre(z, vs, halfL);
+    const float2 vxy = make_float2(vx, vy);
+    float bd = fminf(UNIT_L ? power_dist_unit2(vxy, vz, orec)
+                            : jfa_dist<false>(vx, vy, vz, orec, L), 1e10f);
+    int bl = l;
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+        int idx[9];
+        float4 r[9];
+#pragma unroll
+        for (int k = 0; k < 9; ++k) {
+            idx[k] = xs[a] + ys[k / 3] + zs[k % 3];
+            if (!(a == 1 && k == 4)) r[k] = __ldg(&rin[idx[k]]);
+        }
+#pragma unroll
+        for (int k = 0; k < 9; ++k) {
+            if (a == 1 && k == 4) continue;  // the voxel itself
+            const float d = UNIT_L ? power_dist_unit2(vxy, vz, r[k])
+                                   : jfa_dist<false>(vx, vy, vz, r[k], L);
+            if (d < bd) {
+                bd = d;
+                bl = idx[k];
+            }
+        }
+    }
+    int best = own;
+    float4 brec = orec;
+    if (bl != l) {
+        best = in[bl];
+        brec = __ldg(&rin[bl]);
+    }
+    int changed = 0;
+    if (live) {
+        out[l] = best;
+        rout[l] = brec;
+        changed = best != own;
+    }
+    int cnt = __syncthreads_count(changed);
+    if (threadIdx.x == 0 && cnt) atomicAdd(&changes[pass], (unsigned long long)cnt);
+}
+
 // Voxel coordinates of linear index l (z fastest) in 32-bit arithmetic
 // (R <= 512, so R^3 < 2^31): shifts for a power-of-two R, else divisions.
 __device__ __forceinline__ void vox_xyz(int l, int R, int& x, int& y, int& z) {
