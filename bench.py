@@ -23,6 +23,7 @@ from __future__ import annotations
 
 import argparse
 import json
+import math
 import os
 import subprocess
 import sys
@@ -136,12 +137,25 @@ def measured_peaks():
 
 
 def profile_traffic():
-    """Per-launch DRAM bytes of the JFA pass from the committed ncu summary."""
+    """Per-launch DRAM bytes (ncu dram__bytes_read.sum + dram__bytes_write.sum)
+    from the committed summary, each with the commit and command it came from."""
     path = os.path.join(ROOT, "profiles", "traffic.json")
     try:
         return json.load(open(path))
     except Exception:
         return None
+
+
+def traffic_bytes(traffic, kernel):
+    e = (traffic or {}).get(kernel)
+    return e.get("bytes") if isinstance(e, dict) else None
+
+
+def traffic_source(traffic, kernel):
+    e = (traffic or {}).get(kernel)
+    if not isinstance(e, dict):
+        return None
+    return f"ncu capture at commit {e.get('commit')} ({e.get('workload')})"
 
 
 # ------------------------------------------------------------- CPU arm
@@ -154,21 +168,29 @@ def oracle_sim(foam):
                        jfa_cadence=foam.jfa_cadence)
     sim = O.OracleSim(p, foam.pos, foam.rad)
     sim.initialize()
-    sim.frame = foam.jfa_warm  # steady-state cadence: frame 20 is a JFA frame
     return sim, O
 
 
 def time_cpu(foam, steps, warmup):
+    """The CPU restatement over the frames the GPU arm's resident steps time:
+    the 20 warm-start frames (JFA every frame) and `warmup` cadence steps
+    untimed, then `steps` timed 5-frame steps, each followed by one untimed
+    step (the frames of the GPU arm's interleaved e2e step).  Returns
+    (frames/s, timed seconds, threads, first timed frame)."""
     sim, O = oracle_sim(foam)
-    for _ in range(warmup):
+    for _ in range(foam.jfa_warm + warmup * FRAMES_PER_STEP):
+        sim.step()
+    first = sim.frame
+    dt = 0.0
+    for k in range(steps):
+        t0 = time.perf_counter()
         for _ in range(FRAMES_PER_STEP):
             sim.step()
-    t0 = time.perf_counter()
-    for _ in range(steps):
-        for _ in range(FRAMES_PER_STEP):
-            sim.step()
-    dt = time.perf_counter() - t0
-    return FRAMES_PER_STEP * steps / dt, dt, O.num_threads()
+        dt += time.perf_counter() - t0
+        if k + 1 < steps:
+            for _ in range(FRAMES_PER_STEP):
+                sim.step()
+    return FRAMES_PER_STEP * steps / dt, dt, O.num_threads(), first
 
 
 def run_reference(args):
@@ -179,17 +201,21 @@ def run_reference(args):
     O.build()
     from fos import inputs
     foam = inputs.headline()
-    fps, dt, cores = time_cpu(foam, args.steps, args.warmup)
+    fps, dt, cores, first = time_cpu(foam, args.steps, args.warmup)
     line = {
         "impl": "reference", "metric": METRIC, "value": round(fps, 4), "unit": UNIT,
         "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": round(1000.0 * dt / args.steps, 3), "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-        "config": workload_config(1) | {"path": "CPU restatement of the reference (oracle/)"},
+        "config": workload_config(args.gpus),
+        "impl_path": "CPU restatement of the reference's kernels (oracle/, OpenMP), run on "
+                     "the frames the GPU arm's resident steps time",
         "cpu_baseline": {"value": round(fps, 4), "unit": UNIT, "cores": cores, "kind": "port",
-                         "sample": f"{args.steps} steps x 5 frames of the headline workload "
-                                   f"(steady-state cadence from frame 20), after {args.warmup} "
-                                   f"warm-up steps; reference is Taichi (not installable)"},
+                         "sample": f"{args.steps} timed 5-frame steps from frame {first} (20 "
+                                   f"warm-start JFA frames and {args.warmup} warm-up steps "
+                                   f"untimed; an untimed step between timed ones, as the GPU "
+                                   f"arm's e2e steps); the reference itself is Taichi, which "
+                                   f"is not installable here"},
         "e2e": {"value": round(fps, 4), "unit": UNIT, "h2d_bytes_per_step": 0,
                 "d2h_bytes_per_step": 0},
     }
@@ -256,6 +282,7 @@ def run_fos(args):
     h_fsc = torch.empty((n,), dtype=torch.int32).pin_memory()
     e2e_ms = 0.0
     launches = 0
+    frame_evs = []
     barrier()
     for _ in range(args.steps):
         flush.fill_(1.0)
@@ -263,8 +290,17 @@ def run_fos(args):
         e1 = torch.cuda.Event(enable_timing=True)
         l0 = sim.ctx.launch_count()
         e0.record(s)
-        one_step()
-        e1.record(s)
+        # an event after every frame: the plain frames' intervals are the
+        # dynamics kernel's live, in-step duration (roofline below)
+        prev_ev = e0
+        for _ in range(FRAMES_PER_STEP):
+            kind = "jfa" if sim.cfg.is_jfa_frame(sim.frame) else "plain"
+            sim.step()
+            ev = torch.cuda.Event(enable_timing=True)
+            ev.record(s)
+            frame_evs.append((kind, prev_ev, ev))
+            prev_ev = ev
+        e1 = prev_ev
         launches += sim.ctx.launch_count() - l0
         times.append((e0, e1))
         h_pos.copy_(sim.pos)
@@ -298,6 +334,29 @@ def run_fos(args):
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
     e2e_value = world * FRAMES_PER_STEP * args.steps / (float(t.item()) / 1000.0)
 
+    # ---- late run: frames 800-999 of the 1,000-frame workload (the foam packs
+    # over a run and its frames slow down), 5-frame steps as above
+    while sim.frame < 800:
+        sim.step()
+    late_ms, late_steps = 0.0, 0
+    while sim.frame + FRAMES_PER_STEP <= 1000:
+        flush.fill_(1.0)
+        a = torch.cuda.Event(enable_timing=True)
+        b = torch.cuda.Event(enable_timing=True)
+        a.record(s)
+        one_step()
+        b.record(s)
+        b.synchronize()
+        late_ms += a.elapsed_time(b)
+        late_steps += 1
+    t = torch.tensor([late_ms], dtype=torch.float64, device=dev)
+    if world > 1:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    late_run = {"frames": f"800-{sim.frame - 1}",
+                "value": round(world * FRAMES_PER_STEP * late_steps / (float(t.item()) / 1000.0),
+                               3),
+                "unit": UNIT, "ms_per_step": round(float(t.item()) / late_steps, 4)}
+
     # ---- per-kernel timing on the launching stream, after the timed region
     ctx = sim.ctx
     peaks = measured_peaks()
@@ -305,24 +364,13 @@ def run_fos(args):
     traffic = profile_traffic() or {}
     G3 = sim.cfg.grid_res() ** 3
     # (a) dominant kernel by time: k_frame_coop, the dynamics of one frame (one
-    # launch per frame).  Timed on plain frames outside the graph; the event pair
-    # also covers its 16-byte reset kernel, one memset and the frame-end kernel.
-    coop_ms, coop_n = 0.0, 0
-    sim.use_graph = False
-    while coop_n < 10:
-        if sim.cfg.is_jfa_frame(sim.frame):
-            sim.step()
-            continue
-        flush.fill_(1.0)
-        c0 = torch.cuda.Event(enable_timing=True)
-        c1 = torch.cuda.Event(enable_timing=True)
-        c0.record(s)
-        sim.step()
-        c1.record(s)
-        c1.synchronize()
-        coop_ms += c0.elapsed_time(c1)
-        coop_n += 1
-    sim.use_graph = True
+    # launch per frame).  Its duration is the live one inside the timed steps:
+    # the mean interval of the plain frames, whose graph holds k_frame_coop and
+    # three small launches (a 16-byte reset kernel, one memset, the frame-end
+    # kernel).  The JFA frame's interval is reported beside it.
+    plain_ms = [a.elapsed_time(b) for k, a, b in frame_evs if k == "plain"]
+    jfa_frame_ms = [a.elapsed_time(b) for k, a, b in frame_evs if k == "jfa"]
+    coop_ms, coop_n = float(sum(plain_ms)), len(plain_ms)
     coop_s = coop_ms / 1000.0 / coop_n
     K, M = foam.pbd_iters, foam.pressure_iters
     # algorithmic bytes per launch (first-touch, per particle / per cell), summed
@@ -346,13 +394,19 @@ def run_fos(args):
         j1.synchronize()
         jfa_ms += j0.elapsed_time(j1)
     passes = ctx.num_passes
+    # the interval holds the passes and the one record-grid build before them
     pass_s = jfa_ms / 1000.0 / (reps * passes)
     V = foam.res ** 3
     alg_bytes = 8.0 * V  # int32 label read + write per voxel per pass
     achieved = alg_bytes / pass_s / 1e9
+    # FP32 work: 27 candidates x ~20 FP32 operations per voxel and pass (the
+    # nominal count of the scope table), none of them FMAs (-fmad=false), so
+    # the peak is the lane-operation rate 148 SMs x 128 lanes x 1.965 GHz
+    fp32_ops = 540.0 * V
+    fp32_lane_peak = 148 * 128 * 1.965e9
+    fp32_frac = fp32_ops / pass_s / fp32_lane_peak
     st = FosJfaStats()
     call("fos_jfa_stats", ctx.h, n, C.c_void_p(sim.rad.data_ptr()), C.byref(st), stream())
-    fp32_peak_tflops = 148 * 128 * 1.965e9 / 1e12
 
     surrogate = None if args.no_surrogate else run_surrogate_arm(args, foam, flush, barrier, world)
     ensemble = None if args.no_ensemble else run_ensemble(args, barrier, world, rank)
@@ -368,10 +422,11 @@ def run_fos(args):
     topo = run_topology(sim, foam, not args.no_cpu_baseline)
     cpu = None
     if not args.no_cpu_baseline:
-        fps, dt, cores = time_cpu(foam, args.cpu_sample_steps, 0)
+        fps, dt, cores, first = time_cpu(foam, args.cpu_sample_steps, args.warmup)
         cpu = {"value": round(fps, 4), "unit": UNIT, "cores": cores, "kind": "port",
-               "sample": f"{args.cpu_sample_steps} x 5-frame cadence cycle of the same workload "
-                         f"from a fresh warm-up-PBD foam at frame 20 ({dt:.1f} s, OpenMP oracle)"}
+               "sample": f"{args.cpu_sample_steps} timed 5-frame step(s) from frame {first}, "
+                         f"the GPU arm's first timed frames, after the untimed warm-start and "
+                         f"warm-up frames ({dt:.1f} s timed, OpenMP oracle)"}
     line = {
         "metric": METRIC, "value": round(value, 3), "unit": UNIT, "n_gpus": world,
         "steps": args.steps, "warmup": args.warmup,
@@ -385,18 +440,35 @@ def run_fos(args):
                      "frac": round(coop_achieved / peak, 5),
                      "peak_source": "measured (MEASURED_PEAKS.json hbm_gbs)" if peaks else
                                     "fallback 6650 GB/s",
-                     "traffic": traffic.get("k_frame_coop"),
+                     "traffic": traffic_bytes(traffic, "k_frame_coop"),
+                     "traffic_source": traffic_source(traffic, "k_frame_coop"),
                      "alg_bytes_per_launch": coop_bytes, "launch_us": round(coop_s * 1e6, 2),
+                     "launch_us_source": f"live: mean of {coop_n} plain-frame graph intervals "
+                                         "inside the timed steps (k_frame_coop + reset kernel, "
+                                         "memset, frame-end kernel)",
+                     "jfa_frame_us": round(1000.0 * sum(jfa_frame_ms) / max(1, len(jfa_frame_ms)),
+                                           2),
                      "note": "latency/barrier bound: 14 phases (13 grid barriers) over L2-resident "
                              "data; HBM is not the limiting roof"},
-        "roofline_jfa_pass": {"bound": "hbm", "kernel": "k_jfa_pass (128^3, one pass)",
+        "roofline_jfa_pass": {"bound": "fp32-issue", "kernel": "k_jfa_pass_rec (128^3, one pass)",
                               "achieved": round(achieved, 2), "peak": peak, "unit": "GB/s",
                               "frac": round(achieved / peak, 4),
-                              "traffic": traffic.get("k_jfa_pass"),
+                              "fp32": {"achieved_T_ops_per_s": round(fp32_ops / pass_s / 1e12, 2),
+                                       "peak_T_ops_per_s": round(fp32_lane_peak / 1e12, 2),
+                                       "frac": round(fp32_frac, 4),
+                                       "ops_per_voxel": 540,
+                                       "peak_note": "lane operations without FMA (148 x 128 x "
+                                                    "1.965 GHz); 74.4 TFLOP/s counts an FMA "
+                                                    "as two"},
+                              "traffic": traffic_bytes(traffic, "k_jfa_pass_rec"),
+                              "traffic_source": traffic_source(traffic, "k_jfa_pass_rec"),
                               "alg_bytes_per_launch": alg_bytes,
                               "pass_us": round(pass_s * 1e6, 3),
-                              "note": "issue bound (27 candidate evaluations per voxel); "
-                                      "labels are L2-resident at 128^3"},
+                              "pass_us_source": "CUDA events over 8 passes + the record-grid "
+                                                "build, 10 JFA runs on the bench state",
+                              "note": "27 coalesced seed-record rows per voxel; labels and "
+                                      "records are L2-resident at 128^3"},
+        "late_run": late_run,
         "surrogate": surrogate,
         "warm_jfa": warm,
         "ensemble": ensemble,
@@ -407,7 +479,7 @@ def run_fos(args):
                         "finalize_iterations": st.finalize_iterations,
                         "face_pairs": st.face_pairs, "mean_fsc": round(st.mean_fsc, 3),
                         "voxel_passes_per_s": round(V * passes * value / FRAMES_PER_STEP, 1),
-                        "fp32_peak_tflops_nominal": round(fp32_peak_tflops, 2),
+
                         "topology": topo},
     }
     print(json.dumps(line), flush=True)
@@ -506,39 +578,60 @@ def run_surrogate_arm(args, foam, flush, barrier, world):
         barrier()
         if sim.policy is not None:
             sim.policy.judged.clear()
+            forced0 = sim.policy.forced_total
         ms = 0.0
+        jfa_frames = 0
         for _ in range(args.steps):
             flush.fill_(1.0)
             e0 = torch.cuda.Event(enable_timing=True)
             e1 = torch.cuda.Event(enable_timing=True)
             e0.record(s)
             for _ in range(cycle):
-                sim.step()
+                jfa_frames += 1 if sim.step() else 0
             e1.record(s)
             e1.synchronize()
             ms += e0.elapsed_time(e1)
         t = torch.tensor([ms], dtype=torch.float64, device=flush.device)
         if world > 1:
             torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-        return world * cycle * args.steps / (float(t.item()) / 1000.0)
+        fps = world * cycle * args.steps / (float(t.item()) / 1000.0)
+        forced = sim.policy.forced_total - forced0 if sim.policy is not None else 0
+        return fps, jfa_frames / float(cycle * args.steps), forced
 
-    pol = S.RefreshPolicy(every=cycle, warm_frames=foam.jfa_warm)
-    sim = FoamSim.from_foam(foam, surrogate=sur, policy=pol, surrogate_mode=args.surrogate_mode)
-    sim.initialize()
-    fps_sur = timed(sim)
-    judged = list(pol.judged)
-    sim.ctx.close()
-    plain10 = FoamSim.from_foam(foam, JFA_CADENCE=cycle)
-    plain10.initialize()
-    fps_plain10 = timed(plain10)
-    plain10.ctx.close()
     keys = ("exact_frac", "within1_frac", "mean_abs_err", "stale_exact_frac",
             "stale_within1_frac", "stale_mean_abs_err")
-    agree = {k: round(sum(d[k] for d in judged) / max(1, len(judged)), 4) for k in keys}
+
+    def surrogate_run(pol):
+        sim = FoamSim.from_foam(foam, surrogate=sur, policy=pol,
+                                surrogate_mode=args.surrogate_mode)
+        sim.initialize()
+        fps, jfa_frac, forced = timed(sim)
+        judged = list(pol.judged)
+        sim.ctx.close()
+        agree = {k: round(sum(d[k] for d in judged) / max(1, len(judged)), 4) for k in keys}
+        return fps, jfa_frac, forced, judged, agree
+
+    # the guard at the target (the policy's defaults: >= 99 % of cells exact,
+    # mean error <= 0.05 faces), then the same run with the guard off
+    pol = S.RefreshPolicy(every=cycle, warm_frames=foam.jfa_warm)
+    fps_sur, jfa_frac, forced, judged, agree = surrogate_run(pol)
+    off = S.RefreshPolicy(every=cycle, warm_frames=foam.jfa_warm, min_exact=0.0,
+                          max_mean_abs_err=math.inf)
+    fps_off, jfa_frac_off, _, judged_off, agree_off = surrogate_run(off)
+    plain10 = FoamSim.from_foam(foam, JFA_CADENCE=cycle)
+    plain10.initialize()
+    fps_plain10, _, _ = timed(plain10)
+    plain10.ctx.close()
     return {
         "value": round(fps_sur, 3), "unit": UNIT,
         "path": f"surrogate FSC ({args.surrogate_mode}) on every non-JFA frame, exact JFA "
-                f"refresh every {cycle} frames, judged per cell on each refresh",
+                f"refresh every {cycle} frames, judged per cell on each refresh; drift guard "
+                f"at the target (exact_frac >= {pol.min_exact}, mean_abs_err <= "
+                f"{pol.max_mean_abs_err}) forces the next frame to a JFA refresh",
+        "guard": {"min_exact": pol.min_exact, "max_mean_abs_err": pol.max_mean_abs_err,
+                  "forced_refreshes": forced, "jfa_frame_fraction": round(jfa_frac, 4)},
+        "guard_off": {"value": round(fps_off, 3), "jfa_frame_fraction": round(jfa_frac_off, 4),
+                      "judged_frames": len(judged_off), "agreement": agree_off},
         "plain_jfa_every10_value": round(fps_plain10, 3),
         "judged_frames": len(judged), "agreement": agree,
         "meets_99pct_agreement": agree["exact_frac"] >= 0.99,

@@ -198,7 +198,7 @@ __device__ __forceinline__ void jfa_pass_rec_body(const int32_t* __restrict__ in
     const float vx = voxel_centre(x, vs, halfL), vy = voxel_centre(y, vs, halfL),
                 vz = voxel_centre(z, vs, halfL);
     const float2 vxy = make_float2(vx, vy);
-    float bd = fminf(UNIT_L ? power_dist_unit2(vxy, vz, orec)
+    float bd = fminf(UNIT_L ? power_dist_unit2m(vxy, vz, orec)
                             : jfa_dist<false>(vx, vy, vz, orec, L), 1e10f);
     int bl = l;
 #pragma unroll
@@ -213,7 +213,7 @@ __device__ __forceinline__ void jfa_pass_rec_body(const int32_t* __restrict__ in
 #pragma unroll
         for (int k = 0; k < 9; ++k) {
             if (a == 1 && k == 4) continue;  // the voxel itself
-            const float d = UNIT_L ? power_dist_unit2(vxy, vz, r[k])
+            const float d = UNIT_L ? power_dist_unit2m(vxy, vz, r[k])
                                    : jfa_dist<false>(vx, vy, vz, r[k], L);
             if (d < bd) {
                 bd = d;

@@ -255,7 +255,10 @@ class RefreshPolicy:
       last JFA frame.
     * After a judged JFA frame, drift is ``exact_frac < min_exact`` or
       ``mean_abs_err > max_mean_abs_err``.  Drift makes the next
-      ``force_frames`` frames JFA frames too.
+      ``force_frames`` frames JFA frames too.  The defaults are the target's:
+      at least 99 % of cells with the JFA's FSC, and a mean absolute error of
+      at most 0.05 faces per cell.  ``min_exact=0.0`` with
+      ``max_mean_abs_err=math.inf`` switches the guard off.
     * Between JFA frames the surrogate runs on every ``surrogate_every``-th
       frame; on the others the controller keeps its last FSC, as the
       reference does on every non-JFA frame.
@@ -263,8 +266,8 @@ class RefreshPolicy:
     every: int = 10
     surrogate_every: int = 1
     warm_frames: int = 20
-    min_exact: float = 0.0
-    max_mean_abs_err: float = math.inf
+    min_exact: float = 0.99
+    max_mean_abs_err: float = 0.05
     force_frames: int = 1
     last_jfa: int = -10**9
     forced_left: int = 0

@@ -17,6 +17,8 @@ definitions in include/fos.h on the CPU (tests/surrogate_ref.py):
   refresh cadence and drift-forced refreshes follow the policy; the graph
   replay equals the direct calls.
 """
+import math
+
 import numpy as np
 import pytest
 import torch
@@ -255,8 +257,8 @@ def test_refresh_cadence_judging_and_forced_refresh():
     sur = S.Surrogate()
     sur.standardize_from(X["X"])
     sur.fit(X["X"], X["y"], epochs=5, batch=8192)
-    # no drift threshold: warm frames 0-2, then every 3rd frame
-    calm = S.RefreshPolicy(every=3, warm_frames=3)
+    # drift guard off: warm frames 0-2, then every 3rd frame
+    calm = S.RefreshPolicy(every=3, warm_frames=3, min_exact=0.0, max_mean_abs_err=math.inf)
     sim = _sim(surrogate=sur, policy=calm, foam=foam)
     sim.initialize()
     jfa_frames = [f for f in range(12) if sim.step()]

@@ -70,6 +70,16 @@ def test_refresh_policy_abs_error_threshold():
     assert not pol.is_jfa(2) and pol.is_jfa(11)
 
 
+def test_refresh_policy_defaults_are_the_target():
+    """By default the guard holds the surrogate to the target: fewer than 99 %
+    of cells agreeing, or a mean error above 0.05 faces, forces a refresh."""
+    pol = S.RefreshPolicy()
+    assert pol.min_exact == 0.99 and pol.max_mean_abs_err == 0.05
+    assert pol.observe({"exact_frac": 0.985, "mean_abs_err": 0.0}) is True
+    assert S.RefreshPolicy().observe({"exact_frac": 0.995, "mean_abs_err": 0.06}) is True
+    assert S.RefreshPolicy().observe({"exact_frac": 0.995, "mean_abs_err": 0.01}) is False
+
+
 def test_refresh_policy_surrogate_every():
     pol = S.RefreshPolicy(every=10, warm_frames=0, surrogate_every=3)
     pol.ran(0, True)
