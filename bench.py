@@ -68,14 +68,57 @@ def dist_env():
     return rank, world, local
 
 
+# The workloads a line can be measured on: the headline foam (the metric's
+# configuration, the default), the bandwidth-stress foam (200,000 particles
+# on a 256^3 grid, JFA every frame) and the small CPU-runnable foam.
+WORKLOADS = {
+    "small": {"metric": "frames/s at 1k particles, 64^3 JFA every frame (small)",
+              "frames_per_step": 1, "particles": 1000, "jfa_res": 64,
+              "describe": "small foam: N=1000, r ~ U[0.025, 0.035], 64^3 int32 owner grid, 7 "
+                          "JFA passes every frame, K=4 PBD, M=10 pressure, band [10,16]; step = "
+                          "1 frame"},
+    "headline": {"metric": METRIC, "frames_per_step": 5, "particles": 10000, "jfa_res": 128,
+                 "describe": "headline foam: N=10000, 128^3 int32 owner grid, 8 JFA passes, "
+                             "K=8 PBD, M=20 pressure, band [12,16], JFA every 5th frame after 20 "
+                             "warm-start frames; step = 5-frame cadence cycle"},
+    "stress": {"metric": "frames/s at 200k particles, 256^3 JFA every frame (bandwidth stress)",
+               "frames_per_step": 1, "particles": 200000, "jfa_res": 256,
+               "describe": "stress foam: N=200000, bimodal radii (50% U[0.004,0.005], 50% "
+                           "U[0.007,0.009]), 256^3 int32 owner grid, 9 JFA passes every frame, "
+                           "K=8 PBD, M=20 pressure, band [12,16]; step = 1 frame"},
+}
+
+
+def use_workload(name):
+    """Set the module's metric and step length for the named workload."""
+    global METRIC, FRAMES_PER_STEP, WORKLOAD
+    WORKLOAD = name
+    METRIC = WORKLOADS[name]["metric"]
+    FRAMES_PER_STEP = WORKLOADS[name]["frames_per_step"]
+
+
+WORKLOAD = "headline"
+
+
 def workload_config(n_gpus):
-    return {"workload": "headline foam: N=10000, 128^3 int32 owner grid, 8 JFA passes, K=8 PBD, "
-                        "M=20 pressure, band [12,16], JFA every 5th frame after 20 warm-start "
-                        "frames; step = 5-frame cadence cycle",
-            "particles": 10000, "jfa_res": 128, "frames_per_step": FRAMES_PER_STEP,
+    w = WORKLOADS[WORKLOAD]
+    return {"workload": w["describe"],
+            "particles": w["particles"], "jfa_res": w["jfa_res"], "frames_per_step": FRAMES_PER_STEP,
             "l2": "flushed between timed steps (256 MiB write outside the events)",
             "parallelism": f"replicas x{n_gpus} (independent foams, no collective)",
             "path": "plain exact JFA"}
+
+
+def workload_foam(inputs):
+    return {"small": inputs.small, "headline": inputs.headline,
+            "stress": inputs.stress}[WORKLOAD]()
+
+
+def warm_start_frames(foam):
+    """Frames run before the first warm-up step: the warm start of a foam whose
+    JFA cadence changes after it (20 frames on the headline foam), none on a
+    foam that runs the JFA every frame."""
+    return foam.jfa_warm if foam.jfa_warm < foam.frames else 0
 
 
 # ----------------------------------------------------------------- clocks
@@ -151,6 +194,11 @@ def traffic_bytes(traffic, kernel):
     return e.get("bytes") if isinstance(e, dict) else None
 
 
+def tkey(kernel):
+    """traffic.json key of a kernel on the current workload."""
+    return kernel if WORKLOAD == "headline" else f"{kernel}@{WORKLOAD}"
+
+
 def traffic_source(traffic, kernel):
     e = (traffic or {}).get(kernel)
     if not isinstance(e, dict):
@@ -178,7 +226,7 @@ def time_cpu(foam, steps, warmup):
     step (the frames of the GPU arm's interleaved e2e step).  Returns
     (frames/s, timed seconds, threads, first timed frame)."""
     sim, O = oracle_sim(foam)
-    for _ in range(foam.jfa_warm + warmup * FRAMES_PER_STEP):
+    for _ in range(warm_start_frames(foam) + warmup * FRAMES_PER_STEP):
         sim.step()
     first = sim.frame
     dt = 0.0
@@ -200,7 +248,7 @@ def run_reference(args):
     from oracle import oracle as O
     O.build()
     from fos import inputs
-    foam = inputs.headline()
+    foam = workload_foam(inputs)
     fps, dt, cores, first = time_cpu(foam, args.steps, args.warmup)
     line = {
         "impl": "reference", "metric": METRIC, "value": round(fps, 4), "unit": UNIT,
@@ -211,11 +259,11 @@ def run_reference(args):
         "impl_path": "CPU restatement of the reference's kernels (oracle/, OpenMP), run on "
                      "the frames the GPU arm's resident steps time",
         "cpu_baseline": {"value": round(fps, 4), "unit": UNIT, "cores": cores, "kind": "port",
-                         "sample": f"{args.steps} timed 5-frame steps from frame {first} (20 "
-                                   f"warm-start JFA frames and {args.warmup} warm-up steps "
-                                   f"untimed; an untimed step between timed ones, as the GPU "
-                                   f"arm's e2e steps); the reference itself is Taichi, which "
-                                   f"is not installable here"},
+                         "sample": f"{args.steps} timed {FRAMES_PER_STEP}-frame steps from "
+                                   f"frame {first} ({warm_start_frames(foam)} warm-start frames "
+                                   f"and {args.warmup} warm-up steps untimed; an untimed step "
+                                   f"between timed ones, as the GPU arm's e2e steps); the "
+                                   f"reference itself is Taichi, which is not installable here"},
         "e2e": {"value": round(fps, 4), "unit": UNIT, "h2d_bytes_per_step": 0,
                 "d2h_bytes_per_step": 0},
     }
@@ -244,10 +292,10 @@ def run_fos(args):
     import ctypes as C
     from fos._lib import FosJfaStats, call
 
-    foam = inputs.headline()
+    foam = workload_foam(inputs)
     sim = FoamSim.from_foam(foam, use_graph=True)
     sim.initialize()
-    for _ in range(foam.jfa_warm):  # 20 warm-start frames, JFA every frame
+    for _ in range(warm_start_frames(foam)):  # headline: 20 frames with JFA every frame
         sim.step()
     assert sim.frame % foam.jfa_cadence == 0
     flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)
@@ -334,28 +382,30 @@ def run_fos(args):
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
     e2e_value = world * FRAMES_PER_STEP * args.steps / (float(t.item()) / 1000.0)
 
-    # ---- late run: frames 800-999 of the 1,000-frame workload (the foam packs
-    # over a run and its frames slow down), 5-frame steps as above
-    while sim.frame < 800:
-        sim.step()
-    late_ms, late_steps = 0.0, 0
-    while sim.frame + FRAMES_PER_STEP <= 1000:
-        flush.fill_(1.0)
-        a = torch.cuda.Event(enable_timing=True)
-        b = torch.cuda.Event(enable_timing=True)
-        a.record(s)
-        one_step()
-        b.record(s)
-        b.synchronize()
-        late_ms += a.elapsed_time(b)
-        late_steps += 1
-    t = torch.tensor([late_ms], dtype=torch.float64, device=dev)
-    if world > 1:
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-    late_run = {"frames": f"800-{sim.frame - 1}",
-                "value": round(world * FRAMES_PER_STEP * late_steps / (float(t.item()) / 1000.0),
-                               3),
-                "unit": UNIT, "ms_per_step": round(float(t.item()) / late_steps, 4)}
+    # ---- late run: the last 200 frames of a 1,000-frame workload (the foam
+    # packs over a run and its frames slow down), steps as above
+    late_run = None
+    if foam.frames >= 1000:
+        while sim.frame < foam.frames - 200:
+            sim.step()
+        late_ms, late_steps, first_late = 0.0, 0, sim.frame
+        while sim.frame + FRAMES_PER_STEP <= foam.frames:
+            flush.fill_(1.0)
+            a = torch.cuda.Event(enable_timing=True)
+            b = torch.cuda.Event(enable_timing=True)
+            a.record(s)
+            one_step()
+            b.record(s)
+            b.synchronize()
+            late_ms += a.elapsed_time(b)
+            late_steps += 1
+        t = torch.tensor([late_ms], dtype=torch.float64, device=dev)
+        if world > 1:
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        late_run = {"frames": f"{first_late}-{sim.frame - 1}",
+                    "value": round(world * FRAMES_PER_STEP * late_steps /
+                                   (float(t.item()) / 1000.0), 3),
+                    "unit": UNIT, "ms_per_step": round(float(t.item()) / late_steps, 4)}
 
     # ---- per-kernel timing on the launching stream, after the timed region
     ctx = sim.ctx
@@ -371,7 +421,7 @@ def run_fos(args):
     plain_ms = [a.elapsed_time(b) for k, a, b in frame_evs if k == "plain"]
     jfa_frame_ms = [a.elapsed_time(b) for k, a, b in frame_evs if k == "jfa"]
     coop_ms, coop_n = float(sum(plain_ms)), len(plain_ms)
-    coop_s = coop_ms / 1000.0 / coop_n
+    coop_s = coop_ms / 1000.0 / coop_n if coop_n else float("nan")
     K, M = foam.pbd_iters, foam.pressure_iters
     # algorithmic bytes per launch (first-touch, per particle / per cell), summed
     # over the frame's stages: (K+2) grid rebuilds x (68 B/particle + 16 B/cell),
@@ -405,12 +455,29 @@ def run_fos(args):
     fp32_ops = 540.0 * V
     fp32_lane_peak = 148 * 128 * 1.965e9
     fp32_frac = fp32_ops / pass_s / fp32_lane_peak
+    # (c) face extraction (accumulate_face_area: k_faces_reset, k_faces,
+    # k_compact, k_rows) on the last passes' labels, majority-filtered first
+    ctx.majority_filter()
+    f_ms = 0.0
+    for _ in range(reps):
+        flush.fill_(1.0)
+        j0.record(s)
+        ctx.accumulate_faces(n)
+        j1.record(s)
+        j1.synchronize()
+        f_ms += j0.elapsed_time(j1)
+    faces_s = f_ms / 1000.0 / reps
     st = FosJfaStats()
     call("fos_jfa_stats", ctx.h, n, C.c_void_p(sim.rad.data_ptr()), C.byref(st), stream())
+    # 4 B per voxel (filtered label read) + 8 B per distinct face pair
+    faces_bytes = 4.0 * V + 8.0 * st.face_pairs
+    headline_arms = WORKLOAD == "headline"
 
-    surrogate = None if args.no_surrogate else run_surrogate_arm(args, foam, flush, barrier, world)
-    ensemble = None if args.no_ensemble else run_ensemble(args, barrier, world, rank)
-    warm = None if args.no_warm_jfa else run_warm_jfa(foam, flush)
+    surrogate = (None if args.no_surrogate or not headline_arms
+                 else run_surrogate_arm(args, foam, flush, barrier, world))
+    ensemble = (None if args.no_ensemble or not headline_arms
+                else run_ensemble(args, barrier, world, rank))
+    warm = None if args.no_warm_jfa or not headline_arms else run_warm_jfa(foam, flush)
 
     if world > 1:
         dist.barrier()
@@ -419,23 +486,17 @@ def run_fos(args):
             dist.destroy_process_group()
         return 0
 
-    topo = run_topology(sim, foam, not args.no_cpu_baseline)
+    topo = run_topology(sim, foam, not args.no_cpu_baseline) if headline_arms else None
     cpu = None
     if not args.no_cpu_baseline:
         fps, dt, cores, first = time_cpu(foam, args.cpu_sample_steps, args.warmup)
         cpu = {"value": round(fps, 4), "unit": UNIT, "cores": cores, "kind": "port",
-               "sample": f"{args.cpu_sample_steps} timed 5-frame step(s) from frame {first}, "
-                         f"the GPU arm's first timed frames, after the untimed warm-start and "
-                         f"warm-up frames ({dt:.1f} s timed, OpenMP oracle)"}
-    line = {
-        "metric": METRIC, "value": round(value, 3), "unit": UNIT, "n_gpus": world,
-        "steps": args.steps, "warmup": args.warmup,
-        "ms_per_step": round(total_ms / args.steps, 4), "higher_is_better": True,
-        "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-        "config": workload_config(world),
-        "e2e": {"value": round(e2e_value, 3), "unit": UNIT, "h2d_bytes_per_step": n * 16,
-                "d2h_bytes_per_step": n * 20},
-        "roofline": {"bound": "hbm", "kernel": "k_frame_coop (dynamics of one frame)",
+               "sample": f"{args.cpu_sample_steps} timed {FRAMES_PER_STEP}-frame step(s) from "
+                         f"frame {first}, the GPU arm's first timed frames, after the untimed "
+                         f"warm-start and warm-up frames ({dt:.1f} s timed, OpenMP oracle)"}
+    coop_roof = None
+    if coop_n:
+        coop_roof = {"bound": "hbm", "kernel": "k_frame_coop (dynamics of one frame)",
                      "achieved": round(coop_achieved, 2), "peak": peak, "unit": "GB/s",
                      "frac": round(coop_achieved / peak, 5),
                      "peak_source": "measured (MEASURED_PEAKS.json hbm_gbs)" if peaks else
@@ -449,8 +510,18 @@ def run_fos(args):
                      "jfa_frame_us": round(1000.0 * sum(jfa_frame_ms) / max(1, len(jfa_frame_ms)),
                                            2),
                      "note": "latency/barrier bound: 14 phases (13 grid barriers) over L2-resident "
-                             "data; HBM is not the limiting roof"},
-        "roofline_jfa_pass": {"bound": "fp32-issue", "kernel": "k_jfa_pass_rec (128^3, one pass)",
+                             "data; HBM is not the limiting roof"}
+    line = {
+        "metric": METRIC, "value": round(value, 3), "unit": UNIT, "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": round(total_ms / args.steps, 4), "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": workload_config(world),
+        "e2e": {"value": round(e2e_value, 3), "unit": UNIT, "h2d_bytes_per_step": n * 16,
+                "d2h_bytes_per_step": n * 20},
+        "roofline": coop_roof,
+        "roofline_jfa_pass": {"bound": "fp32-issue",
+                              "kernel": f"k_jfa_pass_rec ({foam.res}^3, one pass)",
                               "achieved": round(achieved, 2), "peak": peak, "unit": "GB/s",
                               "frac": round(achieved / peak, 4),
                               "fp32": {"achieved_T_ops_per_s": round(fp32_ops / pass_s / 1e12, 2),
@@ -460,14 +531,14 @@ def run_fos(args):
                                        "peak_note": "lane operations without FMA (148 x 128 x "
                                                     "1.965 GHz); 74.4 TFLOP/s counts an FMA "
                                                     "as two"},
-                              "traffic": traffic_bytes(traffic, "k_jfa_pass_rec"),
-                              "traffic_source": traffic_source(traffic, "k_jfa_pass_rec"),
+                              "traffic": traffic_bytes(traffic, tkey("k_jfa_pass_rec")),
+                              "traffic_source": traffic_source(traffic, tkey("k_jfa_pass_rec")),
                               "alg_bytes_per_launch": alg_bytes,
                               "pass_us": round(pass_s * 1e6, 3),
                               "pass_us_source": "CUDA events over 8 passes + the record-grid "
                                                 "build, 10 JFA runs on the bench state",
                               "note": "27 coalesced seed-record rows per voxel; labels and "
-                                      "records are L2-resident at 128^3"},
+                                      "records are L2-resident at 128^3, not at 256^3"},
         "late_run": late_run,
         "surrogate": surrogate,
         "warm_jfa": warm,
@@ -482,6 +553,24 @@ def run_fos(args):
 
                         "topology": topo},
     }
+    faces_achieved = faces_bytes / faces_s / 1e9
+    line["roofline_faces"] = {
+        "bound": "hbm", "kernel": f"face extraction ({foam.res}^3: k_faces_reset, k_faces, "
+                                  f"k_compact, k_rows)",
+        "achieved": round(faces_achieved, 2), "peak": peak, "unit": "GB/s",
+        "frac": round(faces_achieved / peak, 4), "alg_bytes_per_launch": faces_bytes,
+        "face_pairs": int(st.face_pairs), "us": round(faces_s * 1e6, 2),
+        "traffic": traffic_bytes(traffic, tkey("k_faces")),
+        "traffic_source": traffic_source(traffic, tkey("k_faces")),
+        "note": "4 B per voxel + 8 B per distinct pair; the pair table is probed at random"}
+    if WORKLOAD != "headline":
+        # every frame runs the JFA: the dominant kernel is the pass (on the
+        # stress foam the bandwidth case: two 67 MB label grids and two
+        # 268 MB record grids do not fit the 126 MB L2)
+        jr = line.pop("roofline_jfa_pass")
+        jr["bound"] = "hbm"
+        line["roofline"] = jr
+        line["jfa_frame_ms"] = round(sum(jfa_frame_ms) / max(1, len(jfa_frame_ms)), 4)
     print(json.dumps(line), flush=True)
     if world > 1:
         dist.destroy_process_group()
@@ -938,6 +1027,8 @@ def run_profile(args):
 
 def main():
     args = parse()
+    if not args.profile:
+        use_workload(args.workload)
     if args.profile:
         return run_profile(args)
     if args.impl == "reference":
