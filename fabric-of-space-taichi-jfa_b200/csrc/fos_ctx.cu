@@ -334,6 +334,24 @@ extern "C" int fos_device_error(FosCtx* c, int* word, fos_stream_t s) {
     return FOS_OK;
 }
 
+__global__ void k_set_dev_int(int* p, int v) { *p = v; }
+
+extern "C" int fos_device_error_clear(FosCtx* c, fos_stream_t s) {
+    FOS_REQUIRE(c != nullptr, FOS_E_ARG, "ctx is NULL");
+    k_set_dev_int<<<1, 1, 0, s>>>(&c->ds->error, 0);
+    FOS_LAUNCHED(c);
+    return FOS_OK;
+}
+
+extern "C" int fos_test_barrier_plan(FosCtx* c, int leave_at_barrier, fos_stream_t s) {
+    FOS_REQUIRE(c != nullptr, FOS_E_ARG, "ctx is NULL");
+    FOS_REQUIRE(leave_at_barrier == 0 || leave_at_barrier >= 2, FOS_E_ARG,
+                "leave_at_barrier must be 0 (off) or >= 2");
+    k_set_dev_int<<<1, 1, 0, s>>>(&c->ds->bar_test, leave_at_barrier);
+    FOS_LAUNCHED(c);
+    return FOS_OK;
+}
+
 // ------------------------------------------------------------------- scan
 // Block-wide exclusive scan of 4 consecutive items per thread (1024 threads,
 // 4096 items per tile) using warp shuffles.

@@ -18,6 +18,7 @@
 #define FOS_ROWCAP 64     // candidate partners kept per particle before the 32-slot cut
 #define FOS_FIN_MAXIT 4096
 #define FOS_BAR_CYCLE_LIMIT 2000000000LL  // ~1 s at the B200's 1.965 GHz SM clock
+#define FOS_BAR_TEST_CYCLES 2000000LL      // ~1 ms: the bound under fos_test_barrier_plan
 
 // ----------------------------------------------------------- device state
 // Small per-context block in device memory: the frame counters the frame
@@ -45,6 +46,7 @@ struct FosDevState {
     unsigned int coop_epoch;      // cooperative frame launches (tags of the pressure words)
     unsigned int rmax_bits;       // cooperative frame: largest radius before the PBD sweeps
     unsigned int rmax0_bits;      // cooperative frame: largest radius at the frame's start
+    int bar_test;                 // fos_test_barrier_plan: 0, or the barrier a block leaves at
     unsigned long long changes[FOS_MAX_PASSES];
 };
 
@@ -357,6 +359,10 @@ __device__ __forceinline__ uint4 philox4x32_10(uint4 c, uint32_t k0, uint32_t k1
 // Bounded: a block that has waited ~1 s (clock64), or that sees the error word
 // set, records FOS_E_TIMEOUT and returns false, so a stuck barrier ends the
 // kernel instead of hanging the GPU.
+// Test plan (ds->bar_test, set by fos_test_barrier_plan; 0 in normal use):
+// when it holds k >= 2, the launch's last block leaves at its k-th barrier
+// without arriving, and every barrier from the second on waits at most
+// FOS_BAR_TEST_CYCLES, so the failure path runs in about a millisecond.
 __device__ __forceinline__ unsigned int ld_acquire_gpu(const unsigned int* p) {
     unsigned int v;
     asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
@@ -388,12 +394,25 @@ __device__ __forceinline__ bool grid_barrier(FosDevState* ds, unsigned int& epoc
     __shared__ int s_ok;
     __shared__ unsigned int s_flags;
     __shared__ unsigned int s_fetch[4];
+    // the launch's test plan (fos_test_barrier_plan), read by thread 0 while
+    // it polls at the launch's first barrier and kept for the later ones
+    __shared__ int s_test;
     __syncthreads();
     if (threadIdx.x == 0) {
         epoch += 1u;
         unsigned int target = epoch * gridDim.x;
+        const bool planned = epoch >= 2u && s_test != 0;
+        if (planned && (int)epoch == s_test && blockIdx.x == gridDim.x - 1) {
+            // the planned failure: this block leaves without arriving, so the
+            // others' bounded waits run out
+            s_ok = 0;
+            s_flags = 0u;
+            for (int k = 0; k < nf; ++k) s_fetch[k] = 0u;
+        } else {
+        const long long limit = planned ? FOS_BAR_TEST_CYCLES : FOS_BAR_CYCLE_LIMIT;
         bool ok = true;
         red_release_gpu_add(&ds->bar_count, 1u);
+        if (epoch == 1u) s_test = *((volatile int*)&ds->bar_test);
         long long t0 = clock64();
         unsigned int polls = 0;
         unsigned int v;
@@ -401,7 +420,7 @@ __device__ __forceinline__ bool grid_barrier(FosDevState* ds, unsigned int& epoc
             // the error word and the clock are checked every 32 polls, so a
             // poll is one L2 round trip and the release is seen sooner
             if ((++polls & 31u) == 0u) {
-                if (*((volatile int*)&ds->error) != 0 || clock64() - t0 > FOS_BAR_CYCLE_LIMIT) {
+                if (*((volatile int*)&ds->error) != 0 || clock64() - t0 > limit) {
                     atomicCAS(&ds->error, 0, (int)FOS_E_TIMEOUT);
                     ok = false;
                     break;
@@ -412,6 +431,7 @@ __device__ __forceinline__ bool grid_barrier(FosDevState* ds, unsigned int& epoc
         s_ok = ok ? 1 : 0;
         s_flags = v >> FOS_BAR_FLAG_SHIFT;
         for (int k = 0; k < nf; ++k) s_fetch[k] = *((const volatile unsigned int*)fetch[k]);
+        }
     }
     __syncthreads();
     if (flags) *flags = s_flags;

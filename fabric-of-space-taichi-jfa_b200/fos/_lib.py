@@ -221,6 +221,8 @@ SIGNATURES = {
     "fos_ensemble_launch_count": [_P],
     "fos_launch_count": [_P],
     "fos_device_error": [_P, C.POINTER(_I), _P],
+    "fos_device_error_clear": [_P, _P],
+    "fos_test_barrier_plan": [_P, _I, _P],
     "fos_status_string": [_I],
     "fos_last_error": [],
 }

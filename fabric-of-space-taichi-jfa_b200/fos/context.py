@@ -108,6 +108,16 @@ class Context:
         call("fos_device_error", self.h, C.byref(w), stream())
         return w.value
 
+    def clear_device_error(self):
+        """Clear the device error word after a failed launch has ended."""
+        call("fos_device_error_clear", self.h, stream())
+
+    def test_barrier_plan(self, leave_at_barrier: int):
+        """For failure-path tests: later cooperative launches lose one block at
+        grid barrier `leave_at_barrier` (>= 2) and their waits give up after
+        ~1 ms with FOS_E_TIMEOUT; 0 turns it off."""
+        call("fos_test_barrier_plan", self.h, int(leave_at_barrier), stream())
+
     # ----------------------------------------------------------------- JFA
     def labels(self) -> torch.Tensor:
         """Final owner grid of the last run, [R, R, R] int32 (view)."""

@@ -632,6 +632,19 @@ long long fos_ensemble_launch_count(FosEnsemble* e);
 long long fos_launch_count(FosCtx* ctx);
 /* Device error word (synchronises) and a static string for a status code. */
 int fos_device_error(FosCtx* ctx, int* word, fos_stream_t s);
+/* Clear the device error word (stream-ordered); the context is usable again
+ * once a failed launch has ended.  No reference counterpart: the reference
+ * raises Taichi exceptions and has only an unused JFA_WATCHDOG_INTERVAL
+ * (config.py:174). */
+int fos_device_error_clear(FosCtx* ctx, fos_stream_t s);
+/* For tests of the failure path, no reference counterpart.  With
+ * leave_at_barrier = k >= 2, every later cooperative launch on ctx (the
+ * frame's dynamics kernel, the finalize fixed point, the ensemble kernel)
+ * makes its last block leave at its k-th grid barrier without arriving, and
+ * bounds every wait from the second barrier on by about 1 ms instead of 1 s:
+ * the other blocks record FOS_E_TIMEOUT in the error word and end.  Nothing
+ * faults and nothing hangs.  0 turns the plan off (the default). */
+int fos_test_barrier_plan(FosCtx* ctx, int leave_at_barrier, fos_stream_t s);
 const char* fos_status_string(int status);
 /* Thread-local text of the last error raised by any entry point. */
 const char* fos_last_error(void);
