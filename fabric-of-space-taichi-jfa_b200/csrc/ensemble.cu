@@ -401,7 +401,7 @@ __global__ void __launch_bounds__(THREADS) k_ens_coop(EnsArgs a) {
                           d.r_min, d.r_max, bg, a.bp_mode, a.contact_tol);
             a.rad[i] = r;
         }
-        if (a.sweeps > 0) a.vol0[i] = powf(r, a.pa.P);
+        if (a.sweeps > 0) a.vol0[i] = pow_P(r, a.pa.P);
     }
     if (!grid_barrier(a.ds, ep)) return;
     // (4) pressure sweeps with each foam's bounds and local hash index

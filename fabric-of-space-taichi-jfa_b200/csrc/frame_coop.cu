@@ -258,7 +258,7 @@ __global__ void __launch_bounds__(COOP_THREADS, COOP_BLOCKS_PER_SM) k_frame_coop
                 ri = nudge_one(ri, __ldcg(&a.rad_target[i]), __ldcg(&a.lmd[i]), a.alpha,
                                a.max_step, a.rmin, a.rmax, bg, a.bp_mode, a.contact_tol);
         }
-        float Vi = live ? powf(ri, pa.P) : 0.f;
+        float Vi = live ? pow_P(ri, pa.P) : 0.f;
         if (live && gl == 0) {
             if (nudge) a.rad[i] = ri;
             st_tagged(&a.ptag[i], tbase | 1u, Vi);
@@ -280,7 +280,7 @@ __global__ void __launch_bounds__(COOP_THREADS, COOP_BLOCKS_PER_SM) k_frame_coop
             if (nb.fc > 0) d = pressure_sum_n<NL>(pa, nb, lane, ri, Vi, vj);
             ri = fmaxf(pa.rmin, fminf(pa.rmax, fadd(ri, d)));
             if (w + 1 < a.sweeps) {
-                Vi = powf(ri, pa.P);
+                Vi = pow_P(ri, pa.P);
                 if (live && gl == 0) st_tagged(&a.ptag[(size_t)(w + 1) * a.n + i], tag + 1u, Vi);
             }
         }
@@ -308,7 +308,7 @@ __global__ void __launch_bounds__(COOP_THREADS, COOP_BLOCKS_PER_SM) k_frame_coop
                               a.max_step, a.rmin, a.rmax, bg, a.bp_mode, a.contact_tol);
                 a.rad[i] = r;
             }
-            if (a.sweeps > 0) a.vol0[i] = powf(r, a.pa.P);
+            if (a.sweeps > 0) a.vol0[i] = pow_P(r, a.pa.P);
         }
     }
     if (!grid_barrier(a.ds, ep)) return;

@@ -421,6 +421,40 @@ __device__ __forceinline__ unsigned int maxov_warp(int kk, int lane, const float
     return b;
 }
 
+// Powers of the pressure sweeps (dynamics.py:1504-1543: rad ** P_exp and
+// V ** (1.0 / P_exp) with f32 P_exp, which Taichi's CPU backend evaluates with
+// libm powf).  For PRESSURE_EXP = 3 (config.py:113) both are computed to the
+// correctly rounded float, which glibc's powf returns for >99.9 % of these
+// arguments (CUDA's powf differs from it more often):
+//   x^3: the product in double (x^2 is exact; one rounding), then one
+//   rounding to float;
+//   y^invP, invP = f32(1/3) = 1/3 + 9.934107481e-9: cbrtf (within 1 ulp),
+//   one Newton step in double (error ~2^-46), times
+//   y^9.934e-9 = 1 + 9.934e-9 ln y (the next term is ~2^-47), rounded once.
+// B200 runs FP64 at half the FP32 rate, so each costs a fraction of powf's
+// instructions: the twenty barrier-free sweeps of a headline frame fell from
+// 50.1 to 45.6 us.  Other exponents use powf.
+__device__ __forceinline__ float pow_P(float x, float P) {
+    if (P == 3.0f) {
+        const double d = (double)x;
+        return __double2float_rn(__dmul_rn(__dmul_rn(d, d), d));
+    }
+    return powf(x, P);
+}
+
+__device__ __forceinline__ float root_P(float y, float invP) {
+    if (invP == 0.333333343f) {
+        const float c = cbrtf(y);
+        const double cd = (double)c;
+        const double e = __dadd_rn(__dmul_rn(__dmul_rn(cd, cd), cd), -(double)y);
+        const double inv = (double)__frcp_rn(fmul(3.0f, fmul(c, c)));
+        const double cn = __dadd_rn(cd, -__dmul_rn(e, inv));
+        const double k = __dmul_rn(9.934107481e-9, (double)__logf(y));
+        return __double2float_rn(__dadd_rn(cn, __dmul_rn(cn, k)));
+    }
+    return powf(y, invP);
+}
+
 // hash_func (dynamics.py:1436-1451) in wrapping int32 arithmetic.
 __device__ __forceinline__ int hash_func(int i, int frame) {
     unsigned int t = (unsigned int)i + 12345u * (unsigned int)frame;
@@ -453,7 +487,7 @@ __device__ __forceinline__ float pressure_group(int i, int lane, const PressureA
     if (fc > 0) {
         int an = fc < a.max_nei ? fc : a.max_nei;
         int st = hash_func(i - a.hoff, a.frame) % fc;
-        float Vi = powf(ri, a.P);
+        float Vi = pow_P(ri, a.P);
         float invP = fdiv(1.0f, a.P);
         for (int base = 0; base < an; base += GS) {
             int kk = base + gl;
@@ -463,11 +497,11 @@ __device__ __forceinline__ float pressure_group(int i, int lane, const PressureA
                 int ni = (st + kk) % fc;
                 int j = LD::ld(&a.face_ids[(size_t)i * FOS_S + ni]);
                 if (!(j < 0 || j >= a.n || j == i)) {
-                    float Vj = powf(LD::ld(&rin[j]), a.P);
+                    float Vj = pow_P(LD::ld(&rin[j]), a.P);
                     float dvr = fmul(a.k, fsub(Vi, Vj));
                     float vmin = fminf(Vi, Vj);
                     float dv = fmaxf(fmul(-a.cap, vmin), fminf(fmul(a.cap, vmin), dvr));
-                    term = fsub(powf(fsub(Vi, dv), invP), ri);
+                    term = fsub(root_P(fsub(Vi, dv), invP), ri);
                     hit = true;
                 }
             }
@@ -577,7 +611,7 @@ __device__ __forceinline__ float pressure_sum_n(const PressureArgs& a, const Pre
             const float dvr = fmul(a.k, fsub(Vi, Vj));
             const float vmin = fminf(Vi, Vj);
             const float dv = fmaxf(fmul(-a.cap, vmin), fminf(fmul(a.cap, vmin), dvr));
-            term[h] = fsub(powf(fsub(Vi, dv), invP), ri);
+            term[h] = fsub(root_P(fsub(Vi, dv), invP), ri);
         }
     }
     float d = 0.f;
@@ -607,17 +641,17 @@ __device__ __forceinline__ float pressure_sweep8x2(int i, int lane, const Pressu
     if (nb.fc > 0) {
         const float rj0 = nb.ok[0] ? LD::ld(&rin[nb.j[0]]) : 0.f;
         const float rj1 = nb.ok[1] ? LD::ld(&rin[nb.j[1]]) : 0.f;
-        const float Vi = powf(ri, a.P);
+        const float Vi = pow_P(ri, a.P);
         const float invP = fdiv(1.0f, a.P);
         float term[2] = {0.f, 0.f};
 #pragma unroll
         for (int h = 0; h < 2; ++h) {
             if (nb.ok[h]) {
-                const float Vj = powf(h == 0 ? rj0 : rj1, a.P);
+                const float Vj = pow_P(h == 0 ? rj0 : rj1, a.P);
                 const float dvr = fmul(a.k, fsub(Vi, Vj));
                 const float vmin = fminf(Vi, Vj);
                 const float dv = fmaxf(fmul(-a.cap, vmin), fminf(fmul(a.cap, vmin), dvr));
-                term[h] = fsub(powf(fsub(Vi, dv), invP), ri);
+                term[h] = fsub(root_P(fsub(Vi, dv), invP), ri);
             }
         }
 #pragma unroll
@@ -638,10 +672,10 @@ __device__ __forceinline__ float pressure_sweep8x2(int i, int lane, const Pressu
 }
 
 // pressure_sweep8x2 with the particle powers V = r^P carried between sweeps:
-// vin[j] == powf(rin[j], P) for every j, so a neighbour costs one powf (its
+// vin[j] == pow_P(rin[j], P) for every j, so a neighbour costs one root (its
 // new-radius term) instead of two, and lane 0 also writes vout[i] =
-// powf(rout[i], P) for the next sweep (vout may be NULL).  The result is
-// pressure_sweep8x2's bit for bit: the same powf of the same values.
+// pow_P(rout[i], P) for the next sweep (vout may be NULL).  The result is
+// pressure_sweep8x2's bit for bit: the same powers of the same values.
 // The radius delta of one 8-lane group's particle (radius ri, power Vi = ri^P)
 // from its neighbours' powers vj0 / vj1 (lane t: neighbours t and t + 8 of
 // the hashed rotation), summed in neighbour order; every lane of the group
@@ -660,7 +694,7 @@ __device__ __forceinline__ float pressure_sum8x2(const PressureArgs& a, const Pr
             const float dvr = fmul(a.k, fsub(Vi, Vj));
             const float vmin = fminf(Vi, Vj);
             const float dv = fmaxf(fmul(-a.cap, vmin), fminf(fmul(a.cap, vmin), dvr));
-            term[h] = fsub(powf(fsub(Vi, dv), invP), ri);
+            term[h] = fsub(root_P(fsub(Vi, dv), invP), ri);
         }
     }
     // neighbour order: lanes 0..7 of the group for h = 0, then for h = 1; the
@@ -698,7 +732,7 @@ __device__ __forceinline__ float pressure_sweep8x2v(int i, int lane, const Press
         delta_r[i] = d;
         const float rn = fmaxf(a.rmin, fminf(a.rmax, fadd(ri, d)));
         rout[i] = rn;
-        if (vout) vout[i] = powf(rn, a.P);
+        if (vout) vout[i] = pow_P(rn, a.P);
     }
     return d;
 }

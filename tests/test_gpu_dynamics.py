@@ -2,7 +2,8 @@
 
 Bar (FP32): positions, radii, volumes within 1e-5 relative (PBD, pressure,
 controller); Brownian jitter and the max-overlap reduction are compared
-exactly; the pressure kernel uses CUDA powf vs libm powf, so it is held to
+exactly; the pressure kernel's powers (two products for r^3, a corrected
+cbrtf for the 1/3 root) differ from libm powf by a few ulp, so it is held to
 the 1e-5 relative tolerance, not bit equality.
 """
 import numpy as np

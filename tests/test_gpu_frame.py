@@ -1,8 +1,8 @@
 """Whole-frame parity: the GPU frame driver against the oracle's frame driver.
 
-Frame 0 involves no powf-dependent step (pressure is a no-op before the first
+Frame 0 involves no power-dependent step (pressure is a no-op before the first
 JFA), so it must be bit-exact end to end.  Later frames run the pressure
-sweeps (CUDA powf vs libm powf differ by a few ulp): positions and radii are
+sweeps (their powers differ from libm powf by a few ulp): positions and radii are
 held to 1e-5 relative after one frame, and longer runs are compared through
 the FSC histogram and the radius distribution, since trajectories diverge.
 """

@@ -9,8 +9,8 @@ same inputs, and compares the outputs:
   neighbour lists, FSC, EMA and hysteresis scores over consecutive runs, the
   pass count and per-pass changes, cell lists, PBD sweeps, overlap depths,
   the controller, Brownian and OU jitter and the dirty tiles;
-- within 1e-5 relative: radii after pressure sweeps (CUDA powf against libm
-  powf).
+- within 1e-5 relative: radii after pressure sweeps (the GPU's powers for
+  P = 3 against libm powf).
 """
 import json
 import os
