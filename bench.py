@@ -52,6 +52,8 @@ def parse():
     ap.add_argument("--workload", default="headline", choices=["small", "headline", "stress"])
     ap.add_argument("--no-surrogate", action="store_true",
                     help="skip the surrogate-FSC arm of the metric")
+    ap.add_argument("--no-surrogate-large", action="store_true",
+                    help="skip the surrogate on the 50,000-particle 192^3 variant")
     ap.add_argument("--surrogate-mode", default="absolute", choices=["absolute", "anchored"])
     ap.add_argument("--no-warm-jfa", action="store_true",
                     help="skip the warm-started JFA arm (frames/s and agreement with the exact JFA)")
@@ -636,26 +638,21 @@ def run_topology(sim, foam, with_cpu):
     return out
 
 
-def run_surrogate_arm(args, foam, flush, barrier, world):
-    """The metric's second arm: frames/s when the learned FSC surrogate
-    supplies FSC between exact JFA refreshes every 10 frames (the spec's
-    "refresh every 5 or 10 frames"), next to the plain path with JFA every 10
-    frames (the same JFA work with no FSC update between: the surrogate's
-    cost floor).  Both start from the same warm-started foam at frame 20; a
-    step is one 10-frame refresh cycle, L2 flushed between steps; each judged
-    JFA frame reads its counters on the host (one sync per cycle, inside the
-    timed region).  Agreement: per-cell rint(surrogate FSC) == JFA fsc on the
-    refresh frames of the timed region, beside the stale FSC the reference
-    reuses (previous JFA fsc vs this one)."""
-    import time as _time
+def surrogate_measure(args, foam, sur, flush, barrier, world, steps):
+    """frames/s of `foam` with the learned FSC surrogate `sur` supplying FSC
+    between exact JFA refreshes every 10 frames (the spec's "refresh every 5 or
+    10 frames"), with the drift guard at the target and off, next to the plain
+    path with JFA every 10 frames (the same JFA work with no FSC update
+    between: the surrogate's cost floor).  Each run starts from the same
+    warm-started foam; a step is one 10-frame refresh cycle, L2 flushed between
+    steps; each judged JFA frame reads its counters on the host (one sync per
+    cycle, inside the timed region).  Agreement: per-cell rint(surrogate FSC)
+    == JFA fsc on the refresh frames of the timed region, beside the stale FSC
+    the reference reuses (previous JFA fsc vs this one)."""
     import torch
     from fos import surrogate as S
     from fos.driver import FoamSim
 
-    t0 = _time.perf_counter()
-    sur = S.train_default()
-    torch.cuda.synchronize()
-    train_s = _time.perf_counter() - t0
     cycle = 10
     s = torch.cuda.current_stream()
 
@@ -670,7 +667,7 @@ def run_surrogate_arm(args, foam, flush, barrier, world):
             forced0 = sim.policy.forced_total
         ms = 0.0
         jfa_frames = 0
-        for _ in range(args.steps):
+        for _ in range(steps):
             flush.fill_(1.0)
             e0 = torch.cuda.Event(enable_timing=True)
             e1 = torch.cuda.Event(enable_timing=True)
@@ -683,9 +680,9 @@ def run_surrogate_arm(args, foam, flush, barrier, world):
         t = torch.tensor([ms], dtype=torch.float64, device=flush.device)
         if world > 1:
             torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-        fps = world * cycle * args.steps / (float(t.item()) / 1000.0)
+        fps = world * cycle * steps / (float(t.item()) / 1000.0)
         forced = sim.policy.forced_total - forced0 if sim.policy is not None else 0
-        return fps, jfa_frames / float(cycle * args.steps), forced
+        return fps, jfa_frames / float(cycle * steps), forced
 
     keys = ("exact_frac", "within1_frac", "mean_abs_err", "stale_exact_frac",
             "stale_within1_frac", "stale_mean_abs_err")
@@ -726,10 +723,46 @@ def run_surrogate_arm(args, foam, flush, barrier, world):
         "meets_99pct_agreement": agree["exact_frac"] >= 0.99,
         "pairs_last": judged[-1]["pairs"] if judged else None,
         "overflow_last": judged[-1]["overflow"] if judged else None,
-        "train": {"seconds": round(train_s, 2), "foams": "headline law, seeds 10-19",
-                  "frames": "JFA frames 20-200", "rows": "3,000,000 sampled pairs",
-                  "epochs": 30, "lr": 1e-3, "batch": 65536},
     }
+
+
+def run_surrogate_arm(args, foam, flush, barrier, world):
+    """The metric's second arm (surrogate_measure) on the headline foam, with
+    the model trained on the headline law (seeds 10-19); then config 4's
+    50,000-particle variant (the same law scaled by (1/5)^(1/3), 192^3 grid):
+    a model trained on JFA frames of that variant's seeds 10-19, measured on
+    held-out seed 20."""
+    import time as _time
+    import torch
+    from fos import inputs
+    from fos import surrogate as S
+
+    t0 = _time.perf_counter()
+    sur = S.train_default()
+    torch.cuda.synchronize()
+    train_s = _time.perf_counter() - t0
+    out = surrogate_measure(args, foam, sur, flush, barrier, world, args.steps)
+    out["train"] = {"seconds": round(train_s, 2), "foams": "headline law, seeds 10-19",
+                    "frames": "JFA frames 20-200", "rows": "3,000,000 sampled pairs",
+                    "epochs": 30, "lr": 1e-3, "batch": 65536}
+    if args.no_surrogate_large:
+        return out
+    t0 = _time.perf_counter()
+    frames = (20, 60, 100)
+    big = S.train_default(foams=[inputs.surrogate_variant(s, large=True) for s in range(10, 20)],
+                          frames=frames)
+    torch.cuda.synchronize()
+    train_big = _time.perf_counter() - t0
+    held = inputs.surrogate_variant(20, large=True)
+    res = surrogate_measure(args, held, big, flush, barrier, world, min(args.steps, 5))
+    res["workload"] = (f"{held.name}: N={held.n}, {held.res}^3, held-out seed 20 of the "
+                       f"variant law")
+    res["train"] = {"seconds": round(train_big, 2), "foams": "50k variant, seeds 10-19",
+                    "frames": "JFA frames " + ", ".join(str(f) for f in frames),
+                    "rows": "3,000,000 sampled pairs", "epochs": 30, "lr": 1e-3,
+                    "batch": 65536}
+    out["large_variant"] = res
+    return out
 
 
 def run_warm_jfa(foam, flush):

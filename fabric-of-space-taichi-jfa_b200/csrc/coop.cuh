@@ -164,6 +164,12 @@ struct OuStep {
     float kick;           // sigma * sqrt(dt)
     unsigned int frame;
     int ctr_base;         // Philox counter = i - ctr_base (index within the foam)
+    // batched ensembles: per-foam values in place of kick, o.k0/o.k1 and
+    // ctr_base, looked up through foam_of[i] (NULL for a single foam)
+    const int32_t* foam_of = nullptr;
+    const float* kick_f = nullptr;   // sigma * sqrt(dt) of each foam's mean radius
+    const uint2* key_f = nullptr;    // each foam's Philox key (its seed)
+    const int32_t* base_f = nullptr; // each foam's first particle index
 };
 
 // A P1 target given directly.
@@ -199,9 +205,20 @@ struct P1Defer {
                                           const OuStep* ou = nullptr) {
         if (i >= 0) {
             float3 p = make_float3(v.x, v.y, v.z);
-            if (ou)
-                p = ou_one(i, (unsigned int)(i - ou->ctr_base), p, ou->vjit, v.w, ou->kick, ou->o,
-                           ou->frame);
+            if (ou) {
+                if (ou->foam_of) {
+                    const int f = __ldg(&ou->foam_of[i]);
+                    OuParams o = ou->o;
+                    const uint2 k = __ldg(&ou->key_f[f]);
+                    o.k0 = k.x;
+                    o.k1 = k.y;
+                    p = ou_one(i, (unsigned int)(i - __ldg(&ou->base_f[f])), p, ou->vjit, v.w,
+                               __ldcg(&ou->kick_f[f]), o, ou->frame);
+                } else {
+                    p = ou_one(i, (unsigned int)(i - ou->ctr_base), p, ou->vjit, v.w, ou->kick,
+                               ou->o, ou->frame);
+                }
+            }
             coop_p1_val(a, geo, i, p, v.w, dst, p1_target(a, t));
         }
         i = -1;

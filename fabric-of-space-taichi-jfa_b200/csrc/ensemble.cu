@@ -47,6 +47,7 @@ struct EnsWords {  // per-foam device words
     int zero_fsc;
     unsigned int omax_bits;
     int pad;
+    unsigned long long rad_sum;  // OU jitter: the foam's radii, 2^-40 fixed point (exact)
     unsigned long long changes[FOS_MAX_PASSES];
 };
 
@@ -70,6 +71,11 @@ struct FosEnsemble {
     float *pos = nullptr, *rad = nullptr, *rad_target = nullptr, *lmd = nullptr,
           *delta_r = nullptr;
     int32_t *cc = nullptr, *cs = nullptr, *ci = nullptr;
+    // OU jitter (fp.ou_jitter): packed velocities and per-foam kick, key, base
+    float* vjit = nullptr;
+    float* ou_kick = nullptr;
+    uint2* ou_key = nullptr;
+    int32_t* ou_base = nullptr;
     FosEnsembleTuning tune{256, 256, 1024, 1};
     cudaGraphExec_t gexec[2] = {nullptr, nullptr};
     bool gvalid[2] = {false, false};
@@ -312,13 +318,21 @@ struct EnsArgs {
     float alpha, max_step;
     PressureArgs pa;
     float strength, domain, L, invL, halfL;
+    // OU jitter (dynamics.py:607-660, run.py:855-867) per foam
+    int ou;
+    float* vjit;
+    float* ou_kick;
+    const uint2* ou_key;
+    const int32_t* ou_base;
+    OuParams ou_p;
 };
 
 // One PBD sweep over every particle of every foam on layout `lay`, into
 // pos_tmp; with p1, each new position also enters the histogram of the next
 // rebuild (count buffer par), wrapped into pos.
 __device__ __forceinline__ void ens_pbd(const EnsArgs& a, const EnsGeo& geo, const CoopLayout& lay,
-                                        int wid, int W_, int lane, bool p1, int par) {
+                                        int wid, int W_, int lane, bool p1, int par,
+                                        const OuStep* ou = nullptr) {
     const int rounds = (a.n + W_ - 1) / W_;
     P1Defer d1;
     int kk_next = wid < a.n ? __ldcg(&a.slot_of[wid]) : 0;
@@ -333,10 +347,10 @@ __device__ __forceinline__ void ens_pbd(const EnsArgs& a, const EnsGeo& geo, con
             int pi = pbd_warp<LdL2>(kk, lane, lay.sp, lay.ci, a.pos_tmp, g,
                                     lay.cs ? lay.cs + d.cell_off : nullptr, lay.cc + d.cell_off,
                                     a.gap1, a.mdf, a.dmul, &nv, lay.cap, d.cell_off);
-            if (p1) d1.put(a, geo, lane, pi, nv, a.pos, coop_p1_par(a, par));
+            if (p1) d1.put(a, geo, lane, pi, nv, a.pos, coop_p1_par(a, par), ou);
         }
     }
-    if (p1) d1.flush(a, geo, a.pos, coop_p1_par(a, par));
+    if (p1) d1.flush(a, geo, a.pos, coop_p1_par(a, par), ou);
 }
 
 template <int THREADS>
@@ -430,10 +444,15 @@ __global__ void __launch_bounds__(THREADS) k_ens_coop(EnsArgs a) {
             if (!grid_barrier(a.ds, ep)) return;
         }
     }
-    // (5) Brownian jitter with each foam's key and local counter; settle -= 1
+    // (5) Brownian jitter with each foam's key and local counter; settle -= 1.
+    // With the OU jitter on, each foam's final radii are also summed exactly
+    // for its mean radius (run.py:860-861).
     for (int i = tid; i < a.n; i += T) {
         if (a.sweeps & 1) a.rad[i] = __ldcg(&a.rad_tmp[i]);
         const EnsFoamDev& d = a.F[a.foam_of[i]];
+        if (a.ou)
+            atomicAdd(&a.W[a.foam_of[i]].rad_sum,
+                      (unsigned long long)rad_fixed(__ldcg(&a.rad[i])));
         brownian_one<LdL2>(i, (unsigned int)(i - d.part_off), a.pos, a.strength, a.domain, a.halfL,
                            d.k0, d.k1, (unsigned int)frame);
         coop_p1_one(a, geo, i, a.pos, a.rad, a.pos, coop_p1_par(a, gk & 1));
@@ -441,12 +460,23 @@ __global__ void __launch_bounds__(THREADS) k_ens_coop(EnsArgs a) {
     for (int f = tid; f < a.nf; f += T)
         if (a.W[f].settle > 0) a.W[f].settle -= 1;
     if (!grid_barrier(a.ds, ep)) return;
-    // (6) PBD sweeps, each on a fresh grid; (7) final rebuild
+    // (6) PBD sweeps, each on a fresh grid; (7) final rebuild.  The OU jitter
+    // (run.py:855-867) runs inside the last sweep's P1 with each foam's kick
+    // (from its mean radius, written here, read after the layout phase's
+    // barrier), key and local counter, as the single-foam frame does.
+    if (a.ou)
+        for (int f = tid; f < a.nf; f += T)
+            a.ou_kick[f] = ou_kick(a.ou_p, mean_from_fixed(
+                                                *((volatile unsigned long long*)&a.W[f].rad_sum),
+                                                a.F[f].n));
+    OuStep ous{a.vjit, a.rad, a.ou_p, 0.f, (unsigned int)frame, 0,
+               a.foam_of, a.ou_kick, a.ou_key, a.ou_base};
     const float* src = a.pos;
     for (int k = 0; k < a.pbd_iters; ++k) {
         if (!coop_grid(a, geo, src, a.pos, a.rad, false, tk, ep, true, gk & 1, false, &lay)) return;
         ++gk;
-        ens_pbd(a, geo, lay, wid, W_, lane, true, gk & 1);
+        ens_pbd(a, geo, lay, wid, W_, lane, true, gk & 1,
+                a.ou && k == a.pbd_iters - 1 ? &ous : nullptr);
         if (!grid_barrier(a.ds, ep)) return;
         src = a.pos_tmp;
     }
@@ -455,7 +485,10 @@ __global__ void __launch_bounds__(THREADS) k_ens_coop(EnsArgs a) {
 
 __global__ void k_ens_coop_prep(FosDevState* ds, EnsWords* W, int nf) {
     int f = blockIdx.x * blockDim.x + threadIdx.x;
-    if (f < nf) W[f].omax_bits = 0u;
+    if (f < nf) {
+        W[f].omax_bits = 0u;
+        W[f].rad_sum = 0ull;
+    }
     if (f == 0) {
         ds->grid_ovf = 0;
         ds->bar_count = 0u;
@@ -479,7 +512,8 @@ extern "C" int fos_ensemble_destroy(FosEnsemble* e) {
         if (e->gexec[k]) cudaGraphExecDestroy(e->gexec[k]);
     void* ptrs[] = {e->df,  e->dw,  e->dvo,        e->foam_of, e->labA, e->labB, e->filt,
                     e->slot, e->seedlin, e->pos,   e->rad,     e->rad_target, e->lmd,
-                    e->delta_r, e->cc, e->cs,      e->ci};
+                    e->delta_r, e->cc, e->cs,      e->ci,      e->vjit, e->ou_kick, e->ou_key,
+                    e->ou_base};
     for (void* q : ptrs)
         if (q) cudaFree(q);
     if (e->c) fos_ctx_destroy(e->c);
@@ -586,6 +620,18 @@ static int ens_create_impl(FosEnsemble* e, const FosEnsembleFoam* foams) {
     FOS_CUDA(cudaMemset(e->cc, 0, (size_t)g3 * 4));
     FOS_CUDA(cudaMemset(e->cs, 0, (size_t)g3 * 4));
     FOS_CUDA(cudaMemset(e->ci, 0, (size_t)ntot * 4));
+    if (e->fp.ou_jitter) {
+        std::vector<uint2> key(nf);
+        for (int f = 0; f < nf; ++f) key[f] = make_uint2(e->hf[f].k0, e->hf[f].k1);
+        FOS_CUDA(cudaMalloc(&e->vjit, (size_t)ntot * 12));
+        FOS_CUDA(cudaMemset(e->vjit, 0, (size_t)ntot * 12));
+        FOS_CUDA(cudaMalloc(&e->ou_kick, nf * sizeof(float)));
+        FOS_CUDA(cudaMalloc(&e->ou_key, nf * sizeof(uint2)));
+        FOS_CUDA(cudaMalloc(&e->ou_base, nf * sizeof(int32_t)));
+        FOS_CUDA(cudaMemcpy(e->ou_key, key.data(), nf * sizeof(uint2), cudaMemcpyHostToDevice));
+        FOS_CUDA(cudaMemcpy(e->ou_base, e->hpo.data(), nf * sizeof(int32_t),
+                            cudaMemcpyHostToDevice));
+    }
     return FOS_OK;
 }
 
@@ -598,7 +644,8 @@ extern "C" int fos_ensemble_create(const FosParams* p, const FosFrameParams* fp,
     FOS_REQUIRE(nfoams >= 1 && nfoams <= 65536, FOS_E_ARG, "nfoams must be in [1, 65536]");
     FOS_REQUIRE(p->early_exit == 0, FOS_E_ARG, "ensembles run every pass: early_exit must be 0");
     FOS_REQUIRE(fp->max_eq_nei <= 16, FOS_E_ARG, "ensembles need max_eq_nei <= 16");
-    FOS_REQUIRE(!fp->ou_jitter, FOS_E_ARG, "ensembles run without the OU jitter (ou_jitter = 0)");
+    FOS_REQUIRE(!fp->ou_jitter || fp->pbd_iters >= 1, FOS_E_ARG,
+                "ensembles run the OU jitter inside a PBD sweep: pbd_iters >= 1");
     for (int f = 0; f < nfoams; ++f) {
         int rc = ens_check_foam(foams[f]);
         if (rc) return rc;
@@ -757,6 +804,13 @@ static int ens_coop_launch(FosEnsemble* e, int mode, cudaStream_t s) {
     a.L = c->L;
     a.invL = c->invL;
     a.halfL = (float)(0.5 * (double)c->L);
+    a.ou = fp->ou_jitter ? 1 : 0;
+    a.vjit = e->vjit;
+    a.ou_kick = e->ou_kick;
+    a.ou_key = e->ou_key;
+    a.ou_base = e->ou_base;
+    a.ou_p = ou_params(fp->jitter_rms, fp->jitter_tau, fp->max_drift_fraction, c->p.gap_fraction,
+                       (float)fp->dt, c->L, c->invL, 0);
     k_ens_coop_prep<<<fos_blocks(e->nf > 0 ? e->nf : 1, 256), 256, 0, s>>>(c->ds, e->dw, e->nf);
     FOS_LAUNCHED(c);
     FOS_CUDA(cudaMemsetAsync(c->coop_cnt, 0, (size_t)e->g3tot * sizeof(int32_t), s));
@@ -805,6 +859,7 @@ extern "C" int fos_ensemble_init(FosEnsemble* e, int frame0, fos_stream_t s_) {
     FOS_CUDA(cudaMemsetAsync(e->lmd, 0, n * 4, s));
     FOS_CUDA(cudaMemsetAsync(e->delta_r, 0, n * 4, s));
     FOS_CUDA(cudaMemsetAsync(e->dw, 0, e->nf * sizeof(EnsWords), s));
+    if (e->vjit) FOS_CUDA(cudaMemsetAsync(e->vjit, 0, n * 12, s));
     FOS_CUDA(cudaMemcpyAsync(e->rad_target, e->rad, n * 4, cudaMemcpyDeviceToDevice, s));
     k_frame_set<<<1, 1, 0, s>>>(c->ds, frame0, 0);
     FOS_LAUNCHED(c);

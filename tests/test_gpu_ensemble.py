@@ -74,6 +74,29 @@ def test_ensemble_equals_single_foams(use_graph):
     ens.close()
 
 
+def test_ensemble_with_ou_jitter_equals_single_foams():
+    """The OU jitter (dynamics.py:607-660, run.py:855-867) inside the
+    ensemble's dynamics kernel: each foam's mean radius from its own exact
+    radius sum, its own Philox key and local counter, so every foam still
+    equals the same foam run alone with the jitter on."""
+    foams = _foams()
+    over = dict(OVER, JITTER_ENABLED=True)
+    ens = Ensemble(foams, **over)
+    sims = [FoamSim.from_foam(f, **over) for f in foams]
+    for s in sims:
+        s.initialize()
+    ens.initialize()
+    for f in range(6):
+        jfa = ens.step()
+        for s in sims:
+            assert s.step() == jfa
+        torch.cuda.synchronize()
+        _assert_same(ens, sims, f"frame {f}")
+    for s in sims:
+        s.ctx.close()
+    ens.close()
+
+
 def test_tuning_does_not_change_results():
     foams = _foams()
     outs = []

@@ -120,8 +120,13 @@ def test_ou_off_leaves_v_jit_untouched():
     assert torch.count_nonzero(a.v_jit).item() == 0
 
 
-def test_ensemble_rejects_ou():
+def test_ensemble_ou_needs_a_pbd_sweep():
+    """Ensembles run the OU jitter inside the last PBD sweep (as the
+    single-foam frame does), so a configuration without PBD sweeps is
+    rejected; with sweeps it is accepted (test_gpu_ensemble covers its
+    results)."""
     from fos import _lib
     from fos.ensemble import Ensemble
     with pytest.raises(_lib.FosError):
-        Ensemble([inputs.ensemble_member(700, 11, 10)], JITTER_ENABLED=True)
+        Ensemble([inputs.ensemble_member(700, 11, 10)], JITTER_ENABLED=True, PBD_ITERS=0)
+    Ensemble([inputs.ensemble_member(700, 11, 10)], JITTER_ENABLED=True).close()
