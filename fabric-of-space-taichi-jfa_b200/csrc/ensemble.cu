@@ -66,6 +66,7 @@ struct FosEnsemble {
     long long vtot = 0;
     int g3tot = 0, max_passes = 0;
     int32_t *labA = nullptr, *labB = nullptr, *filt = nullptr;
+    float4 *recA = nullptr, *recB = nullptr;  // seed records mirroring labA / labB
     unsigned long long* slot = nullptr;
     int32_t* seedlin = nullptr;
     float *pos = nullptr, *rad = nullptr, *rad_target = nullptr, *lmd = nullptr,
@@ -191,6 +192,49 @@ __global__ void __launch_bounds__(512) k_ens_jfa_pass(const long long* __restric
     else
         jfa_pass_body<UNIT_L, false, TIE_LOWER>(in, out, seeds, d.R, d.lgR, d.vs, halfL, L, step,
                                                 W[f].changes, pass, lin);
+}
+
+// The same pass over the packed seed-record grids (jfa_pass_rec_body): the
+// candidates' seeds come as coalesced record rows instead of label loads and
+// seed gathers.  Records of the padding between foams are never read.
+template <bool UNIT_L>
+__global__ void __launch_bounds__(512) k_ens_jfa_pass_rec(const long long* __restrict__ vo,
+                                                          int nf,
+                                                          const EnsFoamDev* __restrict__ F,
+                                                          int32_t* __restrict__ labA,
+                                                          int32_t* __restrict__ labB,
+                                                          float4* __restrict__ recA,
+                                                          float4* __restrict__ recB,
+                                                          float halfL, float L, EnsWords* W,
+                                                          int pass) {
+    const long long v0 = (long long)blockIdx.x * blockDim.x;
+    const int f = ens_vox_foam(vo, nf, v0);
+    const EnsFoamDev d = F[f];
+    if (pass >= d.passes) return;  // block-uniform
+    int step = (d.R / 2) >> pass;
+    if (step < 1) step = 1;
+    const int32_t* in = ((pass & 1) ? labB : labA) + d.vox_off;
+    int32_t* out = ((pass & 1) ? labA : labB) + d.vox_off;
+    const float4* rin = ((pass & 1) ? recB : recA) + d.vox_off;
+    float4* rout = ((pass & 1) ? recA : recB) + d.vox_off;
+    const long long lin = v0 + threadIdx.x - d.vox_off;
+    if (d.pow2)
+        jfa_pass_rec_body<UNIT_L, true>(in, rin, out, rout, d.R, d.lgR, d.vs, halfL, L, step,
+                                        W[f].changes, pass, lin);
+    else
+        jfa_pass_rec_body<UNIT_L, false>(in, rin, out, rout, d.R, d.lgR, d.vs, halfL, L, step,
+                                         W[f].changes, pass, lin);
+}
+
+// Records of the packed label grids (seeds[label], NaN bits when unassigned).
+__global__ void k_ens_rec_from_labels(const int32_t* __restrict__ lab,
+                                      const float4* __restrict__ seeds, float4* __restrict__ rec,
+                                      long long V) {
+    for (long long l = (long long)blockIdx.x * blockDim.x + threadIdx.x; l < V;
+         l += (long long)gridDim.x * blockDim.x) {
+        const int v = lab[l];
+        rec[l] = v >= 0 ? __ldg(&seeds[v]) : rec_none();
+    }
 }
 
 __global__ void __launch_bounds__(512) k_ens_majority(const long long* __restrict__ vo, int nf,
@@ -511,6 +555,7 @@ extern "C" int fos_ensemble_destroy(FosEnsemble* e) {
     for (int k = 0; k < 2; ++k)
         if (e->gexec[k]) cudaGraphExecDestroy(e->gexec[k]);
     void* ptrs[] = {e->df,  e->dw,  e->dvo,        e->foam_of, e->labA, e->labB, e->filt,
+                    e->recA, e->recB,
                     e->slot, e->seedlin, e->pos,   e->rad,     e->rad_target, e->lmd,
                     e->delta_r, e->cc, e->cs,      e->ci,      e->vjit, e->ou_kick, e->ou_key,
                     e->ou_base};
@@ -602,6 +647,8 @@ static int ens_create_impl(FosEnsemble* e, const FosEnsembleFoam* foams) {
     FOS_CUDA(cudaMalloc(&e->labA, vtot * 4));
     FOS_CUDA(cudaMalloc(&e->labB, vtot * 4));
     FOS_CUDA(cudaMalloc(&e->filt, vtot * 4));
+    FOS_CUDA(cudaMalloc(&e->recA, vtot * sizeof(float4)));
+    FOS_CUDA(cudaMalloc(&e->recB, vtot * sizeof(float4)));
     FOS_CUDA(cudaMalloc(&e->slot, vtot * 8));
     FOS_CUDA(cudaMalloc(&e->seedlin, ntot * 4));
     FOS_CUDA(cudaMemset(e->labA, 0xFF, vtot * 4));
@@ -893,6 +940,25 @@ static int ens_seed_passes(FosEnsemble* e, cudaStream_t s) {
     const bool ul = c->L == 1.0f, tie = c->p.tie_lower_index != 0;
     const int pb = e->tune.pass_block;
     const int pgrid = (int)(e->vtot / pb);
+    if (!tie) {
+        // the reference's scan-order tie rule runs over the seed records
+        int rb = fos_blocks(e->vtot, 256);
+        if (rb > 8 * c->num_sms) rb = 8 * c->num_sms;
+        k_ens_rec_from_labels<<<rb, 256, 0, s>>>(e->labA, c->seeds, e->recA, e->vtot);
+        FOS_LAUNCHED(c);
+        for (int p = 0; p < e->max_passes; ++p) {
+            if (ul)
+                k_ens_jfa_pass_rec<true><<<pgrid, pb, 0, s>>>(e->dvo, e->nf, e->df, e->labA,
+                                                              e->labB, e->recA, e->recB, c->halfL,
+                                                              c->L, e->dw, p);
+            else
+                k_ens_jfa_pass_rec<false><<<pgrid, pb, 0, s>>>(e->dvo, e->nf, e->df, e->labA,
+                                                               e->labB, e->recA, e->recB,
+                                                               c->halfL, c->L, e->dw, p);
+            FOS_LAUNCHED(c);
+        }
+        return FOS_OK;
+    }
     for (int p = 0; p < e->max_passes; ++p) {
         if (ul && !tie)
             k_ens_jfa_pass<true, false><<<pgrid, pb, 0, s>>>(e->dvo, e->nf, e->df, e->labA, e->labB,
