@@ -196,10 +196,13 @@ __global__ void __launch_bounds__(512) k_ens_jfa_pass(const long long* __restric
 
 // The same pass over the packed seed-record grids (jfa_pass_rec_body): the
 // candidates' seeds come as coalesced record rows instead of label loads and
-// seed gathers.  Records of the padding between foams are never read.
+// seed gathers.  Records of the padding between foams are never read.  One
+// candidate loop for every R (jfa_pass_rec_body_any) and 3 blocks of 512
+// threads per SM keep it at 40 registers; with a loop per R kind and no
+// bound it took 102, and 16 warps per SM.
 template <bool UNIT_L>
-__global__ void __launch_bounds__(512) k_ens_jfa_pass_rec(const long long* __restrict__ vo,
-                                                          int nf,
+__global__ void __launch_bounds__(512, UNIT_L ? 3 : 2)
+    k_ens_jfa_pass_rec(const long long* __restrict__ vo, int nf,
                                                           const EnsFoamDev* __restrict__ F,
                                                           int32_t* __restrict__ labA,
                                                           int32_t* __restrict__ labB,
@@ -218,12 +221,8 @@ __global__ void __launch_bounds__(512) k_ens_jfa_pass_rec(const long long* __res
     const float4* rin = ((pass & 1) ? recB : recA) + d.vox_off;
     float4* rout = ((pass & 1) ? recA : recB) + d.vox_off;
     const long long lin = v0 + threadIdx.x - d.vox_off;
-    if (d.pow2)
-        jfa_pass_rec_body<UNIT_L, true>(in, rin, out, rout, d.R, d.lgR, d.vs, halfL, L, step,
-                                        W[f].changes, pass, lin);
-    else
-        jfa_pass_rec_body<UNIT_L, false>(in, rin, out, rout, d.R, d.lgR, d.vs, halfL, L, step,
-                                         W[f].changes, pass, lin);
+    jfa_pass_rec_body_any<UNIT_L>(in, rin, out, rout, d.R, d.lgR, d.pow2, d.vs, halfL, L, step,
+                                  W[f].changes, pass, lin);
 }
 
 // Records of the packed label grids (seeds[label], NaN bits when unassigned).

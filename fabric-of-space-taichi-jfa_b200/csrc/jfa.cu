@@ -75,9 +75,11 @@ __global__ void __launch_bounds__(256) k_jfa_pass(const int32_t* __restrict__ in
 
 // Pass over the record grid (jfa_pass_rec_body); the same launch protocol as
 // k_jfa_pass.  Six blocks per SM (at most 40 registers): the pass waits on
-// record-load latency, so residency pays (stress passes 3.91 -> 3.73 ms).
+// record-load latency, so residency pays (stress passes 3.91 -> 3.73 ms).  The
+// general-L distance needs more registers: four blocks per SM (64) for it,
+// where six spilled 340 bytes per thread.
 template <bool UNIT_L, bool POW2>
-__global__ void __launch_bounds__(256, 6) k_jfa_pass_rec(const int32_t* __restrict__ in,
+__global__ void __launch_bounds__(256, UNIT_L ? 6 : 4) k_jfa_pass_rec(const int32_t* __restrict__ in,
                                                       const float4* __restrict__ rin,
                                                       int32_t* __restrict__ out,
                                                       float4* __restrict__ rout, int R, int lgR,

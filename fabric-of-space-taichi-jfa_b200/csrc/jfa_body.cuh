@@ -157,42 +157,15 @@ __device__ __forceinline__ float4 rec_none() {
 // at the end.  The distance of a candidate with the voxel's own label equals
 // the own distance, so it can never replace it and no label is needed per
 // candidate; offset (0, 0, 0) is the voxel itself and is not re-evaluated.
-template <bool UNIT_L, bool POW2>
-__device__ __forceinline__ void jfa_pass_rec_body(const int32_t* __restrict__ in,
-                                                  const float4* __restrict__ rin,
-                                                  int32_t* __restrict__ out,
-                                                  float4* __restrict__ rout, int R, int lgR,
-                                                  float vs, float halfL, float L, int step,
-                                                  unsigned long long* changes, int pass,
-                                                  long long lin) {
-    const int V = R * R * R;  // R <= 512, so V < 2^31
-    const bool live = lin < V;
-    const int l = live ? (int)lin : 0;
-    int x, y, z;
-    if (POW2) {
-        z = l & (R - 1);
-        y = (l >> lgR) & (R - 1);
-        x = l >> (2 * lgR);
-    } else {
-        z = l % R;
-        const int t = l / R;
-        y = t % R;
-        x = t / R;
-    }
-    int xs[3], ys[3], zs[3];
-#pragma unroll
-    for (int k = 0; k < 3; ++k) {
-        int o = (k - 1) * step;
-        if (POW2) {
-            xs[k] = ((x + o) & (R - 1)) << (2 * lgR);
-            ys[k] = ((y + o) & (R - 1)) << lgR;
-            zs[k] = (z + o) & (R - 1);
-        } else {
-            xs[k] = wrap_small(x + o, R) * R * R;
-            ys[k] = wrap_small(y + o, R) * R;
-            zs[k] = wrap_small(z + o, R);
-        }
-    }
+template <bool UNIT_L>
+__device__ __forceinline__ void jfa_rec_core(const int32_t* __restrict__ in,
+                                             const float4* __restrict__ rin,
+                                             int32_t* __restrict__ out,
+                                             float4* __restrict__ rout, float vs, float halfL,
+                                             float L, unsigned long long* changes, int pass,
+                                             int l, bool live, int x, int y, int z,
+                                             const int (&xs)[3], const int (&ys)[3],
+                                             const int (&zs)[3]) {
     const int own = in[l];
     const float4 orec = __ldg(&rin[l]);
     const float vx = voxel_centre(x, vs, halfL), vy = voxel_centre(y, vs, halfL),
@@ -235,6 +208,86 @@ __device__ __forceinline__ void jfa_pass_rec_body(const int32_t* __restrict__ in
     }
     int cnt = __syncthreads_count(changed);
     if (threadIdx.x == 0 && cnt) atomicAdd(&changes[pass], (unsigned long long)cnt);
+}
+
+template <bool UNIT_L, bool POW2>
+__device__ __forceinline__ void jfa_pass_rec_body(const int32_t* __restrict__ in,
+                                                  const float4* __restrict__ rin,
+                                                  int32_t* __restrict__ out,
+                                                  float4* __restrict__ rout, int R, int lgR,
+                                                  float vs, float halfL, float L, int step,
+                                                  unsigned long long* changes, int pass,
+                                                  long long lin) {
+    const int V = R * R * R;  // R <= 512, so V < 2^31
+    const bool live = lin < V;
+    const int l = live ? (int)lin : 0;
+    int x, y, z;
+    if (POW2) {
+        z = l & (R - 1);
+        y = (l >> lgR) & (R - 1);
+        x = l >> (2 * lgR);
+    } else {
+        z = l % R;
+        const int t = l / R;
+        y = t % R;
+        x = t / R;
+    }
+    int xs[3], ys[3], zs[3];
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+        int o = (k - 1) * step;
+        if (POW2) {
+            xs[k] = ((x + o) & (R - 1)) << (2 * lgR);
+            ys[k] = ((y + o) & (R - 1)) << lgR;
+            zs[k] = (z + o) & (R - 1);
+        } else {
+            xs[k] = wrap_small(x + o, R) * R * R;
+            ys[k] = wrap_small(y + o, R) * R;
+            zs[k] = wrap_small(z + o, R);
+        }
+    }
+    jfa_rec_core<UNIT_L>(in, rin, out, rout, vs, halfL, L, changes, pass, l, live, x, y, z, xs,
+                         ys, zs);
+}
+
+// The same pass for a grid whose R is known only at run time (the batched
+// ensembles mix power-of-two and other resolutions in one launch): the
+// coordinates come from shifts or divisions by a block-uniform branch, the
+// wraps from compare-and-add (|x + o| < 2R since step <= R/2), and the
+// candidate loop is shared, so the kernel holds one copy of it.
+template <bool UNIT_L>
+__device__ __forceinline__ void jfa_pass_rec_body_any(const int32_t* __restrict__ in,
+                                                      const float4* __restrict__ rin,
+                                                      int32_t* __restrict__ out,
+                                                      float4* __restrict__ rout, int R, int lgR,
+                                                      bool pow2, float vs, float halfL, float L,
+                                                      int step, unsigned long long* changes,
+                                                      int pass, long long lin) {
+    const int V = R * R * R;
+    const bool live = lin < V;
+    const int l = live ? (int)lin : 0;
+    int x, y, z;
+    if (pow2) {
+        z = l & (R - 1);
+        y = (l >> lgR) & (R - 1);
+        x = l >> (2 * lgR);
+    } else {
+        z = l % R;
+        const int t = l / R;
+        y = t % R;
+        x = t / R;
+    }
+    const int RR = R * R;
+    int xs[3], ys[3], zs[3];
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+        int o = (k - 1) * step;
+        xs[k] = wrap_small(x + o, R) * RR;
+        ys[k] = wrap_small(y + o, R) * R;
+        zs[k] = wrap_small(z + o, R);
+    }
+    jfa_rec_core<UNIT_L>(in, rin, out, rout, vs, halfL, L, changes, pass, l, live, x, y, z, xs,
+                         ys, zs);
 }
 
 // Voxel coordinates of linear index l (z fastest) in 32-bit arithmetic
