@@ -448,6 +448,22 @@ def run_fos(args):
     passes = ctx.num_passes
     # the interval holds the passes and the one record-grid build before them
     pass_s = jfa_ms / 1000.0 / (reps * passes)
+    # the same passes with the record rows staged in shared memory by TMA
+    # copies (off by default; measured here beside the default form)
+    staged_ms = None
+    if foam.res in (32, 64, 128, 256):
+        ctx.set_jfa_staging(True)
+        staged_ms = 0.0
+        for _ in range(reps):
+            flush.fill_(1.0)
+            ctx.jfa_init(sim.pos, sim.rad, n)
+            j0.record(s)
+            ctx.jfa_passes(n)
+            j1.record(s)
+            j1.synchronize()
+            staged_ms += j0.elapsed_time(j1)
+        ctx.set_jfa_staging(False)
+    staged_us = None if staged_ms is None else round(staged_ms * 1000.0 / (reps * passes), 3)
     V = foam.res ** 3
     alg_bytes = 8.0 * V  # int32 label read + write per voxel per pass
     achieved = alg_bytes / pass_s / 1e9
@@ -537,6 +553,7 @@ def run_fos(args):
                               "traffic_source": traffic_source(traffic, tkey("k_jfa_pass_rec")),
                               "alg_bytes_per_launch": alg_bytes,
                               "pass_us": round(pass_s * 1e6, 3),
+                              "tma_staged_pass_us": staged_us,
                               "pass_us_source": "CUDA events over 8 passes + the record-grid "
                                                 "build, 10 JFA runs on the bench state",
                               "note": "27 coalesced seed-record rows per voxel; labels and "

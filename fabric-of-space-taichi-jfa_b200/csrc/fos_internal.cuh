@@ -127,6 +127,11 @@ struct FosCtx {
     int32_t* coop_bsum = nullptr;     // [1024]
     int32_t* ci_tmp = nullptr;        // [max_n]
     int use_coop = 1;                 // plain-frame dynamics as one cooperative kernel
+    // tensor maps (CUtensorMap, 128 bytes each) over recA / recB for the
+    // staged JFA pass (jfa.cu), encoded for resolution tm_res
+    unsigned char tm_rec[2][128] = {};
+    int tm_res = 0, tm_ok = 0;
+    int use_tma = 0;                  // staged record rows in the JFA pass (off: it measured slower)
     int coop_blocks = -1;             // resident blocks of the cooperative kernel (-1: not queried)
     size_t cell_tmp_n = 0;
     float* stats_f = nullptr;         // device stats scratch

@@ -9,6 +9,7 @@
 //   accumulate_face_area jfa.py:702-762 -> warp-aggregated pair table + first-touch order
 //   finalize_faces      jfa.py:788-857  -> exact fixed point of the serial hysteresis
 //   update_fsc_ema      jfa.py:765-785  -> fused into the finalize kernel
+#include <cuda.h>
 #include <math.h>
 #include <string.h>
 
@@ -92,6 +93,146 @@ __global__ void __launch_bounds__(256, UNIT_L ? 6 : 4) k_jfa_pass_rec(const int3
     if (early_exit && jfa_exited_before(ds, pass, (double)V, min_passes, th)) return;
     jfa_pass_rec_body<UNIT_L, POW2>(in, rin, out, rout, R, lgR, vs, halfL, L, step, ds->changes,
                                     pass, (long long)blockIdx.x * blockDim.x + threadIdx.x);
+}
+
+// ------------------------------------------------ pass with staged record rows
+// The same pass with the records a block needs staged in shared memory by
+// the tensor memory accelerator (cp.async.bulk.tensor, no multicast), for
+// unit L and power-of-two R in [32, 256].  A block takes TY = 256 / R
+// consecutive (x, y) rows of R voxels; every candidate of its voxels lies in
+// one of the 9 * TY whole z-rows (x + {-s, 0, s}, y + {-s, 0, s}), wrapped, so
+// each is one tile copy of R records (a tensor map over the record grid as a
+// [R][R][R][4] float array, box 1 x 1 x R x 4) and any step needs the same
+// 36,864 bytes.  The z offsets wrap inside a row.  Candidates, their order and
+// the arithmetic are those of jfa_rec_core; the winner's label is read from
+// the global label grid and its record from the staged rows.  Off by
+// default: 8 passes at 128^3 took 0.643 ms against 0.436 ms for the global
+// rows (9 at 256^3: 5.26 against 3.73 ms).  The pass is held by the L1 /
+// shared-memory data path (27 16-byte records a voxel either way) and FP32
+// issue; the staging adds 144 bytes a voxel of shared-memory writes on that
+// path and a load-then-compute bubble per block.
+#define JFA_TMA_SMEM (9 * 256 * 16)
+
+__device__ __forceinline__ unsigned int smem_addr(const void* p) {
+    return (unsigned int)__cvta_generic_to_shared(p);
+}
+
+__device__ __forceinline__ bool mbar_try_wait(unsigned int bar, unsigned int parity) {
+    unsigned int done;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+        "selp.u32 %0, 1, 0, p;\n\t}"
+        : "=r"(done)
+        : "r"(bar), "r"(parity)
+        : "memory");
+    return done != 0u;
+}
+
+// Waits for phase `parity` of the barrier for at most ~1 s of clock; false
+// (and FOS_E_TIMEOUT in the error word) when it gave up.
+__device__ __forceinline__ bool mbar_wait_bounded(unsigned int bar, unsigned int parity,
+                                                  FosDevState* ds) {
+    const long long t0 = clock64();
+    for (unsigned int it = 1;; ++it) {
+        if (mbar_try_wait(bar, parity)) return true;
+        if ((it & 63u) == 0u && clock64() - t0 > FOS_BAR_CYCLE_LIMIT) {
+            atomicCAS(&ds->error, 0, (int)FOS_E_TIMEOUT);
+            return false;
+        }
+    }
+}
+
+__global__ void __launch_bounds__(256, 6)
+    k_jfa_pass_tma(const __grid_constant__ CUtensorMap tmap, const int32_t* __restrict__ in,
+                   const float4* __restrict__ rin, int32_t* __restrict__ out,
+                   float4* __restrict__ rout, int lgR, float vs, float halfL, int step,
+                   FosDevState* ds, int pass, int early_exit, int min_passes, double th) {
+    extern __shared__ __align__(128) float4 srow[];
+    __shared__ __align__(8) unsigned long long s_bar;
+    asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
+    asm volatile("griddepcontrol.wait;" ::: "memory");
+    const int R = 1 << lgR;
+    const long long V = (long long)R * R * R;
+    if (early_exit && jfa_exited_before(ds, pass, (double)V, min_passes, th)) return;
+    const int TY = 256 >> lgR;
+    const int NR = 9 * TY;
+    const int q0 = blockIdx.x * TY;
+    const int x0 = q0 >> lgR, y0 = q0 & (R - 1);
+    const unsigned int bar = smem_addr(&s_bar);
+    if (threadIdx.x == 0) {
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(bar) : "memory");
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+        asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar),
+                     "r"((unsigned int)(NR * R * 16))
+                     : "memory");
+    }
+    __syncthreads();
+    if ((int)threadIdx.x < NR) {  // row r: x offset ix, block row ty, y offset iy
+        const int r = threadIdx.x;
+        const int ix = r / (3 * TY), rem = r - ix * 3 * TY, ty = rem / 3, iy = rem - ty * 3;
+        const int xr = (x0 + (ix - 1) * step) & (R - 1);
+        const int yr = (y0 + ty + (iy - 1) * step) & (R - 1);
+        asm volatile(
+            "cp.async.bulk.tensor.4d.shared::cluster.global.tile.mbarrier::complete_tx::bytes"
+            " [%0], [%1, {%2, %3, %4, %5}], [%6];" ::"r"(smem_addr(srow + (size_t)r * R)),
+            "l"(reinterpret_cast<unsigned long long>(&tmap)), "r"(0), "r"(0), "r"(yr), "r"(xr),
+            "r"(bar)
+            : "memory");
+    }
+    if (!mbar_wait_bounded(bar, 0u, ds)) {
+        mbar_wait_bounded(bar, 0u, ds);  // copies still in flight: give them one more bound
+        return;
+    }
+    const int ty = threadIdx.x >> lgR, z = threadIdx.x & (R - 1);
+    const int x = x0, y = y0 + ty;
+    const int l = (x << (2 * lgR)) | (y << lgR) | z;
+    int xs[3], ys[3], zs[3];
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+        const int o = (k - 1) * step;
+        xs[k] = ((x + o) & (R - 1)) << (2 * lgR);
+        ys[k] = ((y + o) & (R - 1)) << lgR;
+        zs[k] = (z + o) & (R - 1);
+    }
+    const int own = in[l];
+    const float4 orec = srow[(3 * TY + ty * 3 + 1) * R + z];
+    const float vx = voxel_centre(x, vs, halfL), vy = voxel_centre(y, vs, halfL),
+                vz = voxel_centre(z, vs, halfL);
+    const float2 vxy = make_float2(vx, vy);
+    float bd = fminf(power_dist_unit2m(vxy, vz, orec), 1e10f);
+    int bl = l, bsm = 0;
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+        float4 r[9];
+        int sm[9];
+#pragma unroll
+        for (int k = 0; k < 9; ++k) {
+            sm[k] = (a * 3 * TY + ty * 3 + k / 3) * R + zs[k % 3];
+            if (!(a == 1 && k == 4)) r[k] = srow[sm[k]];
+        }
+#pragma unroll
+        for (int k = 0; k < 9; ++k) {
+            if (a == 1 && k == 4) continue;  // the voxel itself
+            const float d = power_dist_unit2m(vxy, vz, r[k]);
+            if (d < bd) {
+                bd = d;
+                bl = xs[a] + ys[k / 3] + zs[k % 3];
+                bsm = sm[k];
+            }
+        }
+    }
+    int best = own;
+    float4 brec = orec;
+    if (bl != l) {
+        best = in[bl];
+        brec = srow[bsm];
+    }
+    out[l] = best;
+    rout[l] = brec;
+    const int cnt = __syncthreads_count(best != own);
+    if (threadIdx.x == 0 && cnt) atomicAdd(&ds->changes[pass], (unsigned long long)cnt);
 }
 
 // The record grid of a label grid: record v = seeds[label v], or NaN bits for
@@ -571,6 +712,90 @@ static cudaError_t launch_pass_rec(FosCtx* c, int p, int step, int early_exit, c
                               c->p.min_jfa_passes, c->p.th_pass_delta);
 }
 
+// cuTensorMapEncodeTiled through the runtime's driver entry point (no link
+// against libcuda).
+typedef CUresult (*EncodeTiledFn)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*,
+                                  const cuuint64_t*, const cuuint64_t*, const cuuint32_t*,
+                                  const cuuint32_t*, CUtensorMapInterleave, CUtensorMapSwizzle,
+                                  CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+
+static EncodeTiledFn encode_tiled() {
+    static const EncodeTiledFn fn = []() -> EncodeTiledFn {
+        void* p = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) !=
+                cudaSuccess ||
+            q != cudaDriverEntryPointSuccess)
+            return nullptr;
+        return (EncodeTiledFn)p;
+    }();
+    return fn;
+}
+
+static bool tma_applies(const FosCtx* c) {
+    const int R = c->res;
+    return c->use_tma && c->L == 1.0f && is_pow2(R) && R >= 32 && R <= 256;
+}
+
+// The two record grids as [R][R][R][4] float tensors, box 1 x 1 x R x 4
+// (one z-row of records), re-encoded when the resolution changes.
+static bool tma_maps(FosCtx* c) {
+    if (c->tm_res == c->res) return c->tm_ok != 0;
+    c->tm_res = c->res;
+    c->tm_ok = 0;
+    EncodeTiledFn enc = encode_tiled();
+    if (!enc) return false;
+    const cuuint64_t R = (cuuint64_t)c->res;
+    const cuuint64_t dims[4] = {4, R, R, R};
+    const cuuint64_t strides[3] = {16, 16 * R, 16 * R * R};
+    const cuuint32_t box[4] = {4, (cuuint32_t)R, 1, 1};
+    const cuuint32_t estr[4] = {1, 1, 1, 1};
+    float4* bufs[2] = {c->recA, c->recB};
+    for (int b = 0; b < 2; ++b) {
+        CUtensorMap tm;
+        if (enc(&tm, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 4, bufs[b], dims, strides, box, estr,
+                CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+                CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) !=
+            CUDA_SUCCESS)
+            return false;
+        memcpy(c->tm_rec[b], &tm, sizeof(tm));
+    }
+    static_assert(sizeof(CUtensorMap) == 128, "tensor map size");
+    c->tm_ok = 1;
+    return true;
+}
+
+static cudaError_t launch_pass_tma(FosCtx* c, int p, int step, int early_exit, cudaStream_t s) {
+    static bool attr_set = false;
+    if (!attr_set) {
+        cudaError_t e = cudaFuncSetAttribute(k_jfa_pass_tma,
+                                             cudaFuncAttributePreferredSharedMemoryCarveout,
+                                             (int)cudaSharedmemCarveoutMaxShared);
+        if (e != cudaSuccess) return e;
+        attr_set = true;
+    }
+    const int R = c->res;
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3((unsigned)(((long long)R * R * R) / 256));
+    cfg.blockDim = dim3(256);
+    cfg.dynamicSmemBytes = JFA_TMA_SMEM;
+    cfg.stream = s;
+    cudaLaunchAttribute at[1];
+    at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    at[0].val.programmaticStreamSerializationAllowed = 1;
+    cfg.attrs = at;
+    cfg.numAttrs = p > 0 ? 1 : 0;
+    const int32_t* in = (p & 1) ? c->labB : c->labA;
+    int32_t* out = (p & 1) ? c->labA : c->labB;
+    const float4* rin = (p & 1) ? c->recB : c->recA;
+    float4* rout = (p & 1) ? c->recA : c->recB;
+    CUtensorMap tm;
+    memcpy(&tm, c->tm_rec[p & 1], sizeof(tm));
+    return cudaLaunchKernelEx(&cfg, k_jfa_pass_tma, tm, in, rin, out, rout, ilog2(R), c->vs,
+                              c->halfL, step, c->ds, p, early_exit, c->p.min_jfa_passes,
+                              c->p.th_pass_delta);
+}
+
 // `npass` passes from labA, steps first_step, first_step/2, ... (never below 1).
 // The reference's scan-order tie rule runs over the record grid; the
 // lower-index tie rule (which compares labels on equal distances) runs over
@@ -586,10 +811,12 @@ static int run_passes(FosCtx* c, int first_step, int npass, int early_exit, cuda
         if (blocks > 8 * c->num_sms) blocks = 8 * c->num_sms;
         k_rec_from_labels<<<blocks, 256, 0, s>>>(c->labA, c->seeds, c->recA, V);
         FOS_LAUNCHED(c);
+        const bool tma = tma_applies(c) && tma_maps(c);
         for (int p = 0; p < npass; ++p) {
             if (step < 1) step = 1;
             cudaError_t le;
-            if (ul && p2) le = launch_pass_rec<true, true>(c, p, step, early_exit, s);
+            if (tma) le = launch_pass_tma(c, p, step, early_exit, s);
+            else if (ul && p2) le = launch_pass_rec<true, true>(c, p, step, early_exit, s);
             else if (ul) le = launch_pass_rec<true, false>(c, p, step, early_exit, s);
             else if (p2) le = launch_pass_rec<false, true>(c, p, step, early_exit, s);
             else le = launch_pass_rec<false, false>(c, p, step, early_exit, s);
@@ -788,4 +1015,12 @@ extern "C" int fos_jfa_run(FosCtx* c, const float* pos, const float* rad, int n,
     // finalize_faces_kernel + update_fsc_ema, the EMA fused into the
     // materialisation of each particle's new fsc.
     return finalize_impl(c, rad, n, true, s);
+}
+
+// Staged record rows in the JFA pass (k_jfa_pass_tma) on or off; no
+// reference counterpart.  Both give the same labels.
+extern "C" int fos_set_jfa_staging(FosCtx* c, int on) {
+    FOS_REQUIRE(c, FOS_E_ARG, "ctx is NULL");
+    c->use_tma = on ? 1 : 0;
+    return FOS_OK;
 }

@@ -223,6 +223,7 @@ SIGNATURES = {
     "fos_device_error": [_P, C.POINTER(_I), _P],
     "fos_device_error_clear": [_P, _P],
     "fos_test_barrier_plan": [_P, _I, _P],
+    "fos_set_jfa_staging": [_P, _I],
     "fos_status_string": [_I],
     "fos_last_error": [],
 }

@@ -118,6 +118,11 @@ class Context:
         ~1 ms with FOS_E_TIMEOUT; 0 turns it off."""
         call("fos_test_barrier_plan", self.h, int(leave_at_barrier), stream())
 
+    def set_jfa_staging(self, on: bool):
+        """JFA passes with record rows staged in shared memory by TMA copies, or
+        read from global memory (the default); the labels are the same."""
+        call("fos_set_jfa_staging", self.h, int(bool(on)))
+
     # ----------------------------------------------------------------- JFA
     def labels(self) -> torch.Tensor:
         """Final owner grid of the last run, [R, R, R] int32 (view)."""

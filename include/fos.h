@@ -645,6 +645,13 @@ int fos_device_error_clear(FosCtx* ctx, fos_stream_t s);
  * the other blocks record FOS_E_TIMEOUT in the error word and end.  Nothing
  * faults and nothing hangs.  0 turns the plan off (the default). */
 int fos_test_barrier_plan(FosCtx* ctx, int leave_at_barrier, fos_stream_t s);
+/* JFA passes (jfa_step_ping*, jfa.py:523-623) with the candidate record rows
+ * staged in shared memory by tensor-memory-accelerator copies (on) or read
+ * from global memory (off, the default: staging measured about 1.45x slower).
+ * Staging applies to DOMAIN_SIZE 1 and power-of-two resolutions 32..256 under
+ * the reference's tie rule; the labels are the same either way.  No
+ * reference counterpart. */
+int fos_set_jfa_staging(FosCtx* ctx, int on);
 const char* fos_status_string(int status);
 /* Thread-local text of the last error raised by any entry point. */
 const char* fos_last_error(void);

@@ -237,3 +237,36 @@ def test_unwrapped_seed_positions(shift):
     ctx.jfa_run(_dev(pos), _dev(rad), n)
     torch.cuda.synchronize()
     assert np.array_equal(ctx.labels().cpu().numpy().reshape(-1), lab)
+
+
+@pytest.mark.parametrize("R", [32, 64, 128, 256])
+def test_staged_rows_equal_global_rows(R):
+    """The pass with TMA-staged record rows (power-of-two R in 32..256) and the
+    pass reading the rows from global memory give the same labels and the
+    same per-pass change counts, with and without early exit; at R = 32 the
+    staged pass is also checked against the oracle."""
+    rng = np.random.default_rng(R)
+    n = 40 + R * 4
+    pos = wrapped(rng.random((n, 3), dtype=np.float32))
+    rad = rng.uniform(0.5, 1.5, n).astype(np.float32) / R ** 0.5 * 0.2
+    for early in (False, True):
+        cfg = FosConfig(DOMAIN_SIZE=1.0, CELL_SIZE=0.1, JFA_RES=R, JFA_RES_MIN=2, JFA_RES_MAX=R,
+                        JFA_EARLY_EXIT_ENABLED=early, MAX_PARTICLES=n)
+        out = []
+        for staged in (True, False):
+            ctx = Context(cfg, max_n=n, max_res=R)
+            ctx.set_jfa_staging(staged)
+            dpos, drad = _dev(pos), _dev(rad)
+            ctx.jfa_run(dpos, drad, n)
+            st = ctx.jfa_stats(n, drad)
+            out.append((ctx.labels().cpu().numpy().reshape(-1), st["label_changes"],
+                        st["num_passes"], ctx.fsc[:n].cpu().numpy()))
+            assert ctx.device_error() == 0
+            ctx.close()
+        assert np.array_equal(out[0][0], out[1][0])
+        assert out[0][1] == out[1][1] and out[0][2] == out[1][2]
+        assert np.array_equal(out[0][3], out[1][3])
+        if R == 32:
+            p = O.OracleParams(n=n, R=R, early_exit=early, r_max_cell=0.05)
+            lab, ch, done = O.jfa_labels(pos, rad, p)
+            assert np.array_equal(out[0][0], lab) and done == out[0][2]
