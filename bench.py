@@ -464,6 +464,13 @@ def run_fos(args):
             staged_ms += j0.elapsed_time(j1)
         ctx.set_jfa_staging(False)
     staged_us = None if staged_ms is None else round(staged_ms * 1000.0 / (reps * passes), 3)
+    # the default pass form at this size: four voxels a thread along x where
+    # R^3 / 4 threads fill the GPU (R >= 128), else one
+    multi = foam.res >= 128 and (foam.res & (foam.res - 1)) == 0
+    pass_kernel = "k_jfa_pass_recx" if multi else "k_jfa_pass_rec"
+    pass_note = ("four voxels a thread along x: 58 coalesced seed-record rows per 4 voxels"
+                 if multi else "27 coalesced seed-record rows per voxel") + \
+        "; labels and records are L2-resident at 128^3, not at 256^3"
     V = foam.res ** 3
     alg_bytes = 8.0 * V  # int32 label read + write per voxel per pass
     achieved = alg_bytes / pass_s / 1e9
@@ -539,7 +546,7 @@ def run_fos(args):
                 "d2h_bytes_per_step": n * 20},
         "roofline": coop_roof,
         "roofline_jfa_pass": {"bound": "fp32-issue",
-                              "kernel": f"k_jfa_pass_rec ({foam.res}^3, one pass)",
+                              "kernel": f"{pass_kernel} ({foam.res}^3, one pass)",
                               "achieved": round(achieved, 2), "peak": peak, "unit": "GB/s",
                               "frac": round(achieved / peak, 4),
                               "fp32": {"achieved_T_ops_per_s": round(fp32_ops / pass_s / 1e12, 2),
@@ -549,15 +556,14 @@ def run_fos(args):
                                        "peak_note": "lane operations without FMA (148 x 128 x "
                                                     "1.965 GHz); 74.4 TFLOP/s counts an FMA "
                                                     "as two"},
-                              "traffic": traffic_bytes(traffic, tkey("k_jfa_pass_rec")),
-                              "traffic_source": traffic_source(traffic, tkey("k_jfa_pass_rec")),
+                              "traffic": traffic_bytes(traffic, tkey(pass_kernel)),
+                              "traffic_source": traffic_source(traffic, tkey(pass_kernel)),
                               "alg_bytes_per_launch": alg_bytes,
                               "pass_us": round(pass_s * 1e6, 3),
                               "tma_staged_pass_us": staged_us,
                               "pass_us_source": "CUDA events over 8 passes + the record-grid "
                                                 "build, 10 JFA runs on the bench state",
-                              "note": "27 coalesced seed-record rows per voxel; labels and "
-                                      "records are L2-resident at 128^3, not at 256^3"},
+                              "note": pass_note},
         "late_run": late_run,
         "surrogate": surrogate,
         "warm_jfa": warm,

@@ -95,6 +95,86 @@ __global__ void __launch_bounds__(256, UNIT_L ? 6 : 4) k_jfa_pass_rec(const int3
                                     pass, (long long)blockIdx.x * blockDim.x + threadIdx.x);
 }
 
+// ------------------------------------------------ M voxels a thread along x
+// The record pass with M voxels a thread at x = xb, xb + s, ..., xb + (M-1)s
+// (s the step; unit L, power-of-two R >= 16, R / s >= M).  Voxel m's
+// candidates lie in the x-planes xb + (m-1)s .. xb + (m+1)s, so the thread
+// reads the 9 rows of each of M + 2 planes once and every row serves up to
+// three of its voxels: 9 (M + 2) + M record loads for M voxels instead of
+// 27 M (M = 4: 58 against 108).  Lanes run along z, so each load is still a
+// coalesced 512-byte row.  Planes are visited in increasing x and rows in
+// (dy, dz) order, so each voxel sees its own record first and then the 26
+// others in the reference's (dx, dy, dz) order, with the same arithmetic as
+// jfa_rec_core.
+template <int M>
+__global__ void __launch_bounds__(256, 4)
+    k_jfa_pass_recx(const int32_t* __restrict__ in, const float4* __restrict__ rin,
+                    int32_t* __restrict__ out, float4* __restrict__ rout, int lgR, int lgS,
+                    float vs, float halfL, FosDevState* ds, int pass, int early_exit,
+                    int min_passes, double th) {
+    asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
+    asm volatile("griddepcontrol.wait;" ::: "memory");
+    const int R = 1 << lgR, step = 1 << lgS;
+    const long long V = (long long)R * R * R;
+    if (early_exit && jfa_exited_before(ds, pass, (double)V, min_passes, th)) return;
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;  // < R^3 / M
+    const int z = t & (R - 1), y = (t >> lgR) & (R - 1), xi = t >> (2 * lgR);
+    const int xb = ((xi >> lgS) * M << lgS) + (xi & (step - 1));
+    int ys[3], zs[3], xp[M + 2];
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+        const int o = (k - 1) * step;
+        ys[k] = ((y + o) & (R - 1)) << lgR;
+        zs[k] = (z + o) & (R - 1);
+    }
+#pragma unroll
+    for (int p = 0; p < M + 2; ++p) xp[p] = ((xb + (p - 1) * step) & (R - 1)) << (2 * lgR);
+    const float vy = voxel_centre(y, vs, halfL), vz = voxel_centre(z, vs, halfL);
+    float vx[M], bd[M];
+    int bl[M], own[M];
+#pragma unroll
+    for (int m = 0; m < M; ++m) {
+        const int l = xp[m + 1] + ys[1] + zs[1];
+        vx[m] = voxel_centre(xb + m * step, vs, halfL);
+        own[m] = in[l];
+        bd[m] = fminf(power_dist_unit2m(make_float2(vx[m], vy), vz, __ldg(&rin[l])), 1e10f);
+        bl[m] = l;
+    }
+#pragma unroll
+    for (int p = 0; p < M + 2; ++p) {
+#pragma unroll
+        for (int k = 0; k < 9; ++k) {
+            // voxels m with dx = p - m - 1 in {-1, 0, 1}, less the voxel itself
+            bool used = false;
+#pragma unroll
+            for (int m = 0; m < M; ++m)
+                if (p - m >= 0 && p - m <= 2 && !(p - m == 1 && k == 4)) used = true;
+            if (!used) continue;
+            const int idx = xp[p] + ys[k / 3] + zs[k % 3];
+            const float4 r = __ldg(&rin[idx]);
+#pragma unroll
+            for (int m = 0; m < M; ++m) {
+                if (p - m < 0 || p - m > 2 || (p - m == 1 && k == 4)) continue;
+                const float d = power_dist_unit2m(make_float2(vx[m], vy), vz, r);
+                if (d < bd[m]) {
+                    bd[m] = d;
+                    bl[m] = idx;
+                }
+            }
+        }
+    }
+#pragma unroll
+    for (int m = 0; m < M; ++m) {
+        const int l = xp[m + 1] + ys[1] + zs[1];
+        int best = own[m];
+        if (bl[m] != l) best = in[bl[m]];
+        out[l] = best;
+        rout[l] = __ldg(&rin[bl[m]]);
+        const int cnt = __syncthreads_count(best != own[m]);
+        if (threadIdx.x == 0 && cnt) atomicAdd(&ds->changes[pass], (unsigned long long)cnt);
+    }
+}
+
 // ------------------------------------------------ pass with staged record rows
 // The same pass with the records a block needs staged in shared memory by
 // the tensor memory accelerator (cp.async.bulk.tensor, no multicast), for
@@ -712,6 +792,33 @@ static cudaError_t launch_pass_rec(FosCtx* c, int p, int step, int early_exit, c
                               c->p.min_jfa_passes, c->p.th_pass_delta);
 }
 
+static cudaError_t launch_pass_recx(FosCtx* c, int p, int step, int early_exit,
+                                    cudaStream_t s) {
+    const int R = c->res;
+    const int lgS = ilog2(step);
+    const int M = (R >> lgS) >= 4 ? 4 : 2;
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3((unsigned)(((long long)R * R * R / M) / 256));
+    cfg.blockDim = dim3(256);
+    cfg.stream = s;
+    cudaLaunchAttribute at[1];
+    at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    at[0].val.programmaticStreamSerializationAllowed = 1;
+    cfg.attrs = at;
+    cfg.numAttrs = p > 0 ? 1 : 0;
+    const int32_t* in = (p & 1) ? c->labB : c->labA;
+    int32_t* out = (p & 1) ? c->labA : c->labB;
+    const float4* rin = (p & 1) ? c->recB : c->recA;
+    float4* rout = (p & 1) ? c->recA : c->recB;
+    if (M == 4)
+        return cudaLaunchKernelEx(&cfg, k_jfa_pass_recx<4>, in, rin, out, rout, ilog2(R), lgS,
+                                  c->vs, c->halfL, c->ds, p, early_exit, c->p.min_jfa_passes,
+                                  c->p.th_pass_delta);
+    return cudaLaunchKernelEx(&cfg, k_jfa_pass_recx<2>, in, rin, out, rout, ilog2(R), lgS, c->vs,
+                              c->halfL, c->ds, p, early_exit, c->p.min_jfa_passes,
+                              c->p.th_pass_delta);
+}
+
 // cuTensorMapEncodeTiled through the runtime's driver entry point (no link
 // against libcuda).
 typedef CUresult (*EncodeTiledFn)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*,
@@ -812,10 +919,16 @@ static int run_passes(FosCtx* c, int first_step, int npass, int early_exit, cuda
         k_rec_from_labels<<<blocks, 256, 0, s>>>(c->labA, c->seeds, c->recA, V);
         FOS_LAUNCHED(c);
         const bool tma = tma_applies(c) && tma_maps(c);
+        // several voxels a thread where the grid still fills the GPU (at 64^3,
+        // 65k threads: 0.084 against 0.077 ms for 7 passes), or when forced
+        const bool recx = ul && p2 && R >= 16 &&
+                          (c->use_recx == 2 ||
+                           (c->use_recx == 1 && V / 4 >= (long long)c->num_sms * 1024));
         for (int p = 0; p < npass; ++p) {
             if (step < 1) step = 1;
             cudaError_t le;
             if (tma) le = launch_pass_tma(c, p, step, early_exit, s);
+            else if (recx) le = launch_pass_recx(c, p, step, early_exit, s);
             else if (ul && p2) le = launch_pass_rec<true, true>(c, p, step, early_exit, s);
             else if (ul) le = launch_pass_rec<true, false>(c, p, step, early_exit, s);
             else if (p2) le = launch_pass_rec<false, true>(c, p, step, early_exit, s);
@@ -1022,5 +1135,15 @@ extern "C" int fos_jfa_run(FosCtx* c, const float* pos, const float* rad, int n,
 extern "C" int fos_set_jfa_staging(FosCtx* c, int on) {
     FOS_REQUIRE(c, FOS_E_ARG, "ctx is NULL");
     c->use_tma = on ? 1 : 0;
+    return FOS_OK;
+}
+
+// Record pass form: 0 one voxel a thread (k_jfa_pass_rec), 1 several voxels
+// a thread along x (k_jfa_pass_recx) where R^3 / 4 threads fill the GPU, 2
+// always several; no reference counterpart.  All give the same labels.
+extern "C" int fos_set_jfa_multi_voxel(FosCtx* c, int mode) {
+    FOS_REQUIRE(c, FOS_E_ARG, "ctx is NULL");
+    FOS_REQUIRE(mode >= 0 && mode <= 2, FOS_E_ARG, "mode must be 0, 1 or 2");
+    c->use_recx = mode;
     return FOS_OK;
 }

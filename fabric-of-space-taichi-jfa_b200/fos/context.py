@@ -123,6 +123,11 @@ class Context:
         read from global memory (the default); the labels are the same."""
         call("fos_set_jfa_staging", self.h, int(bool(on)))
 
+    def set_jfa_multi_voxel(self, mode: int):
+        """JFA record passes: 0 one voxel a thread, 1 four along x where the
+        grid fills the GPU (default), 2 always four; the labels are the same."""
+        call("fos_set_jfa_multi_voxel", self.h, int(mode))
+
     # ----------------------------------------------------------------- JFA
     def labels(self) -> torch.Tensor:
         """Final owner grid of the last run, [R, R, R] int32 (view)."""

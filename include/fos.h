@@ -652,6 +652,13 @@ int fos_test_barrier_plan(FosCtx* ctx, int leave_at_barrier, fos_stream_t s);
  * the reference's tie rule; the labels are the same either way.  No
  * reference counterpart. */
 int fos_set_jfa_staging(FosCtx* ctx, int on);
+/* JFA record passes with four voxels a thread along x, sharing the candidate
+ * rows of their common x-planes, or one voxel a thread.  mode 0: one voxel a
+ * thread; 1 (the default): four where R^3 / 4 threads still fill the GPU
+ * (R >= 128 on a B200); 2: four (two at the first step) at every R >= 16.
+ * Applies to DOMAIN_SIZE 1 and power-of-two R under the reference's tie
+ * rule; the labels are the same in every mode.  No reference counterpart. */
+int fos_set_jfa_multi_voxel(FosCtx* ctx, int mode);
 const char* fos_status_string(int status);
 /* Thread-local text of the last error raised by any entry point. */
 const char* fos_last_error(void);

@@ -239,6 +239,42 @@ def test_unwrapped_seed_positions(shift):
     assert np.array_equal(ctx.labels().cpu().numpy().reshape(-1), lab)
 
 
+@pytest.mark.parametrize("R", [16, 32, 64, 128, 256])
+def test_pass_forms_agree(R):
+    """The record pass with four voxels a thread along x (forced at every R),
+    the one-voxel-a-thread pass and (R >= 32) the pass with TMA-staged rows
+    give the same labels and per-pass change counts, with and without early
+    exit; at R = 16 and 32 the four-voxel pass is also checked against the
+    oracle."""
+    rng = np.random.default_rng(R + 1)
+    n = 40 + R * 4
+    pos = wrapped(rng.random((n, 3), dtype=np.float32))
+    rad = rng.uniform(0.5, 1.5, n).astype(np.float32) / R ** 0.5 * 0.2
+    forms = [(2, False), (0, False)] + ([(0, True)] if R >= 32 else [])
+    for early in (False, True):
+        cfg = FosConfig(DOMAIN_SIZE=1.0, CELL_SIZE=0.1, JFA_RES=R, JFA_RES_MIN=2, JFA_RES_MAX=R,
+                        JFA_EARLY_EXIT_ENABLED=early, MAX_PARTICLES=n)
+        out = []
+        for multi, staged in forms:
+            ctx = Context(cfg, max_n=n, max_res=R)
+            ctx.set_jfa_multi_voxel(multi)
+            ctx.set_jfa_staging(staged)
+            drad = _dev(rad)
+            ctx.jfa_run(_dev(pos), drad, n)
+            st = ctx.jfa_stats(n, drad)
+            out.append((ctx.labels().cpu().numpy().reshape(-1), st["label_changes"],
+                        st["num_passes"]))
+            assert ctx.device_error() == 0
+            ctx.close()
+        for o in out[1:]:
+            assert np.array_equal(out[0][0], o[0]) and out[0][1] == o[1] and out[0][2] == o[2]
+        if R <= 32:
+            p = O.OracleParams(n=n, R=R, early_exit=early, r_max_cell=0.05)
+            lab, ch, done = O.jfa_labels(pos, rad, p)
+            assert np.array_equal(out[0][0], lab) and done == out[0][2]
+            assert out[0][1] == [int(c) for c in ch]
+
+
 @pytest.mark.parametrize("R", [32, 64, 128, 256])
 def test_staged_rows_equal_global_rows(R):
     """The pass with TMA-staged record rows (power-of-two R in 32..256) and the
