@@ -304,6 +304,38 @@ __device__ __forceinline__ float power_dist_unit2m(float2 vxy, float vz, float4 
     return fsub(d2, s.w);
 }
 
+// power_dist_unit2m split for voxels that share y and z (several voxels a
+// thread along x): the wrapped, squared y and z offsets of seed s once
+// (pdist_yz2m), then each voxel's x term and the sum in power_dist_unit2m's
+// order ((dx^2 + dy^2) + dz^2) - r^2, two voxels in packed pairs
+// (pdist_x2m) or one (pdist_x1m).  The same roundings in the same order, so
+// the same floats.
+__device__ __forceinline__ float2 pdist_yz2m(float2 vyz, float4 s) {
+    const float M = 12582912.0f;
+    float2 d = f2sub(vyz, make_float2(s.y, s.z));
+    const float2 t = f2sub(f2add(d, make_float2(M, M)), make_float2(M, M));
+    d = f2sub(d, t);
+    return f2mul(d, d);
+}
+
+__device__ __forceinline__ float2 pdist_x2m(float2 vx2, float2 qyz, float4 s) {
+    const float M = 12582912.0f;
+    float2 d = f2sub(vx2, make_float2(s.x, s.x));
+    const float2 t = f2sub(f2add(d, make_float2(M, M)), make_float2(M, M));
+    d = f2sub(d, t);
+    const float2 a = f2add(f2mul(d, d), make_float2(qyz.x, qyz.x));
+    const float2 b = f2add(a, make_float2(qyz.y, qyz.y));
+    return f2sub(b, make_float2(s.w, s.w));
+}
+
+__device__ __forceinline__ float pdist_x1m(float vx, float2 qyz, float4 s) {
+    const float M = 12582912.0f;
+    float d = fsub(vx, s.x);
+    const float t = fsub(fadd(d, M), M);
+    d = fsub(d, t);
+    return fsub(fadd(fadd(fmul(d, d), qyz.x), qyz.y), s.w);
+}
+
 // voxel_to_world (jfa.py:273-287)
 __device__ __forceinline__ float voxel_centre(int idx, float vs, float halfL) {
     return fsub(fmul(fadd((float)idx, 0.5f), vs), halfL);

@@ -152,13 +152,28 @@ __global__ void __launch_bounds__(256, 4)
             if (!used) continue;
             const int idx = xp[p] + ys[k / 3] + zs[k % 3];
             const float4 r = __ldg(&rin[idx]);
+            // the voxels this row serves (at most three), y and z terms once,
+            // the x terms of two voxels in a packed pair
+            int vm[3] = {0, 0, 0}, nv = 0;
 #pragma unroll
-            for (int m = 0; m < M; ++m) {
-                if (p - m < 0 || p - m > 2 || (p - m == 1 && k == 4)) continue;
-                const float d = power_dist_unit2m(make_float2(vx[m], vy), vz, r);
-                if (d < bd[m]) {
-                    bd[m] = d;
-                    bl[m] = idx;
+            for (int m = 0; m < M; ++m)
+                if (p - m >= 0 && p - m <= 2 && !(p - m == 1 && k == 4)) vm[nv++] = m;
+            const float2 qyz = pdist_yz2m(make_float2(vy, vz), r);
+            float dv[3];
+            if (nv >= 2) {
+                const float2 d2 = pdist_x2m(make_float2(vx[vm[0]], vx[vm[1]]), qyz, r);
+                dv[0] = d2.x;
+                dv[1] = d2.y;
+                if (nv == 3) dv[2] = pdist_x1m(vx[vm[2]], qyz, r);
+            } else {
+                dv[0] = pdist_x1m(vx[vm[0]], qyz, r);
+            }
+#pragma unroll
+            for (int q = 0; q < 3; ++q) {
+                if (q >= nv) break;
+                if (dv[q] < bd[vm[q]]) {
+                    bd[vm[q]] = dv[q];
+                    bl[vm[q]] = idx;
                 }
             }
         }
