@@ -78,6 +78,16 @@ struct FosEnsemble {
     uint2* ou_key = nullptr;
     int32_t* ou_base = nullptr;
     FosEnsembleTuning tune{256, 256, 1024, 1};
+    // runs of the four-voxel record pass (k_ens_jfa_pass_recx): per pass, the
+    // foams that take M voxels a thread, with their thread offsets
+    struct Run {
+        int pass, M, nr;
+        long long foam_base, to_base, threads;
+    };
+    std::vector<Run> runs;
+    int32_t* drfoam = nullptr;
+    long long* drto = nullptr;
+    int multi_voxel = 1;
     cudaGraphExec_t gexec[2] = {nullptr, nullptr};
     bool gvalid[2] = {false, false};
     FosEnsembleTuning gtune[2];
@@ -223,6 +233,71 @@ __global__ void __launch_bounds__(512, UNIT_L ? 3 : 2)
     const long long lin = v0 + threadIdx.x - d.vox_off;
     jfa_pass_rec_body_any<UNIT_L>(in, rin, out, rout, d.R, d.lgR, d.pow2, d.vs, halfL, L, step,
                                   W[f].changes, pass, lin);
+}
+
+// The four-voxel record pass (recx_scan) over the packed grids, unit L.
+// One launch covers the foams of one run: those whose pass `pass` takes M
+// voxels a thread (M = 4 where R is a multiple of 4s, 2 where it is a multiple
+// of 2s, else 1; s the foam's step).  Run foam j's threads start at rto[j]
+// (multiples of 256, so a block stays in one foam), R^3 / M of them; a thread
+// takes x = xb + m s (m < M) at one (y, z), xb = (xi / s) M s + xi % s.
+template <int M>
+__global__ void __launch_bounds__(256, 4)
+    k_ens_jfa_pass_recx(const long long* __restrict__ rto, const int32_t* __restrict__ rfoam,
+                        int nr, const EnsFoamDev* __restrict__ F, int32_t* __restrict__ labA,
+                        int32_t* __restrict__ labB, float4* __restrict__ recA,
+                        float4* __restrict__ recB, float halfL, EnsWords* W, int pass) {
+    const long long t0 = (long long)blockIdx.x * blockDim.x;
+    const int j = ens_vox_foam(rto, nr, t0);
+    const int f = __ldg(&rfoam[j]);
+    const EnsFoamDev d = F[f];
+    const int R = d.R;
+    int step = (R / 2) >> pass;
+    if (step < 1) step = 1;
+    const int32_t* in = ((pass & 1) ? labB : labA) + d.vox_off;
+    int32_t* out = ((pass & 1) ? labA : labB) + d.vox_off;
+    const float4* rin = ((pass & 1) ? recB : recA) + d.vox_off;
+    float4* rout = ((pass & 1) ? recA : recB) + d.vox_off;
+    const long long V = (long long)R * R * R;
+    const long long tl = t0 + threadIdx.x - rto[j];
+    const bool live = tl < V / M;
+    const int tt = live ? (int)tl : 0;
+    const int z = tt % R, yz = tt / R, y = yz % R, xi = yz / R;
+    const int g = xi / step;
+    const int xb = g * M * step + (xi - g * step);
+    int ys[3], zs[3], xp[M + 2];
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+        const int o = (k - 1) * step;
+        ys[k] = wrap_small(y + o, R) * R;
+        zs[k] = wrap_small(z + o, R);
+    }
+#pragma unroll
+    for (int p = 0; p < M + 2; ++p) xp[p] = wrap_small(xb + (p - 1) * step, R) * R * R;
+    const float vy = voxel_centre(y, d.vs, halfL), vz = voxel_centre(z, d.vs, halfL);
+    float vx[M], bd[M];
+    int bl[M], own[M];
+#pragma unroll
+    for (int m = 0; m < M; ++m) {
+        const int l = xp[m + 1] + ys[1] + zs[1];
+        vx[m] = voxel_centre(xb + m * step, d.vs, halfL);
+        own[m] = in[l];
+        bd[m] = fminf(power_dist_unit2m(make_float2(vx[m], vy), vz, __ldg(&rin[l])), 1e10f);
+        bl[m] = l;
+    }
+    recx_scan<M>(rin, xp, ys, zs, vx, vy, vz, bd, bl);
+#pragma unroll
+    for (int m = 0; m < M; ++m) {
+        const int l = xp[m + 1] + ys[1] + zs[1];
+        int best = own[m];
+        if (bl[m] != l) best = in[bl[m]];
+        if (live) {
+            out[l] = best;
+            rout[l] = __ldg(&rin[bl[m]]);
+        }
+        const int cnt = __syncthreads_count(live && best != own[m]);
+        if (threadIdx.x == 0 && cnt) atomicAdd(&W[f].changes[pass], (unsigned long long)cnt);
+    }
 }
 
 // Records of the packed label grids (seeds[label], NaN bits when unassigned).
@@ -557,7 +632,7 @@ extern "C" int fos_ensemble_destroy(FosEnsemble* e) {
                     e->recA, e->recB,
                     e->slot, e->seedlin, e->pos,   e->rad,     e->rad_target, e->lmd,
                     e->delta_r, e->cc, e->cs,      e->ci,      e->vjit, e->ou_kick, e->ou_key,
-                    e->ou_base};
+                    e->ou_base, e->drfoam, e->drto};
     for (void* q : ptrs)
         if (q) cudaFree(q);
     if (e->c) fos_ctx_destroy(e->c);
@@ -622,6 +697,40 @@ static int ens_create_impl(FosEnsemble* e, const FosEnsembleFoam* foams) {
     e->vtot = vtot;
     e->g3tot = (int)g3;
     e->max_passes = maxp;
+    {
+        // runs of the four-voxel pass: foam f's step at pass q is
+        // max(1, (R/2) >> q); M = 4 where R is a multiple of 4 steps, 2 where
+        // it is a multiple of 2, else 1
+        std::vector<int32_t> rf;
+        std::vector<long long> rt;
+        for (int q = 0; q < maxp; ++q)
+            for (int M : {4, 2, 1}) {
+                FosEnsemble::Run run{q, M, 0, (long long)rf.size(), (long long)rt.size(), 0};
+                long long off = 0;
+                for (int f = 0; f < nf; ++f) {
+                    const EnsFoamDev& d = e->hf[f];
+                    if (q >= d.passes) continue;
+                    int st = (d.R / 2) >> q;
+                    if (st < 1) st = 1;
+                    const int m = d.R % (4 * st) == 0 ? 4 : d.R % (2 * st) == 0 ? 2 : 1;
+                    if (m != M) continue;
+                    rf.push_back(f);
+                    rt.push_back(off);
+                    const long long T = (long long)d.R * d.R * d.R / M;
+                    off += (T + 255) / 256 * 256;
+                    ++run.nr;
+                }
+                if (!run.nr) continue;
+                rt.push_back(off);
+                run.threads = off;
+                e->runs.push_back(run);
+            }
+        FOS_CUDA(cudaMalloc(&e->drfoam, rf.size() * 4));
+        FOS_CUDA(cudaMalloc(&e->drto, rt.size() * sizeof(long long)));
+        FOS_CUDA(cudaMemcpy(e->drfoam, rf.data(), rf.size() * 4, cudaMemcpyHostToDevice));
+        FOS_CUDA(cudaMemcpy(e->drto, rt.data(), rt.size() * sizeof(long long),
+                            cudaMemcpyHostToDevice));
+    }
     // internal context for the packed particle-level buffers: its cell
     // scratch must hold the packed cell table, its own voxel grid is unused
     FosParams cp = e->p;
@@ -945,6 +1054,27 @@ static int ens_seed_passes(FosEnsemble* e, cudaStream_t s) {
         if (rb > 8 * c->num_sms) rb = 8 * c->num_sms;
         k_ens_rec_from_labels<<<rb, 256, 0, s>>>(e->labA, c->seeds, e->recA, e->vtot);
         FOS_LAUNCHED(c);
+        if (ul && e->multi_voxel) {
+            for (const FosEnsemble::Run& r : e->runs) {
+                const unsigned grid = (unsigned)(r.threads / 256);
+                const long long* to = e->drto + r.to_base;
+                const int32_t* rf = e->drfoam + r.foam_base;
+                if (r.M == 4)
+                    k_ens_jfa_pass_recx<4><<<grid, 256, 0, s>>>(to, rf, r.nr, e->df, e->labA,
+                                                                e->labB, e->recA, e->recB,
+                                                                c->halfL, e->dw, r.pass);
+                else if (r.M == 2)
+                    k_ens_jfa_pass_recx<2><<<grid, 256, 0, s>>>(to, rf, r.nr, e->df, e->labA,
+                                                                e->labB, e->recA, e->recB,
+                                                                c->halfL, e->dw, r.pass);
+                else
+                    k_ens_jfa_pass_recx<1><<<grid, 256, 0, s>>>(to, rf, r.nr, e->df, e->labA,
+                                                                e->labB, e->recA, e->recB,
+                                                                c->halfL, e->dw, r.pass);
+                FOS_LAUNCHED(c);
+            }
+            return FOS_OK;
+        }
         for (int p = 0; p < e->max_passes; ++p) {
             if (ul)
                 k_ens_jfa_pass_rec<true><<<pgrid, pb, 0, s>>>(e->dvo, e->nf, e->df, e->labA,
@@ -1240,5 +1370,14 @@ extern "C" int fos_ensemble_autotune(FosEnsemble* e, int reps, FosEnsembleTuning
     if (best) *best = t;
     if (report_ms)
         for (int k = 0; k < report_cap && k < (int)rep.size(); ++k) report_ms[k] = rep[k];
+    return FOS_OK;
+}
+
+// Record passes of the batched ensemble with four voxels a thread (on, the
+// default) or one; no reference counterpart.  Both give the same labels.
+extern "C" int fos_ensemble_set_multi_voxel(FosEnsemble* e, int on) {
+    FOS_REQUIRE(e, FOS_E_ARG, "ensemble is NULL");
+    e->multi_voxel = on ? 1 : 0;
+    e->gvalid[0] = e->gvalid[1] = false;  // the graphs are recaptured on next use
     return FOS_OK;
 }

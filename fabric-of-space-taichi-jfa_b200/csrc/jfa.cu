@@ -140,44 +140,7 @@ __global__ void __launch_bounds__(256, 4)
         bd[m] = fminf(power_dist_unit2m(make_float2(vx[m], vy), vz, __ldg(&rin[l])), 1e10f);
         bl[m] = l;
     }
-#pragma unroll
-    for (int p = 0; p < M + 2; ++p) {
-#pragma unroll
-        for (int k = 0; k < 9; ++k) {
-            // voxels m with dx = p - m - 1 in {-1, 0, 1}, less the voxel itself
-            bool used = false;
-#pragma unroll
-            for (int m = 0; m < M; ++m)
-                if (p - m >= 0 && p - m <= 2 && !(p - m == 1 && k == 4)) used = true;
-            if (!used) continue;
-            const int idx = xp[p] + ys[k / 3] + zs[k % 3];
-            const float4 r = __ldg(&rin[idx]);
-            // the voxels this row serves (at most three), y and z terms once,
-            // the x terms of two voxels in a packed pair
-            int vm[3] = {0, 0, 0}, nv = 0;
-#pragma unroll
-            for (int m = 0; m < M; ++m)
-                if (p - m >= 0 && p - m <= 2 && !(p - m == 1 && k == 4)) vm[nv++] = m;
-            const float2 qyz = pdist_yz2m(make_float2(vy, vz), r);
-            float dv[3];
-            if (nv >= 2) {
-                const float2 d2 = pdist_x2m(make_float2(vx[vm[0]], vx[vm[1]]), qyz, r);
-                dv[0] = d2.x;
-                dv[1] = d2.y;
-                if (nv == 3) dv[2] = pdist_x1m(vx[vm[2]], qyz, r);
-            } else {
-                dv[0] = pdist_x1m(vx[vm[0]], qyz, r);
-            }
-#pragma unroll
-            for (int q = 0; q < 3; ++q) {
-                if (q >= nv) break;
-                if (dv[q] < bd[vm[q]]) {
-                    bd[vm[q]] = dv[q];
-                    bl[vm[q]] = idx;
-                }
-            }
-        }
-    }
+    recx_scan<M>(rin, xp, ys, zs, vx, vy, vz, bd, bl);
 #pragma unroll
     for (int m = 0; m < M; ++m) {
         const int l = xp[m + 1] + ys[1] + zs[1];

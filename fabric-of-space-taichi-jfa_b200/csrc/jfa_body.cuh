@@ -290,6 +290,58 @@ __device__ __forceinline__ void jfa_pass_rec_body_any(const int32_t* __restrict_
                          ys, zs);
 }
 
+// The candidate scan of M voxels at x-planes 1..M of xp[] (offsets of the
+// M + 2 planes, y rows ys[], z offsets zs[]) that share y and z: the 9 rows of
+// each plane are read once, in increasing plane and (dy, dz) order, and each
+// row updates the voxels it serves (dx = plane - m - 1 in {-1, 0, 1}, less
+// the voxel itself) with power_dist_unit2m's floats (pdist_yz2m once per
+// row, pdist_x2m / pdist_x1m per voxel).  bd / bl hold each voxel's best
+// distance and voxel index, started from its own record.
+template <int M>
+__device__ __forceinline__ void recx_scan(const float4* __restrict__ rin, const int (&xp)[M + 2],
+                                          const int (&ys)[3], const int (&zs)[3],
+                                          const float (&vx)[M], float vy, float vz,
+                                          float (&bd)[M], int (&bl)[M]) {
+#pragma unroll
+    for (int p = 0; p < M + 2; ++p) {
+#pragma unroll
+        for (int k = 0; k < 9; ++k) {
+            // voxels m with dx = p - m - 1 in {-1, 0, 1}, less the voxel itself
+            bool used = false;
+#pragma unroll
+            for (int m = 0; m < M; ++m)
+                if (p - m >= 0 && p - m <= 2 && !(p - m == 1 && k == 4)) used = true;
+            if (!used) continue;
+            const int idx = xp[p] + ys[k / 3] + zs[k % 3];
+            const float4 r = __ldg(&rin[idx]);
+            // the voxels this row serves (at most three), y and z terms once,
+            // the x terms of two voxels in a packed pair
+            int vm[3] = {0, 0, 0}, nv = 0;
+#pragma unroll
+            for (int m = 0; m < M; ++m)
+                if (p - m >= 0 && p - m <= 2 && !(p - m == 1 && k == 4)) vm[nv++] = m;
+            const float2 qyz = pdist_yz2m(make_float2(vy, vz), r);
+            float dv[3];
+            if (nv >= 2) {
+                const float2 d2 = pdist_x2m(make_float2(vx[vm[0]], vx[vm[1]]), qyz, r);
+                dv[0] = d2.x;
+                dv[1] = d2.y;
+                if (nv == 3) dv[2] = pdist_x1m(vx[vm[2]], qyz, r);
+            } else {
+                dv[0] = pdist_x1m(vx[vm[0]], qyz, r);
+            }
+#pragma unroll
+            for (int q = 0; q < 3; ++q) {
+                if (q >= nv) break;
+                if (dv[q] < bd[vm[q]]) {
+                    bd[vm[q]] = dv[q];
+                    bl[vm[q]] = idx;
+                }
+            }
+        }
+    }
+}
+
 // Voxel coordinates of linear index l (z fastest) in 32-bit arithmetic
 // (R <= 512, so R^3 < 2^31): shifts for a power-of-two R, else divisions.
 __device__ __forceinline__ void vox_xyz(int l, int R, int& x, int& y, int& z) {

@@ -191,6 +191,11 @@ class Ensemble:
         t = FosEnsembleTuning(**{k: int(d[k]) for k, _ in FosEnsembleTuning._fields_})
         call("fos_ensemble_set_tuning", self.h, C.byref(t))
 
+    def set_multi_voxel(self, on: bool):
+        """Record passes with four voxels a thread (default) or one; the labels
+        are the same."""
+        call("fos_ensemble_set_multi_voxel", self.h, int(bool(on)))
+
     def signature(self) -> str:
         """Device name + shape of the ensemble (counts, JFA res, hash res)."""
         shape = [(f.n, c.JFA_RES, c.grid_res()) for f, c in zip(self.foams, self.cfgs)]

@@ -615,6 +615,11 @@ int fos_ensemble_frame(FosEnsemble* e, int jfa_frame, fos_stream_t s);
 int fos_ensemble_frame_graph(FosEnsemble* e, int jfa_frame, fos_stream_t s);
 int fos_ensemble_set_tuning(FosEnsemble* e, const FosEnsembleTuning* t);
 int fos_ensemble_get_tuning(FosEnsemble* e, FosEnsembleTuning* t);
+/* Record passes with four voxels a thread along x where a foam's R allows it
+ * (on, the default; the pass block of the tuning then does not apply), or
+ * one voxel a thread (off).  DOMAIN_SIZE 1 only; the labels are the same
+ * either way.  No reference counterpart. */
+int fos_ensemble_set_multi_voxel(FosEnsemble* e, int on);
 /* Times every candidate shape of each tuned stage on the current state (the
  * JFA stages on this state's positions, the dynamics from a snapshot that is
  * restored afterwards), keeps the fastest per stage and applies it.
