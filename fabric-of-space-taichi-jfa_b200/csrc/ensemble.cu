@@ -88,6 +88,9 @@ struct FosEnsemble {
     int32_t* drfoam = nullptr;
     long long* drto = nullptr;
     int multi_voxel = 1;
+    // per-foam hash-grid side, first cell and radius bound (surrogate pairs)
+    int32_t *dfG = nullptr, *dfcell = nullptr;
+    float* dfrmax = nullptr;
     cudaGraphExec_t gexec[2] = {nullptr, nullptr};
     bool gvalid[2] = {false, false};
     FosEnsembleTuning gtune[2];
@@ -632,7 +635,7 @@ extern "C" int fos_ensemble_destroy(FosEnsemble* e) {
                     e->recA, e->recB,
                     e->slot, e->seedlin, e->pos,   e->rad,     e->rad_target, e->lmd,
                     e->delta_r, e->cc, e->cs,      e->ci,      e->vjit, e->ou_kick, e->ou_key,
-                    e->ou_base, e->drfoam, e->drto};
+                    e->ou_base, e->drfoam, e->drto, e->dfG, e->dfcell, e->dfrmax};
     for (void* q : ptrs)
         if (q) cudaFree(q);
     if (e->c) fos_ctx_destroy(e->c);
@@ -730,6 +733,19 @@ static int ens_create_impl(FosEnsemble* e, const FosEnsembleFoam* foams) {
         FOS_CUDA(cudaMemcpy(e->drfoam, rf.data(), rf.size() * 4, cudaMemcpyHostToDevice));
         FOS_CUDA(cudaMemcpy(e->drto, rt.data(), rt.size() * sizeof(long long),
                             cudaMemcpyHostToDevice));
+        std::vector<int32_t> fg(nf), fc(nf);
+        std::vector<float> fr(nf);
+        for (int f = 0; f < nf; ++f) {
+            fg[f] = e->hf[f].G;
+            fc[f] = e->hf[f].cell_off;
+            fr[f] = e->hf[f].r_max;
+        }
+        FOS_CUDA(cudaMalloc(&e->dfG, nf * 4));
+        FOS_CUDA(cudaMalloc(&e->dfcell, nf * 4));
+        FOS_CUDA(cudaMalloc(&e->dfrmax, nf * 4));
+        FOS_CUDA(cudaMemcpy(e->dfG, fg.data(), nf * 4, cudaMemcpyHostToDevice));
+        FOS_CUDA(cudaMemcpy(e->dfcell, fc.data(), nf * 4, cudaMemcpyHostToDevice));
+        FOS_CUDA(cudaMemcpy(e->dfrmax, fr.data(), nf * 4, cudaMemcpyHostToDevice));
     }
     // internal context for the packed particle-level buffers: its cell
     // scratch must hold the packed cell table, its own voxel grid is unused
@@ -1203,6 +1219,60 @@ extern "C" int fos_ensemble_frame(FosEnsemble* e, int jfa_frame, fos_stream_t s_
     k_frame_end<<<1, 1, 0, s>>>(e->c->ds);
     FOS_LAUNCHED(e->c);
     return FOS_OK;
+}
+
+// A frame of every foam with the learned FSC surrogate (fos_frame_surrogate's
+// order per foam): the dynamics, then on a non-JFA frame the surrogate's FSC,
+// its EMA and the targets from it; on a JFA frame the surrogate's estimate
+// for the same positions, the JFA and its targets, then the judging.  Pairs
+// are searched on each foam's own grid, so each foam's FSC is the one the
+// same foam gets alone.  No reference counterpart.
+extern "C" int fos_ensemble_frame_surrogate(FosEnsemble* e, const FosSurrogate* m, int jfa_frame,
+                                            fos_stream_t s_) {
+    FOS_REQUIRE(e != nullptr && m != nullptr, FOS_E_ARG, "ensemble or surrogate model is NULL");
+    cudaStream_t s = (cudaStream_t)s_;
+    FosCtx* c = e->c;
+    int rc = ens_kernel_attributes();
+    if (rc) return rc;
+    rc = fos_sur_prepare(c);
+    if (rc) return rc;
+    rc = ens_coop_launch(e, 0, s);
+    if (rc) return rc;
+    const SurEnsGrid g{e->ntot, e->pos,     e->rad, e->cs,     e->cc,
+                       e->ci,   e->foam_of, e->dfG, e->dfcell, e->dfrmax};
+    if (!jfa_frame) {
+        rc = fos_sur_ens_between(c, m, g, s);
+        if (rc) return rc;
+        const FosFrameParams* fp = &e->fp;
+        k_ens_targets<<<fos_blocks(e->ntot, 256), 256, 0, s>>>(
+            e->ntot, e->df, e->foam_of, e->dw, c->ds, e->rad, e->rad_target, fos_sur_fsc_int(c),
+            c->ema, (float)fp->growth_pct, c->deadband, fp->warmstart_frames,
+            fp->zero_rate_thresh, fp->adjustment_frames);
+        FOS_LAUNCHED(c);
+    } else {
+        rc = fos_sur_ens_before_jfa(c, m, g, s);
+        if (rc) return rc;
+        rc = ens_jfa(e, s);
+        if (rc) return rc;
+        rc = fos_sur_frame_judge(c, e->ntot, s);
+        if (rc) return rc;
+    }
+    k_frame_end<<<1, 1, 0, s>>>(c->ds);
+    FOS_LAUNCHED(c);
+    return FOS_OK;
+}
+
+// The surrogate mode (FOS_SUR_ABSOLUTE / FOS_SUR_ANCHORED) and the counters
+// of the last pair build and judged JFA frame, over all foams.
+extern "C" int fos_ensemble_surrogate_mode(FosEnsemble* e, int mode) {
+    FOS_REQUIRE(e != nullptr, FOS_E_ARG, "ensemble is NULL");
+    return fos_surrogate_set_mode(e->c, mode);
+}
+
+extern "C" int fos_ensemble_surrogate_stats(FosEnsemble* e, FosSurrogateStats* out,
+                                            fos_stream_t s) {
+    FOS_REQUIRE(e != nullptr, FOS_E_ARG, "ensemble is NULL");
+    return fos_surrogate_stats(e->c, out, s);
 }
 
 extern "C" int fos_ensemble_frame_graph(FosEnsemble* e, int jfa_frame, fos_stream_t s_) {

@@ -62,6 +62,20 @@ struct FosGraphKey {
 
 struct FosSurBufs;  // surrogate.cu
 
+// A batched ensemble's packed grid as the surrogate's pair search sees it.
+struct SurEnsGrid {
+    int n;
+    const float* pos;
+    const float* rad;
+    const int32_t* cs;
+    const int32_t* cc;
+    const int32_t* ci;
+    const int32_t* foam_of;
+    const int32_t* fG;     // [nf] hash-grid cells a side
+    const int32_t* fcell;  // [nf] first cell in the packed table
+    const float* frmax;    // [nf] radius bound
+};
+
 #define FOS_SKIP_BLOCKS 1024
 #define FOS_PTAG_MAX_N 32768  // particles the tagged pressure words are allocated for
 #define FOS_PTAG_SWEEPS 64    // most sweeps they hold (one word per particle and sweep)
@@ -193,6 +207,9 @@ int fos_sur_frame_before_jfa(FosCtx* c, const FosSurrogate* m, const FosState* s
 int fos_sur_frame_judge(FosCtx* c, int n, cudaStream_t s);
 int fos_sur_frame_between(FosCtx* c, const FosSurrogate* m, const FosState* st,
                           const FosFrameParams* fp, cudaStream_t s);
+int fos_sur_ens_between(FosCtx* c, const FosSurrogate* m, const SurEnsGrid& g, cudaStream_t s);
+int fos_sur_ens_before_jfa(FosCtx* c, const FosSurrogate* m, const SurEnsGrid& g, cudaStream_t s);
+const int32_t* fos_sur_fsc_int(FosCtx* c);
 // end_frame: the kernel is the frame's last one and advances the frame counter
 // itself (k_frame_end's job).
 int fos_frame_coop_dynamics(FosCtx* c, const FosState* st, const FosFrameParams* fp,

@@ -96,18 +96,19 @@ enum SurCnt {
 };
 
 // ------------------------------------------------------------ pair search
-__global__ void __launch_bounds__(256) k_sur_pairs(const float4* __restrict__ sp,
-                                                   const int32_t* __restrict__ ci, int n, GridGeom g,
-                                                   const int32_t* __restrict__ cs,
-                                                   const int32_t* __restrict__ cc, float cutoff,
-                                                   float r_max, int32_t* __restrict__ pj,
-                                                   float* __restrict__ pnd,
-                                                   int32_t* __restrict__ pcount,
-                                                   int32_t* __restrict__ hist,
-                                                   unsigned long long* __restrict__ counters) {
-    const int kk = (int)(((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5);
-    const int lane = threadIdx.x & 31;
-    if (kk >= n) return;  // warp-uniform
+// The candidates of the particle at cell-ordered slot kk (one warp): g, cs
+// and cc describe the hash grid the particle lives in (a batched ensemble
+// passes its foam's grid: cs / cc at the foam's cell offset, whose entries
+// are slots of the packed cell-ordered arrays), r_max that grid's radius bound.
+__device__ __forceinline__ void sur_pairs_warp(int kk, int lane, const float4* __restrict__ sp,
+                                               const int32_t* __restrict__ ci, const GridGeom g,
+                                               const int32_t* __restrict__ cs,
+                                               const int32_t* __restrict__ cc, float cutoff,
+                                               float r_max, int32_t* __restrict__ pj,
+                                               float* __restrict__ pnd,
+                                               int32_t* __restrict__ pcount,
+                                               int32_t* __restrict__ hist,
+                                               unsigned long long* __restrict__ counters) {
     const float4 me = sp[kk];
     const int i = ci[kk];
     const int G = g.G;
@@ -218,6 +219,41 @@ __global__ void __launch_bounds__(256) k_sur_pairs(const float4* __restrict__ sp
         pcount[i] = cnt < SUR_CAP ? cnt : SUR_CAP;
         if (cnt > SUR_CAP) atomicAdd(&counters[SC_OVERFLOW], 1ull);
     }
+}
+
+__global__ void __launch_bounds__(256) k_sur_pairs(const float4* __restrict__ sp,
+                                                   const int32_t* __restrict__ ci, int n, GridGeom g,
+                                                   const int32_t* __restrict__ cs,
+                                                   const int32_t* __restrict__ cc, float cutoff,
+                                                   float r_max, int32_t* __restrict__ pj,
+                                                   float* __restrict__ pnd,
+                                                   int32_t* __restrict__ pcount,
+                                                   int32_t* __restrict__ hist,
+                                                   unsigned long long* __restrict__ counters) {
+    const int kk = (int)(((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5);
+    if (kk >= n) return;  // warp-uniform
+    sur_pairs_warp(kk, threadIdx.x & 31, sp, ci, g, cs, cc, cutoff, r_max, pj, pnd, pcount, hist,
+                   counters);
+}
+
+// The same over a batched ensemble's packed grid: particle i of foam f =
+// foam_of[i] searches foam f's hash grid (fG[f] cells a side, its cell
+// table at fcell[f]) with foam f's radius bound frmax[f].  Pairs never cross
+// foams, since each grid holds only its foam's particles.
+__global__ void __launch_bounds__(256) k_sur_pairs_ens(
+    const float4* __restrict__ sp, const int32_t* __restrict__ ci, int n, float L, float invL,
+    float halfL, const int32_t* __restrict__ foam_of, const int32_t* __restrict__ fG,
+    const int32_t* __restrict__ fcell, const float* __restrict__ frmax,
+    const int32_t* __restrict__ cs, const int32_t* __restrict__ cc, float cutoff,
+    int32_t* __restrict__ pj, float* __restrict__ pnd, int32_t* __restrict__ pcount,
+    int32_t* __restrict__ hist, unsigned long long* __restrict__ counters) {
+    const int kk = (int)(((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5);
+    if (kk >= n) return;  // warp-uniform
+    const int f = __ldg(&foam_of[__ldg(&ci[kk])]);
+    const GridGeom g{__ldg(&fG[f]), L, invL, halfL};
+    const int off = __ldg(&fcell[f]);
+    sur_pairs_warp(kk, threadIdx.x & 31, sp, ci, g, cs + off, cc + off, cutoff, __ldg(&frmax[f]),
+                   pj, pnd, pcount, hist, counters);
 }
 
 // The 16 raw features of pair (i, j) at normalised distance nd; hi and hj
@@ -1261,3 +1297,57 @@ int fos_sur_frame_between(FosCtx* c, const FosSurrogate* m, const FosState* st,
                                   (float)fp->r_max, c->ds, fp->warmstart_frames,
                                   fp->zero_rate_thresh, fp->adjustment_frames, s);
 }
+
+// ------------------------------------------------------------ ensemble hooks
+// The surrogate over a batched ensemble's packed particles (ensemble.cu):
+// candidate pairs on each foam's own hash grid (k_sur_pairs_ens), then the
+// inference and the per-particle steps of the single-foam hooks above, which
+// do not depend on which foam a particle belongs to.
+static int sur_ens_pairs_predict(FosCtx* c, const FosSurrogate* m, const SurEnsGrid& g,
+                                 cudaStream_t s) {
+    int rc = fos_sur_prepare(c);
+    if (rc) return rc;
+    FosSurBufs* b = c->sur;
+    rc = fos_grid_gather_sorted(c, g.ci, g.pos, g.rad, g.n, s);
+    if (rc) return rc;
+    FOS_CUDA(cudaMemsetAsync(b->cnt + SC_OVERFLOW, 0, 8, s));
+    k_sur_pairs_ens<<<fos_blocks(32LL * g.n, 256), 256, 0, s>>>(
+        c->sorted, g.ci, g.n, c->L, c->invL, c->halfL, g.foam_of, g.fG, g.fcell, g.frmax, g.cs,
+        g.cc, m->cutoff, b->pj, b->pnd, b->pcount, b->hist, b->cnt);
+    FOS_LAUNCHED(c);
+    b->n = g.n;
+    b->cutoff = m->cutoff;
+    return sur_predict_impl(c, m, g.rad, nullptr, nullptr, nullptr, s);
+}
+
+// A non-JFA frame: the mode's FSC f and fsc_ema <- alpha f + (1 - alpha)
+// fsc_ema; the caller sets the targets from fos_sur_fsc_int(c).
+int fos_sur_ens_between(FosCtx* c, const FosSurrogate* m, const SurEnsGrid& g, cudaStream_t s) {
+    int rc = sur_ens_pairs_predict(c, m, g, s);
+    if (rc) return rc;
+    FosSurBufs* b = c->sur;
+    k_sur_combine<<<fos_blocks(g.n, 256), 256, 0, s>>>(g.n, c->sur_mode, b->raw, c->fsc,
+                                                       b->anchor, b->anchor_valid, b->fscf,
+                                                       b->fsci);
+    FOS_LAUNCHED(c);
+    k_sur_ema<<<fos_blocks(g.n, 256), 256, 0, s>>>(g.n, b->fscf, c->ema, c->ema_alpha);
+    FOS_LAUNCHED(c);
+    return FOS_OK;
+}
+
+// A JFA frame: the estimate for the same positions and the stale baseline,
+// judged by fos_sur_frame_judge after the JFA.
+int fos_sur_ens_before_jfa(FosCtx* c, const FosSurrogate* m, const SurEnsGrid& g,
+                           cudaStream_t s) {
+    int rc = sur_ens_pairs_predict(c, m, g, s);
+    if (rc) return rc;
+    FosSurBufs* b = c->sur;
+    FOS_CUDA(cudaMemcpyAsync(b->prev, c->fsc, (size_t)g.n * 4, cudaMemcpyDeviceToDevice, s));
+    k_sur_combine<<<fos_blocks(g.n, 256), 256, 0, s>>>(g.n, c->sur_mode, b->raw, b->prev,
+                                                       b->anchor, b->anchor_valid, b->fscf,
+                                                       b->fsci);
+    FOS_LAUNCHED(c);
+    return FOS_OK;
+}
+
+const int32_t* fos_sur_fsc_int(FosCtx* c) { return c->sur ? c->sur->fsci : nullptr; }

@@ -216,6 +216,9 @@ SIGNATURES = {
     "fos_ensemble_frame_graph": [_P, _I, _P],
     "fos_ensemble_set_tuning": [_P, C.POINTER(FosEnsembleTuning)],
     "fos_ensemble_set_multi_voxel": [_P, _I],
+    "fos_ensemble_frame_surrogate": [_P, _P, _I, _P],
+    "fos_ensemble_surrogate_mode": [_P, _I],
+    "fos_ensemble_surrogate_stats": [_P, C.POINTER(FosSurrogateStats), _P],
     "fos_ensemble_get_tuning": [_P, C.POINTER(FosEnsembleTuning)],
     "fos_ensemble_autotune": [_P, _I, C.POINTER(FosEnsembleTuning), _P, _I, _P],
     "fos_ensemble_frame_index": [_P, C.POINTER(_I), _P],

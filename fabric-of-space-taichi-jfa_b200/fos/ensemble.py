@@ -130,6 +130,8 @@ class Ensemble:
         torch.cuda.synchronize(self.device)
         self.frame = 0
         self.use_graph = True
+        self.surrogate = None
+        self.policy = None
 
     def close(self):
         if getattr(self, "h", None):
@@ -150,10 +152,52 @@ class Ensemble:
     def is_jfa_frame(self, frame: int) -> bool:
         return self.cfg.is_jfa_frame(frame)
 
+    def attach_surrogate(self, surrogate, policy=None, mode: str = "anchored"):
+        """Run the learned FSC surrogate between JFA frames, as FoamSim does for
+        one foam: the policy (fos.surrogate.RefreshPolicy; default a refresh
+        every 2 cadences after the warm start) picks the JFA frames, every JFA
+        frame after the warm start is judged over all foams, and drift forces
+        refreshes.  Each foam's pairs come from its own grid, so every foam
+        gets the FSC it gets alone."""
+        from .surrogate import MODES, RefreshPolicy
+        if policy is None:
+            c = self.cfg
+            policy = RefreshPolicy(every=2 * c.JFA_CADENCE, warm_frames=c.JFA_WARM_FRAMES)
+        self.surrogate, self.policy = surrogate, policy
+        call("fos_ensemble_surrogate_mode", self.h, MODES[mode])
+
+    def surrogate_stats(self) -> dict:
+        """Counters of the last pair build and judged JFA frame, all foams."""
+        from ._lib import FosSurrogateStats
+        st = FosSurrogateStats()
+        call("fos_ensemble_surrogate_stats", self.h, C.byref(st), stream())
+        d = {k: getattr(st, k) for k, _ in FosSurrogateStats._fields_}
+        j = max(d["judged"], 1)
+        d.update(exact_frac=d["exact"] / j, within1_frac=d["within1"] / j,
+                 stale_exact_frac=d["stale_exact"] / j, stale_within1_frac=d["stale_within1"] / j,
+                 mean_abs_err=d["abs_err"] / j, stale_mean_abs_err=d["stale_abs_err"] / j)
+        return d
+
     def step(self) -> bool:
+        if self.surrogate is not None:
+            return self._step_surrogate()
         jfa = 1 if self.is_jfa_frame(self.frame) else 0
         fn = "fos_ensemble_frame_graph" if self.use_graph else "fos_ensemble_frame"
         call(fn, self.h, jfa, stream())
+        self.frame += 1
+        return bool(jfa)
+
+    def _step_surrogate(self) -> bool:
+        f, pol = self.frame, self.policy
+        jfa = pol.is_jfa(f)
+        if jfa or pol.is_surrogate(f):
+            call("fos_ensemble_frame_surrogate", self.h, self.surrogate.h, int(jfa), stream())
+        else:
+            fn = "fos_ensemble_frame_graph" if self.use_graph else "fos_ensemble_frame"
+            call(fn, self.h, 0, stream())
+        pol.ran(f, jfa)
+        if jfa and f >= pol.warm_frames:
+            pol.observe(self.surrogate_stats() | {"frame": f})
         self.frame += 1
         return bool(jfa)
 

@@ -620,6 +620,17 @@ int fos_ensemble_get_tuning(FosEnsemble* e, FosEnsembleTuning* t);
  * one voxel a thread (off).  DOMAIN_SIZE 1 only; the labels are the same
  * either way.  No reference counterpart. */
 int fos_ensemble_set_multi_voxel(FosEnsemble* e, int on);
+/* fos_frame_surrogate for every foam of the ensemble (no reference
+ * counterpart): the dynamics, then on a non-JFA frame the surrogate's FSC
+ * (candidate pairs on each foam's own hash grid, inference, the mode's FSC),
+ * its EMA and the targets; on a JFA frame the surrogate's estimate for the
+ * same positions, the JFA with its targets, then the per-cell judging.  Each
+ * foam's results equal the same foam's under fos_frame_surrogate. */
+int fos_ensemble_frame_surrogate(FosEnsemble* e, const FosSurrogate* m, int jfa_frame,
+                                 fos_stream_t s);
+/* fos_surrogate_set_mode / fos_surrogate_stats over all foams of the ensemble. */
+int fos_ensemble_surrogate_mode(FosEnsemble* e, int mode);
+int fos_ensemble_surrogate_stats(FosEnsemble* e, FosSurrogateStats* out, fos_stream_t s);
 /* Times every candidate shape of each tuned stage on the current state (the
  * JFA stages on this state's positions, the dynamics from a snapshot that is
  * restored afterwards), keeps the fastest per stage and applies it.

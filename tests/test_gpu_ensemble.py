@@ -150,3 +150,40 @@ def test_rejects_invalid_configurations():
     with pytest.raises(_lib.FosError):
         ens.tuning = dict(FIXED, pass_block=96)
     ens.close()
+
+
+@pytest.mark.parametrize("mode", ["anchored", "absolute"])
+def test_ensemble_with_surrogate_equals_single_foams(mode):
+    """The learned FSC surrogate between JFA frames inside the ensemble
+    (fos_ensemble_frame_surrogate): pairs on each foam's own grid, the same
+    model, mode and refresh schedule, so every foam equals the same foam run
+    alone with the surrogate, through surrogate frames, plain frames (the
+    policy's surrogate_every) and judged JFA frames."""
+    import math
+
+    from fos import surrogate as S
+    sur = S.Surrogate(seed=3)
+
+    def policy():
+        return S.RefreshPolicy(every=3, warm_frames=2, surrogate_every=2, min_exact=0.0,
+                               max_mean_abs_err=math.inf)
+    foams = _foams()
+    ens = Ensemble(foams, **OVER)
+    ens.attach_surrogate(sur, policy(), mode)
+    sims = [FoamSim.from_foam(f, surrogate=sur, policy=policy(), surrogate_mode=mode, **OVER)
+            for f in foams]
+    for s in sims:
+        s.initialize()
+    ens.initialize()
+    for f in range(10):
+        jfa = ens.step()
+        for s in sims:
+            assert s.step() == jfa
+        torch.cuda.synchronize()
+        _assert_same(ens, sims, f"frame {f}")
+    st = ens.surrogate_stats()
+    assert st["judged"] == sum(f.n for f in foams)
+    assert st["pairs"] > 0 and ens.policy.judged
+    for s in sims:
+        s.ctx.close()
+    ens.close()
