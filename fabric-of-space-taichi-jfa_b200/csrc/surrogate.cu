@@ -256,10 +256,34 @@ __global__ void __launch_bounds__(256) k_sur_pairs_ens(
                    pj, pnd, pcount, hist, counters);
 }
 
+// Memory features of pair (i, j) from the last JFA frame (its neighbour
+// lists nl [n][32] with used counts, and its fsc): whether the two were
+// neighbours (j in i's list or i in j's), and fsc_i + fsc_j.
+// The rows are read as 16-byte vectors (a row is 128 bytes, 16-byte aligned).
+__device__ __forceinline__ bool sur_in_row(const int32_t* __restrict__ nl,
+                                           const int32_t* __restrict__ used, int a, int b) {
+    const int u = min(__ldg(&used[a]), FOS_S);
+    const int4* row = reinterpret_cast<const int4*>(nl + (size_t)a * FOS_S);
+    bool m = false;
+    for (int q = 0; q < u; q += 4) {
+        const int4 v = __ldg(&row[q >> 2]);
+        m |= (v.x == b) | ((q + 1 < u) & (v.y == b)) | ((q + 2 < u) & (v.z == b)) |
+             ((q + 3 < u) & (v.w == b));
+    }
+    return m;
+}
+
+__device__ __forceinline__ float sur_member(const int32_t* __restrict__ nl,
+                                            const int32_t* __restrict__ used, int i, int j) {
+    return (sur_in_row(nl, used, i, j) || sur_in_row(nl, used, j, i)) ? 1.f : 0.f;
+}
+
 // The 16 raw features of pair (i, j) at normalised distance nd; hi and hj
-// are the two particles' histogram rows (13 ints each).
+// are the two particles' histogram rows (SUR_NB ints each), mem and fsum
+// the memory features.
 __device__ __forceinline__ void sur_features(float ri, float rj, float nd, const int32_t* hi,
-                                             const int32_t* hj, float inv_cut_bins, float* x) {
+                                             const int32_t* hj, float inv_cut_bins, float mem,
+                                             float fsum, float* x) {
     x[0] = nd;
     x[1] = fdiv(ri, rj);
     x[2] = nd > 0.f ? fdiv(fsub(ri, rj), fmul(fmul(2.0f, nd), fadd(ri, rj))) : 0.f;
@@ -271,7 +295,10 @@ __device__ __forceinline__ void sur_features(float ri, float rj, float nd, const
         const int v = __ldg(&hi[b]) + __ldg(&hj[b]) - (b == bin ? 2 : 0);
         x[3 + b] = (float)v;
     }
+    x[3 + SUR_NB] = mem;
+    x[4 + SUR_NB] = fsum;
 }
+static_assert(SUR_NF == SUR_NB + 5, "feature layout: 3 geometric, the bins, 2 memory");
 
 // Training export: one warp per owner i writes its pairs' raw FP32 feature
 // rows, labels (j in i's JFA neighbour list) and indices at pstart[i] + slot.
@@ -283,7 +310,10 @@ __global__ void __launch_bounds__(256) k_sur_export(int n, const int32_t* __rest
                                                     int32_t* __restrict__ fi,
                                                     int32_t* __restrict__ fj, float* __restrict__ X,
                                                     float* __restrict__ y,
-                                                    const int32_t* __restrict__ nl) {
+                                                    const int32_t* __restrict__ nl,
+                                                    const int32_t* __restrict__ mnl,
+                                                    const int32_t* __restrict__ mused,
+                                                    const int32_t* __restrict__ mfsc) {
     const int i = (int)(((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5);
     const int lane = threadIdx.x & 31;
     if (i >= n) return;
@@ -295,7 +325,8 @@ __global__ void __launch_bounds__(256) k_sur_export(int n, const int32_t* __rest
         const float nd = pnd[(size_t)i * SUR_CAP + s];
         float x[SUR_NF];
         sur_features(ri, rad[j], nd, hist + (size_t)i * SUR_NB, hist + (size_t)j * SUR_NB,
-                     inv_cut_bins, x);
+                     inv_cut_bins, sur_member(mnl, mused, i, j),
+                     (float)(__ldg(&mfsc[i]) + __ldg(&mfsc[j])), x);
         const size_t row = (size_t)b0 + s;
         if (X) {
 #pragma unroll
@@ -474,7 +505,8 @@ __global__ void __launch_bounds__(256) k_sur_mlp_seg(
     const float* __restrict__ pnd, const float* __restrict__ rad, const int32_t* __restrict__ hist,
     float cutoff, const float* __restrict__ norm, const __nv_bfloat16* __restrict__ wbf,
     const float* __restrict__ params, const int32_t* __restrict__ pstart, float* __restrict__ prob,
-    unsigned long long* __restrict__ acc) {
+    unsigned long long* __restrict__ acc, const int32_t* __restrict__ mnl,
+    const int32_t* __restrict__ mused, const int32_t* __restrict__ mfsc) {
     __shared__ SurSmem sm;
     __shared__ __align__(16) unsigned int s_x[8][16 * SUR_XS];
     sur_load_weights(sm, wbf, params, norm);
@@ -534,6 +566,8 @@ __global__ void __launch_bounds__(256) k_sur_mlp_seg(
 #pragma unroll
                     for (int b = 5; b < SUR_NB; ++b)
                         x[b - 5] = (float)(__ldg(&hi[b]) + __ldg(&hj[b]) - (b == bin ? 2 : 0));
+                    x[SUR_NB - 5] = sur_member(mnl, mused, i, j);
+                    x[SUR_NB - 4] = (float)(__ldg(&mfsc[i]) + __ldg(&mfsc[j]));
                 }
                 unsigned int pk[4];
 #pragma unroll
@@ -1141,7 +1175,7 @@ static int sur_predict_impl(FosCtx* c, const FosSurrogate* m, const float* rad, 
     const long long groups = (n + SUR_GROUP - 1) / SUR_GROUP;
     k_sur_mlp_seg<<<sur_persistent_blocks(c->num_sms, groups), 256, 0, s>>>(
         n, b->pcount, b->pj, b->pnd, rad, b->hist, m->cutoff, m->norm, m->wbf, m->params,
-        b->pstart, pair_prob, b->acc);
+        b->pstart, pair_prob, b->acc, c->nl, c->used, c->fsc);
     FOS_LAUNCHED(c);
     k_sur_fsc<<<fos_blocks(n, 256), 256, 0, s>>>(n, b->acc, b->raw, fsc_float, fsc_int);
     FOS_LAUNCHED(c);
@@ -1181,15 +1215,23 @@ extern "C" int fos_surrogate_pair_count(FosCtx* c, int* pairs, int* overflow, fo
 }
 
 extern "C" int fos_surrogate_export(FosCtx* c, const float* rad, float* X, float* y,
-                                    int32_t* pair_i, int32_t* pair_j, fos_stream_t s) {
+                                    int32_t* pair_i, int32_t* pair_j, const int32_t* mem_nl,
+                                    const int32_t* mem_used, const int32_t* mem_fsc,
+                                    fos_stream_t s) {
     FOS_REQUIRE(c && rad, FOS_E_ARG, "NULL argument");
+    if (!mem_nl) mem_nl = c->nl;
+    if (!mem_used) mem_used = c->used;
+    if (!mem_fsc) mem_fsc = c->fsc;
+    FOS_REQUIRE(((uintptr_t)mem_nl & 15u) == 0, FOS_E_ARG,
+                "mem_nl must be 16-byte aligned (its rows are read as 16-byte vectors)");
     FOS_REQUIRE(c->sur && c->sur->n > 0, FOS_E_STATE, "no pair build on this context");
     FosSurBufs* b = c->sur;
     const int n = b->n;
     int rc = sur_scan(c, (cudaStream_t)s);
     if (rc) return rc;
     k_sur_export<<<fos_blocks(32LL * n, 256), 256, 0, (cudaStream_t)s>>>(
-        n, b->pj, b->pnd, b->pstart, rad, b->hist, b->cutoff, pair_i, pair_j, X, y, c->nl);
+        n, b->pj, b->pnd, b->pstart, rad, b->hist, b->cutoff, pair_i, pair_j, X, y, c->nl,
+        mem_nl, mem_used, mem_fsc);
     FOS_LAUNCHED(c);
     return FOS_OK;
 }

@@ -113,7 +113,7 @@ class FosEnsembleView(C.Structure):
 
 SUR_FEATURES = 16
 SUR_HIDDEN = 64
-SUR_BINS = 13
+SUR_BINS = 11
 SUR_PAIR_CAP = 96
 SUR_NPARAM = 64 * 16 + 64 + 64 * 64 + 64 + 64 + 1
 SUR_ABSOLUTE = 0
@@ -199,7 +199,7 @@ SIGNATURES = {
     "fos_surrogate_forward": [_P, _P, _I, _P, _P],
     "fos_surrogate_pairs": [_P, _P, _P, _P, _I, _F, _P, _P, _P, _P],
     "fos_surrogate_pair_count": [_P, C.POINTER(_I), C.POINTER(_I), _P],
-    "fos_surrogate_export": [_P, _P, _P, _P, _P, _P, _P],
+    "fos_surrogate_export": [_P, _P, _P, _P, _P, _P, _P, _P, _P, _P],
     "fos_surrogate_predict": [_P, _P, _P, _P, _P, _P, _P],
     "fos_surrogate_stats": [_P, C.POINTER(FosSurrogateStats), _P],
     "fos_surrogate_set_mode": [_P, _I],

@@ -194,9 +194,11 @@ def pair_count(ctx: Context):
     return p.value, o.value
 
 
-def export(ctx: Context, rad, labels: bool = True) -> dict:
+def export(ctx: Context, rad, labels: bool = True, memory=None) -> dict:
     """Features, labels (pair in the last JFA neighbour list) and pair indices
-    of the last pair build."""
+    of the last pair build.  memory = (neighbor_list, neighbor_used_count,
+    fsc) of an earlier JFA frame for the memory features 14-15 (None: the
+    context's current ones, as inference sees them)."""
     P, overflow = pair_count(ctx)
     dev = rad.device
     X = torch.empty((P, NF), dtype=torch.float32, device=dev)
@@ -204,8 +206,9 @@ def export(ctx: Context, rad, labels: bool = True) -> dict:
     pi = torch.empty(P, dtype=torch.int32, device=dev)
     pj = torch.empty(P, dtype=torch.int32, device=dev)
     if P > 0:
+        mem = [None, None, None] if memory is None else list(memory)
         call("fos_surrogate_export", ctx.h, ptr(rad, torch.float32, "rad"), ptr(X), ptr(y),
-             ptr(pi), ptr(pj), stream())
+             ptr(pi), ptr(pj), ptr(mem[0]), ptr(mem[1]), ptr(mem[2]), stream())
     return {"X": X, "y": y, "i": pi, "j": pj, "overflow": overflow}
 
 
@@ -305,22 +308,29 @@ def collect(foams, sur: Surrogate, export_frames=(15, 25), max_rows: int | None 
     """Labelled pairs from JFA frames of plain simulations.  For each foam,
     the plain frame loop runs up to the last export frame; at every export
     frame (which must be a JFA frame) the pairs of the post-frame positions
-    are built and labelled by that frame's JFA neighbour lists.  With
-    max_rows, a seeded uniform subset of that many rows is kept."""
+    are built and labelled by that frame's JFA neighbour lists, and their
+    memory features come from the JFA frame before it (the lists a surrogate
+    frame would see).  With max_rows, a seeded uniform subset of that many
+    rows is kept."""
     from .driver import FoamSim
     Xs, ys = [], []
     for foam in foams:
         sim = FoamSim.from_foam(foam)
         sim.initialize()
         last = max(export_frames)
+        mem = None
         for f in range(last + 1):
+            if f in export_frames:
+                n = sim.n
+                mem = (sim.neighbor_list[:n].clone(), sim.ctx.neighbor_used_count[:n].clone(),
+                       sim.fsc[:n].clone())
             jfa = sim.step()
             if f in export_frames:
                 if not jfa:
                     raise ValueError(f"export frame {f} is not a JFA frame")
                 build_pairs(sim.ctx, sur, sim.pos, sim.rad, sim.n, float(sim.cfg.R_MAX),
                             sim.cell_start, sim.cell_count, sim.cell_indices)
-                d = export(sim.ctx, sim.rad)
+                d = export(sim.ctx, sim.rad, memory=mem)
                 Xs.append(d["X"])
                 ys.append(d["y"])
         sim.ctx.close()

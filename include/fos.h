@@ -433,8 +433,11 @@ int fos_topo_update_radii(FosCtx* ctx, float* rad, const float* deg_effective, f
  *   2       signed offset of the power bisector from the midpoint, over
  *           r_i + r_j: (r_i^2 - r_j^2) / (2 |d| (r_i + r_j)), evaluated as
  *           (r_i - r_j) / ((2 * x0) * (r_i + r_j)) (0 when x0 == 0)
- *   3..15   13-bin histogram (bins of width cutoff/13 in normalised distance)
- *           of both particles' other candidates, counts summed over i and j.
+ *   3..13   11-bin histogram (bins of width cutoff/11 in normalised distance)
+ *           of both particles' other candidates, counts summed over i and j;
+ *   14      1 when i and j were neighbours at the last JFA frame (j in i's
+ *           neighbour list or i in j's), else 0;
+ *   15      fsc_i + fsc_j of the last JFA frame.
  * The model is an MLP 16 -> 64 -> ReLU -> 64 -> ReLU -> 1 -> sigmoid giving
  * the probability that the pair shares a face.  A particle's FSC estimate is
  * the sum of its pairs' probabilities.  Inference uses BF16 weights and
@@ -446,7 +449,7 @@ int fos_topo_update_radii(FosCtx* ctx, float* rad, const float* deg_effective, f
  * with W[out][in]. */
 #define FOS_SUR_FEATURES 16
 #define FOS_SUR_HIDDEN 64
-#define FOS_SUR_BINS 13
+#define FOS_SUR_BINS 11
 #define FOS_SUR_PAIR_CAP 96 /* pairs kept per owner particle */
 #define FOS_SUR_NPARAM (64 * 16 + 64 + 64 * 64 + 64 + 64 + 1)
 
@@ -512,10 +515,14 @@ int fos_surrogate_pair_count(FosCtx* ctx, int* pairs, int* overflow, fos_stream_
 /* Training export of the last pair build, in pair order (owner i
  * ascending, then search order): X [P][16] raw features, y [P] = 1 when j is
  * in i's JFA neighbour list on ctx (the last finalize), pair_i/pair_j [P].
- * Any output may be NULL.  Asynchronous; size the outputs with
- * fos_surrogate_pair_count. */
+ * Features 14-15 come from mem_nl [n][32] (16-byte aligned), mem_used [n] and mem_fsc [n] (an
+ * earlier JFA frame's neighbour lists, used counts and fsc, so that the
+ * label is not among the inputs); NULL takes the context's current ones, as
+ * inference does.  Any output may be NULL.  Asynchronous; size the outputs
+ * with fos_surrogate_pair_count. */
 int fos_surrogate_export(FosCtx* ctx, const float* rad, float* X, float* y, int32_t* pair_i,
-                         int32_t* pair_j, fos_stream_t s);
+                         int32_t* pair_j, const int32_t* mem_nl, const int32_t* mem_used,
+                         const int32_t* mem_fsc, fos_stream_t s);
 /* Inference over the last pair build: fsc_float[n] = sum of pair
  * probabilities, fsc_int[n] = rint(fsc_float), pair_prob[P] in export order
  * (each may be NULL).  Without pair_prob: no host sync, graph-capturable. */

@@ -14,7 +14,7 @@ from __future__ import annotations
 import numpy as np
 import torch
 
-NB = 13
+NB = 11
 NF = 16
 NH = 64
 F = np.float32
@@ -31,10 +31,12 @@ def owns(i, j):
     return (i < j) == (((i + j) & 1) == 1)
 
 
-def pairs_and_features(pos, rad, cutoff, L=1.0, chunk=512):
+def pairs_and_features(pos, rad, cutoff, L=1.0, chunk=512, nl=None, used=None, fsc=None):
     """All pairs with nd = |d| / (r_i + r_j) < cutoff, each once as (owner i,
     other j), their raw features [P, 16] (include/fos.h order, d = x_j - x_i)
-    and the per-particle histograms."""
+    and the per-particle histograms.  nl [n, 32], used [n] and fsc [n] are the
+    last JFA frame's neighbour lists, used counts and fsc (features 14-15;
+    zeros when not given)."""
     pos = np.ascontiguousarray(pos, F)
     rad = np.ascontiguousarray(rad, F)
     n = rad.shape[0]
@@ -74,7 +76,17 @@ def pairs_and_features(pos, rad, cutoff, L=1.0, chunk=512):
     bins = np.minimum((ND * inv_bins).astype(F).astype(np.int64), NB - 1)
     H = hist[I] + hist[J]
     H[np.arange(len(I)), bins] -= 2
-    X[:, 3:] = H.astype(F)
+    X[:, 3:3 + NB] = H.astype(F)
+    if nl is not None:
+        nl = np.asarray(nl)
+        u = np.minimum(np.asarray(used), nl.shape[1])
+        cols = np.arange(nl.shape[1])[None, :]
+        live = cols < u[:, None]
+        mem = np.zeros(len(I), bool)
+        for a, b in ((I, J), (J, I)):
+            mem |= ((nl[a] == b[:, None]) & live[a]).any(axis=1)
+        X[:, 3 + NB] = mem.astype(F)
+        X[:, 4 + NB] = (np.asarray(fsc)[I] + np.asarray(fsc)[J]).astype(F)
     return {"i": I, "j": J, "nd": ND, "X": X, "hist": hist}
 
 

@@ -74,11 +74,17 @@ def test_pairs_and_features_bit_exact(case):
         G = cfg.grid_res()
         reach = int(np.floor(cutoff * (0.05 + foam.r_max) / (1.0 / G))) + 1
         assert 2 * reach + 1 >= G  # exercises the whole-axis branch
+    ctx.jfa_run(pos, rad, foam.n)  # the memory features' lists and fsc
     S.build_pairs(ctx, sur, pos, rad, foam.n, foam.r_max, cs, cc, ci)
     d = S.export(ctx, rad, labels=False)
     torch.cuda.synchronize()
     assert d["overflow"] == 0
-    ref = R.pairs_and_features(pos.cpu().numpy(), rad.cpu().numpy(), cutoff)
+    n = foam.n
+    ref = R.pairs_and_features(pos.cpu().numpy(), rad.cpu().numpy(), cutoff,
+                               nl=ctx.neighbor_list[:n].cpu().numpy(),
+                               used=ctx.neighbor_used_count[:n].cpu().numpy(),
+                               fsc=ctx.fsc[:n].cpu().numpy())
+    assert 0 < ref["X"][:, 14].sum() < len(ref["X"])
     gi, gj, gX = _sorted(d["i"].cpu().numpy(), d["j"].cpu().numpy(), d["X"].cpu().numpy())
     ri, rj, rX = _sorted(ref["i"], ref["j"], ref["X"])
     assert len(gi) == len(ri) and len(ri) > 0

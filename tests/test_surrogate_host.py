@@ -25,12 +25,12 @@ def _header_define(name):
 def test_constants_match_header():
     assert _header_define("FOS_SUR_FEATURES") == _lib.SUR_FEATURES == 16
     assert _header_define("FOS_SUR_HIDDEN") == _lib.SUR_HIDDEN == 64
-    assert _header_define("FOS_SUR_BINS") == _lib.SUR_BINS == 13
+    assert _header_define("FOS_SUR_BINS") == _lib.SUR_BINS == 11
     assert _header_define("FOS_SUR_PAIR_CAP") == _lib.SUR_PAIR_CAP
     assert _header_define("FOS_SUR_NPARAM") == _lib.SUR_NPARAM == 5313
     assert _header_define("FOS_SUR_ABSOLUTE") == _lib.SUR_ABSOLUTE
     assert _header_define("FOS_SUR_ANCHORED") == _lib.SUR_ANCHORED
-    assert 3 + _lib.SUR_BINS == _lib.SUR_FEATURES
+    assert 3 + _lib.SUR_BINS + 2 == _lib.SUR_FEATURES  # geometry, bins, memory
 
 
 def test_param_layout_round_trip():
