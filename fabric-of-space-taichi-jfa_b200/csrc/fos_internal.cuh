@@ -147,6 +147,7 @@ struct FosCtx {
     int tm_res = 0, tm_ok = 0;
     int use_tma = 0;                  // staged record rows in the JFA pass (off: it measured slower)
     int use_recx = 1;                 // JFA record pass with several voxels a thread along x
+    int sur_tc = 1;                   // surrogate inference on tcgen05 (1) or mma.sync (0)
     int coop_blocks = -1;             // resident blocks of the cooperative kernel (-1: not queried)
     size_t cell_tmp_n = 0;
     float* stats_f = nullptr;         // device stats scratch

@@ -605,6 +605,286 @@ __global__ void __launch_bounds__(256) k_sur_mlp_seg(
     }
 }
 
+// ------------------------------------------------ tcgen05 inference (sm_100a)
+// The same inference on the 5th-generation tensor cores: a CTA of 128
+// threads takes tiles of 128 flat pair rows (row = thread = TMEM lane).  Each
+// thread builds its row's 16 features into a shared-memory A tile; one thread
+// issues tcgen05.mma (kind::f16, BF16 x BF16 -> FP32, M = 128, N = 64) into a
+// TMEM accumulator and commits it to an mbarrier; each warp reads its 32 rows
+// back with tcgen05.ld, adds the bias, applies ReLU and writes the BF16
+// hidden layer as the second A tile (four K = 16 slabs); four more MMAs give
+// the second layer, whose read-back feeds the 64 -> 1 output, the sigmoid and
+// the per-particle fixed-point sums.  Operands sit in shared memory in the
+// canonical K-major layout without swizzle: 8-row x 16-byte core matrices,
+// the two K halves of a slab 128 bytes apart (leading byte offset) and
+// consecutive 8-row groups 256 bytes apart (stride byte offset).
+#define SUR_TC_ROWS 128
+#define SUR_TC_COLS 128  // TMEM columns: layer 1 at 0, layer 2 at 64
+#define SUR_TC_PAD (24 * 1024)  // dynamic shared-memory padding (residency cap)
+
+struct SurTcSmem {
+    alignas(1024) unsigned char a1[SUR_TC_ROWS * 16 * 2];
+    alignas(1024) unsigned char a2[4][SUR_TC_ROWS * 16 * 2];
+    alignas(1024) unsigned char w1[SUR_H * 16 * 2];
+    alignas(1024) unsigned char w2[4][SUR_H * 16 * 2];
+    float b1[SUR_H], b2[SUR_H], w3[SUR_H], norm[2 * SUR_NF];
+    alignas(8) unsigned long long bar;
+    unsigned int tmem;
+};
+
+// Byte offset of element (r, k) of a K = 16 slab in the canonical layout.
+__device__ __forceinline__ int sur_tc_ofs(int r, int k) {
+    return (r >> 3) * 256 + (k >> 3) * 128 + (r & 7) * 16 + (k & 7) * 2;
+}
+
+// Shared-memory matrix descriptor of a slab at shared address addr:
+// start >> 4, leading byte offset 128 >> 4, stride byte offset 256 >> 4,
+// descriptor version 1, no swizzle.
+__device__ __forceinline__ unsigned long long sur_tc_desc(unsigned int addr) {
+    return (unsigned long long)((addr & 0x3FFFFu) >> 4) | (8ull << 16) | (16ull << 32) |
+           (1ull << 46);
+}
+
+// Instruction descriptor: FP32 accumulate (bit 4), BF16 A (bit 7) and B
+// (bit 10), both K-major, N / 8 = 8 at bit 17, M / 16 = 8 at bit 24.
+#define SUR_TC_IDESC 0x08100490u
+
+__device__ __forceinline__ void sur_tc_mma(unsigned int tmem_d, unsigned long long da,
+                                           unsigned long long db, unsigned int accumulate) {
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "setp.ne.b32 p, %4, 0;\n\t"
+        "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n\t}"
+        :
+        : "r"(tmem_d), "l"(da), "l"(db), "r"(SUR_TC_IDESC), "r"(accumulate), "r"(0u), "r"(0u),
+          "r"(0u), "r"(0u)
+        : "memory");
+}
+
+__device__ __forceinline__ void sur_tc_commit(unsigned int bar) {
+    asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
+                     bar)
+                 : "memory");
+}
+
+__device__ __forceinline__ bool sur_tc_try_wait(unsigned int bar, unsigned int parity) {
+    unsigned int done;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+        "selp.u32 %0, 1, 0, p;\n\t}"
+        : "=r"(done)
+        : "r"(bar), "r"(parity)
+        : "memory");
+    return done != 0u;
+}
+
+// Bounded wait (about 1 s of clock): false, with FOS_E_TIMEOUT recorded, if
+// the phase never completed.
+__device__ __forceinline__ bool sur_tc_wait(unsigned int bar, unsigned int parity,
+                                            int* err) {
+    const long long t0 = clock64();
+    for (unsigned int it = 1;; ++it) {
+        if (sur_tc_try_wait(bar, parity)) return true;
+        if ((it & 63u) == 0u && clock64() - t0 > FOS_BAR_CYCLE_LIMIT) {
+            atomicCAS(err, 0, (int)FOS_E_TIMEOUT);
+            return false;
+        }
+    }
+}
+
+// 64 FP32 columns of this warp's 32 TMEM lanes starting at column col.
+__device__ __forceinline__ void sur_tc_ld64(unsigned int taddr, float (&v)[64]) {
+    unsigned int r[64];
+    asm volatile(
+        "tcgen05.ld.sync.aligned.32x32b.x64.b32 "
+        "{%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, %15, "
+        "%16, %17, %18, %19, %20, %21, %22, %23, %24, %25, %26, %27, %28, %29, %30, %31, "
+        "%32, %33, %34, %35, %36, %37, %38, %39, %40, %41, %42, %43, %44, %45, %46, %47, "
+        "%48, %49, %50, %51, %52, %53, %54, %55, %56, %57, %58, %59, %60, %61, %62, %63}, "
+        "[%64];"
+        : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]),
+          "=r"(r[7]), "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]),
+          "=r"(r[13]), "=r"(r[14]), "=r"(r[15]), "=r"(r[16]), "=r"(r[17]), "=r"(r[18]),
+          "=r"(r[19]), "=r"(r[20]), "=r"(r[21]), "=r"(r[22]), "=r"(r[23]), "=r"(r[24]),
+          "=r"(r[25]), "=r"(r[26]), "=r"(r[27]), "=r"(r[28]), "=r"(r[29]), "=r"(r[30]),
+          "=r"(r[31]), "=r"(r[32]), "=r"(r[33]), "=r"(r[34]), "=r"(r[35]), "=r"(r[36]),
+          "=r"(r[37]), "=r"(r[38]), "=r"(r[39]), "=r"(r[40]), "=r"(r[41]), "=r"(r[42]),
+          "=r"(r[43]), "=r"(r[44]), "=r"(r[45]), "=r"(r[46]), "=r"(r[47]), "=r"(r[48]),
+          "=r"(r[49]), "=r"(r[50]), "=r"(r[51]), "=r"(r[52]), "=r"(r[53]), "=r"(r[54]),
+          "=r"(r[55]), "=r"(r[56]), "=r"(r[57]), "=r"(r[58]), "=r"(r[59]), "=r"(r[60]),
+          "=r"(r[61]), "=r"(r[62]), "=r"(r[63])
+        : "r"(taddr)
+        : "memory");
+    asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+#pragma unroll
+    for (int c = 0; c < 64; ++c) v[c] = __uint_as_float(r[c]);
+}
+
+__global__ void __launch_bounds__(SUR_TC_ROWS) k_sur_mlp_tc(
+    int n, const int32_t* __restrict__ pstart, const int32_t* __restrict__ pj,
+    const float* __restrict__ pnd, const float* __restrict__ rad, const int32_t* __restrict__ hist,
+    float cutoff, const float* __restrict__ norm, const __nv_bfloat16* __restrict__ wbf,
+    const float* __restrict__ params, float* __restrict__ prob, unsigned long long* __restrict__ acc,
+    const int32_t* __restrict__ mnl, const int32_t* __restrict__ mused,
+    const int32_t* __restrict__ mfsc, int* err) {
+    __shared__ SurTcSmem sm;
+    const int t = threadIdx.x, warp = t >> 5;
+    // weights into the canonical layout, biases and standardisation
+    for (int e = t; e < SUR_H * 16; e += blockDim.x) {
+        const int nrow = e >> 4, k = e & 15;
+        *reinterpret_cast<__nv_bfloat16*>(sm.w1 + sur_tc_ofs(nrow, k)) = wbf[e];
+    }
+    for (int e = t; e < SUR_H * SUR_H; e += blockDim.x) {
+        const int nrow = e >> 6, k = e & 63;
+        *reinterpret_cast<__nv_bfloat16*>(sm.w2[k >> 4] + sur_tc_ofs(nrow, k & 15)) =
+            wbf[SUR_H * SUR_NF + e];
+    }
+    for (int e = t; e < SUR_H; e += blockDim.x) {
+        sm.b1[e] = params[SUR_OFF_B1 + e];
+        sm.b2[e] = params[SUR_OFF_B2 + e];
+        sm.w3[e] = __bfloat162float(wbf[SUR_H * SUR_NF + SUR_H * SUR_H + e]);
+    }
+    for (int e = t; e < 2 * SUR_NF; e += blockDim.x) sm.norm[e] = norm[e];
+    const unsigned int bar = (unsigned int)__cvta_generic_to_shared(&sm.bar);
+    if (t == 0) {
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(bar) : "memory");
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    if (warp == 0) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(
+                         (unsigned int)__cvta_generic_to_shared(&sm.tmem)),
+                     "r"(SUR_TC_COLS)
+                     : "memory");
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+    }
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    __syncthreads();
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    const unsigned int tmem = sm.tmem;
+    const unsigned int lane_base = (unsigned int)(warp * 32) << 16;
+    const unsigned int a1 = (unsigned int)__cvta_generic_to_shared(sm.a1);
+    const unsigned int w1 = (unsigned int)__cvta_generic_to_shared(sm.w1);
+    const float inv_cut_bins = (float)SUR_NB / cutoff;
+    const float b3 = params[SUR_OFF_B3];
+    const int P = pstart[n];
+    const int tiles = (P + SUR_TC_ROWS - 1) / SUR_TC_ROWS;
+    unsigned int phase = 0;
+    bool ok = true;
+    for (int tile = blockIdx.x; tile < tiles && ok; tile += gridDim.x) {
+        // (1) this thread's row: owner i by binary search over pstart
+        const int g = tile * SUR_TC_ROWS + t;
+        const bool valid = g < P;
+        int i = 0, j = 0;
+        uint4 lo = make_uint4(0u, 0u, 0u, 0u), hi = lo;
+        if (valid) {
+            int a = 0, b = n;  // largest a with pstart[a] <= g
+            while (b - a > 1) {
+                const int m = (a + b) >> 1;
+                if (__ldg(&pstart[m]) <= g) a = m;
+                else b = m;
+            }
+            i = a;
+            const int slot = g - __ldg(&pstart[i]);
+            j = pj[(size_t)i * SUR_CAP + slot];
+            const float nd = pnd[(size_t)i * SUR_CAP + slot];
+            float x[SUR_NF];
+            sur_features(rad[i], rad[j], nd, hist + (size_t)i * SUR_NB, hist + (size_t)j * SUR_NB,
+                         inv_cut_bins, sur_member(mnl, mused, i, j),
+                         (float)(__ldg(&mfsc[i]) + __ldg(&mfsc[j])), x);
+            unsigned int pk[8];
+#pragma unroll
+            for (int f = 0; f < SUR_NF; f += 2)
+                pk[f / 2] = pack_bf16x2((x[f] - sm.norm[f]) * sm.norm[SUR_NF + f],
+                                        (x[f + 1] - sm.norm[f + 1]) * sm.norm[SUR_NF + f + 1]);
+            lo = make_uint4(pk[0], pk[1], pk[2], pk[3]);
+            hi = make_uint4(pk[4], pk[5], pk[6], pk[7]);
+        }
+        *reinterpret_cast<uint4*>(sm.a1 + sur_tc_ofs(t, 0)) = lo;
+        *reinterpret_cast<uint4*>(sm.a1 + sur_tc_ofs(t, 8)) = hi;
+        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+        asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+        __syncthreads();
+        asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+        // (2) layer 1: D[0, 64) = A1 (128 x 16) . W1^T
+        if (t == 0) {
+            sur_tc_mma(tmem, sur_tc_desc(a1), sur_tc_desc(w1), 0u);
+            sur_tc_commit(bar);
+        }
+        // the block agrees on the outcome, so every thread takes the same path
+        if (!__syncthreads_and(sur_tc_wait(bar, phase, err))) {
+            ok = false;
+            break;
+        }
+        phase ^= 1u;
+        asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+        // (3) bias, ReLU, BF16 -> the second A tile (four K = 16 slabs)
+        {
+            float h[64];
+            sur_tc_ld64(tmem + lane_base, h);
+#pragma unroll
+            for (int sl = 0; sl < 4; ++sl) {
+                unsigned int pk[8];
+#pragma unroll
+                for (int q = 0; q < 8; ++q) {
+                    const int c = sl * 16 + 2 * q;
+                    pk[q] = pack_bf16x2(fmaxf(h[c] + sm.b1[c], 0.f),
+                                        fmaxf(h[c + 1] + sm.b1[c + 1], 0.f));
+                }
+                *reinterpret_cast<uint4*>(sm.a2[sl] + sur_tc_ofs(t, 0)) =
+                    make_uint4(pk[0], pk[1], pk[2], pk[3]);
+                *reinterpret_cast<uint4*>(sm.a2[sl] + sur_tc_ofs(t, 8)) =
+                    make_uint4(pk[4], pk[5], pk[6], pk[7]);
+            }
+        }
+        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+        asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+        __syncthreads();
+        asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+        // (4) layer 2: D[64, 128) = A2 (128 x 64) . W2^T, four K slabs
+        if (t == 0) {
+#pragma unroll
+            for (int sl = 0; sl < 4; ++sl)
+                sur_tc_mma(tmem + 64, sur_tc_desc((unsigned int)__cvta_generic_to_shared(sm.a2[sl])),
+                           sur_tc_desc((unsigned int)__cvta_generic_to_shared(sm.w2[sl])),
+                           sl > 0 ? 1u : 0u);
+            sur_tc_commit(bar);
+        }
+        if (!__syncthreads_and(sur_tc_wait(bar, phase, err))) {
+            ok = false;
+            break;
+        }
+        phase ^= 1u;
+        asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+        // (5) bias, ReLU, the 64 -> 1 output, sigmoid, fixed-point sums
+        {
+            float h[64];
+            sur_tc_ld64(tmem + lane_base + 64, h);
+            float z = 0.f;
+#pragma unroll
+            for (int c = 0; c < 64; ++c) z += fmaxf(h[c] + sm.b2[c], 0.f) * sm.w3[c];
+            if (valid) {
+                const float pr = 1.0f / (1.0f + expf(-(z + b3)));
+                if (prob) prob[g] = pr;
+                const unsigned long long qv = (unsigned long long)(pr * SUR_FIX + 0.5f);
+                atomicAdd(&acc[i], qv);
+                atomicAdd(&acc[j], qv);
+            }
+        }
+        asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+        __syncthreads();
+    }
+    // every MMA this CTA issued has completed (waited on above); free TMEM
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    __syncthreads();
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    if (warp == 0)
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem),
+                     "r"(SUR_TC_COLS)
+                     : "memory");
+}
+
 __global__ void k_sur_fsc(int n, const unsigned long long* __restrict__ acc,
                           float* __restrict__ raw, float* __restrict__ fs,
                           int32_t* __restrict__ fsi) {
@@ -1167,11 +1447,32 @@ static int sur_pairs_impl(FosCtx* c, const FosSurrogate* m, const float* pos, co
     return FOS_OK;
 }
 
+static int sur_scan(FosCtx* c, cudaStream_t s);
+
 static int sur_predict_impl(FosCtx* c, const FosSurrogate* m, const float* rad, float* fsc_float,
                             int32_t* fsc_int, float* pair_prob, cudaStream_t s) {
     FosSurBufs* b = c->sur;
     const int n = b->n;
     FOS_CUDA(cudaMemsetAsync(b->acc, 0, (size_t)n * 8, s));
+    if (c->sur_tc) {
+        // tcgen05 tiles over the flat rows: pstart and the row count first
+        int rc = sur_scan(c, s);
+        if (rc) return rc;
+        static bool attr = false;
+        if (!attr) {
+            FOS_CUDA(cudaFuncSetAttribute(k_sur_mlp_tc, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                          SUR_TC_PAD));
+            attr = true;
+        }
+        // the padding keeps at most four CTAs (4 x 128 TMEM columns) on an SM
+        k_sur_mlp_tc<<<c->num_sms * 4, SUR_TC_ROWS, SUR_TC_PAD, s>>>(
+            n, b->pstart, b->pj, b->pnd, rad, b->hist, m->cutoff, m->norm, m->wbf, m->params,
+            pair_prob, b->acc, c->nl, c->used, c->fsc, &c->ds->error);
+        FOS_LAUNCHED(c);
+        k_sur_fsc<<<fos_blocks(n, 256), 256, 0, s>>>(n, b->acc, b->raw, fsc_float, fsc_int);
+        FOS_LAUNCHED(c);
+        return FOS_OK;
+    }
     const long long groups = (n + SUR_GROUP - 1) / SUR_GROUP;
     k_sur_mlp_seg<<<sur_persistent_blocks(c->num_sms, groups), 256, 0, s>>>(
         n, b->pcount, b->pj, b->pnd, rad, b->hist, m->cutoff, m->norm, m->wbf, m->params,
@@ -1393,3 +1694,12 @@ int fos_sur_ens_before_jfa(FosCtx* c, const FosSurrogate* m, const SurEnsGrid& g
 }
 
 const int32_t* fos_sur_fsc_int(FosCtx* c) { return c->sur ? c->sur->fsci : nullptr; }
+
+// Inference kernel of the surrogate on ctx: 0 the mma.sync segment kernel
+// (k_sur_mlp_seg), 1 the tcgen05 / TMEM tile kernel (k_sur_mlp_tc).
+extern "C" int fos_surrogate_set_inference(FosCtx* c, int kind) {
+    FOS_REQUIRE(c, FOS_E_ARG, "ctx is NULL");
+    FOS_REQUIRE(kind == 0 || kind == 1, FOS_E_ARG, "kind must be 0 (mma.sync) or 1 (tcgen05)");
+    c->sur_tc = kind;
+    return FOS_OK;
+}

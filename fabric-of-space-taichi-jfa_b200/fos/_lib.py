@@ -228,6 +228,7 @@ SIGNATURES = {
     "fos_device_error_clear": [_P, _P],
     "fos_test_barrier_plan": [_P, _I, _P],
     "fos_set_jfa_staging": [_P, _I],
+    "fos_surrogate_set_inference": [_P, _I],
     "fos_set_jfa_multi_voxel": [_P, _I],
     "fos_status_string": [_I],
     "fos_last_error": [],

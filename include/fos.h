@@ -478,6 +478,15 @@ typedef struct FosSurrogateStats {
 #define FOS_SUR_ABSOLUTE 0
 #define FOS_SUR_ANCHORED 1
 int fos_surrogate_set_mode(FosCtx* ctx, int mode);
+/* The inference kernel on ctx: FOS_SUR_TCGEN05 (the default) runs 128-pair
+ * tiles on the 5th-generation tensor cores (tcgen05.mma into TMEM, read back
+ * with tcgen05.ld); FOS_SUR_MMA_SYNC runs warp-level mma.sync m16n8k16 tiles
+ * of 16 pairs.  Both round inputs and hidden activations to BF16 and
+ * accumulate in FP32; the FP32 sums run in different orders, so the
+ * probabilities agree to a few ulps, not bit for bit. */
+#define FOS_SUR_MMA_SYNC 0
+#define FOS_SUR_TCGEN05 1
+int fos_surrogate_set_inference(FosCtx* ctx, int kind);
 
 /* A model on `device` with candidate cutoff `cutoff` (in units of r_i + r_j).
  * Weights start at zero; set them with fos_surrogate_set_weights. */

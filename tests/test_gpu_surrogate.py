@@ -217,6 +217,8 @@ def test_predict_sums_pair_probabilities():
     params, _, _ = _random_model(4)
     sur.set_weights(params, np.zeros(16, np.float32) + 5.0, np.ones(16, np.float32) * 10.0)
     S.build_pairs(ctx, sur, pos, rad, foam.n, foam.r_max, cs, cc, ci)
+    from fos._lib import call
+    call("fos_surrogate_set_inference", ctx.h, 0)  # mma.sync: the same tiles as forward()
     out = S.predict(ctx, sur, rad, foam.n, with_pairs=True)
     d = S.export(ctx, rad, labels=False)
     P, _ = S.pair_count(ctx)
@@ -304,3 +306,63 @@ def test_surrogate_graph_equals_direct(mode):
         sim.ctx.close()
     for x, y in zip(*outs):
         assert torch.equal(x, y)
+
+
+def test_tcgen05_inference_matches_mma_sync_and_reference():
+    """The tcgen05 / TMEM inference (128-pair tiles, tcgen05.mma into tensor
+    memory, tcgen05.ld back) against the mma.sync kernel on the same pairs and
+    against the torch BF16 reference on the exported rows.  The two kernels
+    sum in different FP32 orders, and a hidden unit can land on the other
+    side of a BF16 rounding boundary, so they agree within the reference's
+    tolerance, not bit for bit."""
+    from fos._lib import call
+    foam = inputs.headline()
+    cfg, ctx, sur, pos, rad, cc, cs, ci = _grid(foam, 2.5)
+    n = foam.n
+    ctx.jfa_run(pos, rad, n)
+    params, mu, sd = _random_model(4, scale=3.0)
+    sur.set_weights(params, mu, sd)
+    S.build_pairs(ctx, sur, pos, rad, n, foam.r_max, cs, cc, ci)
+    call("fos_surrogate_set_inference", ctx.h, 0)
+    seg = S.predict(ctx, sur, rad, n, with_pairs=True)
+    call("fos_surrogate_set_inference", ctx.h, 1)
+    tc = S.predict(ctx, sur, rad, n, with_pairs=True)
+    torch.cuda.synchronize()
+    assert ctx.device_error() == 0
+    P, _ = S.pair_count(ctx)
+    assert P > 100_000
+    p_seg = seg["prob"][:P].cpu().numpy()
+    p_tc = tc["prob"][:P].cpu().numpy()
+    d = np.abs(p_tc - p_seg)
+    assert d.max() <= 4e-3 and d.mean() <= 2e-5, (d.max(), d.mean())
+    X = S.export(ctx, rad, labels=False)["X"].cpu().numpy()
+    ref = R.mlp_forward_bf16(X, params, mu, sd).numpy()
+    # the memory features (fsc sums) standardise to large values here, where a
+    # BF16 rounding of an input or hidden unit moves a probability by up to
+    # ~1e-2; the tcgen05 kernel stays as close to the reference as mma.sync
+    err, err_seg = np.abs(p_tc - ref), np.abs(p_seg - ref)
+    assert err.max() <= max(2e-3, 1.5 * err_seg.max()), (err.max(), err_seg.max())
+    assert err.mean() <= 2e-4, err.mean()
+    f = np.abs(tc["fsc_float"].cpu().numpy() - seg["fsc_float"].cpu().numpy())
+    assert f.max() <= 0.02
+    ctx.close()
+
+
+def test_tcgen05_frames_run_clean():
+    """Surrogate frames with the tcgen05 inference: graph capture, the TMEM
+    allocation of every CTA freed (later frames allocate again), no device
+    error."""
+    from fos._lib import call
+    sur = S.Surrogate(seed=3)
+    sim = FoamSim.from_foam(inputs.small(), surrogate=sur, surrogate_mode="absolute",
+                            policy=S.RefreshPolicy(every=4, warm_frames=2, min_exact=0.0,
+                                                   max_mean_abs_err=math.inf),
+                            JFA_WARM_FRAMES=2, JFA_CADENCE=4)
+    call("fos_surrogate_set_inference", sim.ctx.h, 1)
+    sim.initialize()
+    for _ in range(12):
+        sim.step()
+    torch.cuda.synchronize()
+    assert sim.ctx.device_error() == 0
+    assert torch.isfinite(sim.fsc_ema).all()
+    sim.ctx.close()
