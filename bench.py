@@ -46,7 +46,8 @@ def parse():
     ap.add_argument("--impl", default="fos", choices=["fos", "reference"])
     ap.add_argument("--cpu-sample-steps", type=int, default=1)
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--profile", default=None, choices=["jfa", "frame", "surrogate", "ensemble"],
+    ap.add_argument("--profile", default=None,
+                    choices=["jfa", "frame", "surrogate", "ensemble", "inference"],
                     help="stage-timing mode for profiling (one small JSON line)")
     ap.add_argument("--reps", type=int, default=5)
     ap.add_argument("--workload", default="headline", choices=["small", "headline", "stress"])
@@ -1050,6 +1051,34 @@ def run_profile(args):
         out["ms_per_frame"] = round(a.elapsed_time(b) / 5, 4)
         out["workload"] = "ensemble-64"
         ens.close()
+    elif args.profile == "inference":
+        # surrogate inference alone on the candidate pairs of the headline foam
+        # at frame 60 (a seeded random model): 3 rounds of 1 + 20 predict calls
+        # with the mma.sync kernel, then 1 + 20 with the tcgen05 kernel
+        from fos import surrogate as S
+        from fos._lib import call
+        sim = FoamSim.from_foam(foam)
+        sim.initialize()
+        sim.run(60)
+        torch.cuda.synchronize()
+        sur = S.Surrogate(seed=3)
+        ctx, n = sim.ctx, foam.n
+        S.build_pairs(ctx, sur, sim.pos, sim.rad, n, float(sim.cfg.R_MAX), sim.cell_start,
+                      sim.cell_count, sim.cell_indices)
+        out["pairs"] = S.pair_count(ctx)[0]
+        for rnd in range(3):
+            for kind in (0, 1):
+                call("fos_surrogate_set_inference", ctx.h, kind)
+                S.predict(ctx, sur, sim.rad, n)
+                a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                a.record(s)
+                for _ in range(20):
+                    S.predict(ctx, sur, sim.rad, n)
+                b.record(s)
+                b.synchronize()
+                key = "tcgen05_us" if kind else "mma_sync_us"
+                out.setdefault(key, []).append(round(a.elapsed_time(b) / 20 * 1000, 2))
+        out["device_error"] = ctx.device_error()
     elif args.profile == "surrogate":
         # 20 steady-state surrogate frames (2 refresh cycles) between
         # cudaProfilerStart/Stop, for `ncu --profile-from-start off`; the
