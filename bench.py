@@ -46,6 +46,10 @@ def parse():
     ap.add_argument("--impl", default="fos", choices=["fos", "reference"])
     ap.add_argument("--cpu-sample-steps", type=int, default=1)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--jfa-form", default="multi", choices=["multi", "single", "staged", "label"],
+                    help="JFA pass form for --profile jfa / frame: four voxels a thread "
+                         "(default), one, TMA-staged rows, or the label-gather pass (the "
+                         "lower-index tie rule)")
     ap.add_argument("--profile", default=None,
                     choices=["jfa", "frame", "surrogate", "ensemble", "inference"],
                     help="stage-timing mode for profiling (one small JSON line)")
@@ -1006,9 +1010,15 @@ def run_profile(args):
     foam = inputs.WORKLOADS[args.workload]()
     s = torch.cuda.current_stream()
     out = {"profile": args.profile, "workload": foam.name, "reps": args.reps}
+    form_cfg = {"TIE_LOWER_INDEX": True} if args.jfa_form == "label" else {}
+
+    def set_form(ctx):
+        ctx.set_jfa_multi_voxel(0 if args.jfa_form in ("single", "staged") else 1)
+        ctx.set_jfa_staging(args.jfa_form == "staged")
     if args.profile == "jfa":
-        cfg = FosConfig.for_foam(foam)
+        cfg = FosConfig.for_foam(foam, **form_cfg)
         ctx = Context(cfg, max_n=foam.n, max_res=cfg.JFA_RES)
+        set_form(ctx)
         f = np.float32
         p = foam.pos - np.floor(foam.pos + f(0.5))
         pos = torch.as_tensor(np.ascontiguousarray(p, np.float32)).cuda()
@@ -1106,7 +1116,8 @@ def run_profile(args):
                                                               "pairs")}
                          for d in sim.policy.judged[-2:]]
     else:
-        sim = FoamSim.from_foam(foam, use_graph=True)
+        sim = FoamSim.from_foam(foam, use_graph=True, **form_cfg)
+        set_form(sim.ctx)
         sim.initialize()
         for _ in range(min(foam.jfa_warm, 25)):
             sim.step()
