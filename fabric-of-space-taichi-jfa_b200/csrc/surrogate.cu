@@ -134,6 +134,18 @@ __device__ __forceinline__ void sur_pairs_warp(int kk, int lane, const float4* _
     int cnt = 0;
     const int z0 = wrap_mod(hz + r0, G);
     const int len1 = span < G - z0 ? span : G - z0;
+    // Cells beyond reach_dist = cutoff * (r_i + r_max) of the particle hold no
+    // candidate: a column whose nearest point in x-y is farther is skipped,
+    // and each other column's z run is trimmed to the cells its z-extent
+    // reaches (bounds from the particle's offset in its home cell, less a
+    // margin for float error; the run stays in the same cyclic order, so the
+    // candidates are a subsequence of the untrimmed walk).  Needs span < G,
+    // so that each offset is a distinct cell.
+    const bool trim = span < G;
+    const float margin = 1e-5f * g.L + 1e-6f;
+    const float rd = cutoff * (me.w + r_max) * 1.0001f + margin;
+    const float rel[3] = {wx - ((float)hx * cellw - g.halfL), wy - ((float)hy * cellw - g.halfL),
+                          wz - ((float)hz * cellw - g.halfL)};
     // The span x span columns each hold a z run of one or two contiguous
     // cell ranges ("pieces").  32 pieces at a time: each lane loads one
     // piece's particle range, a warp scan lays the ranges end to end, and the
@@ -148,8 +160,34 @@ __device__ __forceinline__ void sur_pairs_warp(int kk, int lane, const float4* _
         if (pc < npieces) {
             const int col = pc >> 1, piece = pc & 1;
             const int ox = col / span, oy = col - (col / span) * span;
-            const int za = piece == 0 ? z0 : 0;
-            const int zl = piece == 0 ? len1 : span - len1;
+            int za = piece == 0 ? z0 : 0;
+            int zl = piece == 0 ? len1 : span - len1;
+            if (trim) {
+                const int o2[2] = {r0 + ox, r0 + oy};
+                float bxy2 = 0.f;
+#pragma unroll
+                for (int a = 0; a < 2; ++a) {
+                    const int o = o2[a];
+                    float b = o == 0 ? 0.f
+                                     : (o < 0 ? rel[a] + (float)(-o - 1) * cellw
+                                              : (cellw - rel[a]) + (float)(o - 1) * cellw);
+                    b = fmaxf(0.f, b - margin);
+                    bxy2 += b * b;
+                }
+                if (bxy2 > rd * rd) {
+                    zl = 0;
+                } else {
+                    const float sz = sqrtf(rd * rd - bxy2) + margin;
+                    const int kneg = min(reach, max(0, (int)floorf((sz - rel[2]) / cellw) + 1));
+                    const int kpos =
+                        min(reach, max(0, (int)floorf((sz - (cellw - rel[2])) / cellw) + 1));
+                    const int length = kneg + kpos + 1;
+                    const int zs = wrap_mod(hz - kneg, G);
+                    const int l1 = length < G - zs ? length : G - zs;
+                    za = piece == 0 ? zs : 0;
+                    zl = piece == 0 ? l1 : length - l1;
+                }
+            }
             if (zl > 0) {
                 const int nx = wrap_mod(hx + r0 + ox, G);
                 const int ny = wrap_mod(hy + r0 + oy, G);
