@@ -371,21 +371,29 @@ __device__ bool coop_grid(const Args& a, const Geo& geo, const float* src, float
     if (tid == 0) atomicAnd(&a.ds->grid_ovf, ~(1 << (par ^ 1)));
     if (a.cfix && !want_csr && !ovf && rad) {
         // fixed-capacity rows: sort each cell's (<= COOP_CAP) arrivals by
-        // index.  A warp takes two cells per round and loads both rows whole
-        // (slots past the count hold stale entries and are ignored) together
-        // with the counts, so a round waits for one load latency.
+        // index.  A warp takes two cells per round; their counts are loaded
+        // one round ahead, so a round waits for one load latency, and only
+        // the occupied slots of a row are read (the slots past the count hold
+        // stale entries that would mostly come from DRAM).
         const int lane = threadIdx.x & 31, W = T >> 5, wid = tid >> 5;
+        int mn[2];
+#pragma unroll
+        for (int h = 0; h < 2; ++h) mn[h] = wid + h * W < a.G3 ? __ldcg(&cnt[wid + h * W]) : 0;
         for (int c0 = wid; c0 < a.G3; c0 += 2 * W) {
             const int cc2[2] = {c0, c0 + W};
             int m[2], id[2];
             float4 pr[2];
 #pragma unroll
             for (int h = 0; h < 2; ++h) {
-                const bool ok = cc2[h] < a.G3;  // warp-uniform
-                const size_t base = (size_t)(ok ? cc2[h] : 0) * COOP_CAP;
-                m[h] = ok ? __ldcg(&cnt[cc2[h]]) : 0;  // <= COOP_CAP
-                id[h] = ok ? __ldcg(&a.cfix[base + lane]) : 0;
-                pr[h] = ok ? __ldcg(&a.spst[base + lane]) : make_float4(0.f, 0.f, 0.f, 0.f);
+                m[h] = mn[h];  // <= COOP_CAP; 0 past the table
+                const int cn = c0 + (2 + h) * W;
+                mn[h] = cn < a.G3 ? __ldcg(&cnt[cn]) : 0;
+            }
+#pragma unroll
+            for (int h = 0; h < 2; ++h) {
+                const size_t base = (size_t)cc2[h] * COOP_CAP;
+                id[h] = lane < m[h] ? __ldcg(&a.cfix[base + lane]) : 0;
+                pr[h] = lane < m[h] ? __ldcg(&a.spst[base + lane]) : make_float4(0.f, 0.f, 0.f, 0.f);
             }
 #pragma unroll
             for (int h = 0; h < 2; ++h) {

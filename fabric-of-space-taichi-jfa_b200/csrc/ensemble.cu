@@ -46,7 +46,7 @@ struct EnsWords {  // per-foam device words
     int settle;
     int zero_fsc;
     unsigned int omax_bits;
-    int pad;
+    unsigned int rmax_bits;      // the foam's largest radius after the pressure sweeps
     unsigned long long rad_sum;  // OU jitter: the foam's radii, 2^-40 fixed point (exact)
     unsigned long long changes[FOS_MAX_PASSES];
 };
@@ -462,12 +462,17 @@ __device__ __forceinline__ void ens_pbd(const EnsArgs& a, const EnsGeo& geo, con
         const int kk = kk_next;
         kk_next = i + W_ < a.n ? __ldcg(&a.slot_of[i + W_]) : 0;
         if (i < a.n) {  // warp-uniform
-            const EnsFoamDev& d = a.F[a.foam_of[i]];
+            const int f = a.foam_of[i];
+            const EnsFoamDev& d = a.F[f];
             const GridGeom g{d.G, a.L, a.invL, a.halfL};
+            // the stencil skips the cells beyond reach of the foam's largest
+            // radius (set in the Brownian phase; radii are fixed during PBD)
+            const float rmax = d.G >= 5 ? __uint_as_float(__ldcg(&a.W[f].rmax_bits)) : 0.f;
             float4 nv = make_float4(0.f, 0.f, 0.f, 0.f);
             int pi = pbd_warp<LdL2>(kk, lane, lay.sp, lay.ci, a.pos_tmp, g,
                                     lay.cs ? lay.cs + d.cell_off : nullptr, lay.cc + d.cell_off,
-                                    a.gap1, a.mdf, a.dmul, &nv, lay.cap, d.cell_off);
+                                    a.gap1, a.mdf, a.dmul, &nv, lay.cap, d.cell_off, rmax,
+                                    a.L / (float)d.G);
             if (p1) d1.put(a, geo, lane, pi, nv, a.pos, coop_p1_par(a, par), ou);
         }
     }
@@ -570,10 +575,25 @@ __global__ void __launch_bounds__(THREADS) k_ens_coop(EnsArgs a) {
     // for its mean radius (run.py:860-861).
     for (int i = tid; i < a.n; i += T) {
         if (a.sweeps & 1) a.rad[i] = __ldcg(&a.rad_tmp[i]);
-        const EnsFoamDev& d = a.F[a.foam_of[i]];
-        if (a.ou)
-            atomicAdd(&a.W[a.foam_of[i]].rad_sum,
-                      (unsigned long long)rad_fixed(__ldcg(&a.rad[i])));
+        const int f = a.foam_of[i];
+        const EnsFoamDev& d = a.F[f];
+        const float r_i = __ldcg(&a.rad[i]);
+        if (a.ou) atomicAdd(&a.W[f].rad_sum, (unsigned long long)rad_fixed(r_i));
+        // the foam's largest radius (positive floats order as their bits):
+        // one atomic per warp when its particles share a foam (foams are
+        // contiguous index ranges), else one per particle
+        {
+            const unsigned int am = __activemask();
+            const unsigned int rb = __float_as_uint(r_i);
+            const int f0 = __shfl_sync(am, f, __ffs(am) - 1);
+            if (__all_sync(am, f == f0)) {
+                const unsigned int wm = __reduce_max_sync(am, rb);
+                if (lane == __ffs(am) - 1 && wm > __ldcg(&a.W[f].rmax_bits))
+                    atomicMax(&a.W[f].rmax_bits, wm);
+            } else {
+                atomicMax(&a.W[f].rmax_bits, rb);
+            }
+        }
         brownian_one<LdL2>(i, (unsigned int)(i - d.part_off), a.pos, a.strength, a.domain, a.halfL,
                            d.k0, d.k1, (unsigned int)frame);
         coop_p1_one(a, geo, i, a.pos, a.rad, a.pos, coop_p1_par(a, gk & 1));
@@ -608,6 +628,7 @@ __global__ void k_ens_coop_prep(FosDevState* ds, EnsWords* W, int nf) {
     int f = blockIdx.x * blockDim.x + threadIdx.x;
     if (f < nf) {
         W[f].omax_bits = 0u;
+        W[f].rmax_bits = 0u;
         W[f].rad_sum = 0ull;
     }
     if (f == 0) {

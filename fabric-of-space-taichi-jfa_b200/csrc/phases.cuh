@@ -145,12 +145,15 @@ struct GridGeom {
 // the 1e-7 offset of the cell assignment; a cell whose squared bound exceeds
 // reach2 is skipped.  The other candidates keep their stencil order, so any
 // pair within reach is enumerated exactly as by stencil_ranges.  Needs G >= 5,
-// so that the adjacent cells are the nearest periodic images.
+// so that the adjacent cells are the nearest periodic images.  cap == 0: the
+// CSR form, cell cid starting at cstart[cid]; cell_base as in stencil_ranges.
 template <class LD>
 __device__ __forceinline__ Stencil stencil_ranges_near(float px, float py, float pz,
                                                        const GridGeom& g, float cs,
                                                        const int32_t* cc, int lane, int cap,
-                                                       float reach2, float margin) {
+                                                       float reach2, float margin,
+                                                       const int32_t* cstart = nullptr,
+                                                       int cell_base = 0) {
     const float p3[3] = {px, py, pz};
     int h[3];
     float rel[3];
@@ -167,14 +170,16 @@ __device__ __forceinline__ Stencil stencil_ranges_near(float px, float py, float
         const int ny = wrap_near(h[1] + o[1], g.G);
         const int nz = wrap_near(h[2] + o[2], g.G);
         const int cid = (nx * g.G + ny) * g.G + nz;
-        st = cid * cap;
         float b2 = 0.f;
 #pragma unroll
         for (int a = 0; a < 3; ++a) {
             const float b = o[a] == 0 ? 0.f : fmaxf(0.f, (o[a] < 0 ? rel[a] : cs - rel[a]) - margin);
             b2 += b * b;
         }
-        ct = b2 > reach2 ? 0 : LD::ld(&cc[cid]);
+        if (b2 <= reach2) {
+            st = cap ? (cell_base + cid) * cap : LD::ld(&cstart[cid]);
+            ct = LD::ld(&cc[cid]);
+        }
     }
     int incl = ct;
 #pragma unroll
@@ -281,16 +286,27 @@ __device__ __forceinline__ float3 pbd_move(float px, float py, float pz, float r
 // sum bit for bit.  Must be called by all 32 lanes.
 // Returns particle i to lane 0 (-1 to the other lanes); with np != NULL,
 // lane 0 also gets the new (wrapped) position and the radius in *np.
-// cap / cell_base as in stencil_ranges.
+// cap / cell_base as in stencil_ranges.  rmax > 0 (the largest radius of any
+// candidate; G >= 5): only the cells that can hold a particle within
+// (ri + rmax) * gap1 are visited, as in pbd_warp_rows; the candidates left keep
+// their order, so the hits and their sum are unchanged.
 template <class LD>
 __device__ __forceinline__ int pbd_warp(int kk, int lane, const float4* sp, const int32_t* ci,
                                         float* pout, const GridGeom g, const int32_t* cs,
                                         const int32_t* cc, float gap1, float mdf, float dmul,
-                                        float4* np = nullptr, int cap = 0, int cell_base = 0) {
+                                        float4* np = nullptr, int cap = 0, int cell_base = 0,
+                                        float rmax = 0.f, float cell_w = 0.f) {
     float4 me = LD::ld(&sp[kk]);
     float px = me.x, py = me.y, pz = me.z, ri = me.w;
-    Stencil r = stencil_ranges<LD>(px, py, pz, g.L, g.invL, g.halfL, g.G, cs, cc, lane, cap,
-                                   cell_base);
+    Stencil r;
+    if (rmax > 0.f) {
+        const float reach = (ri + rmax) * gap1 * 1.0001f;
+        r = stencil_ranges_near<LD>(px, py, pz, g, cell_w, cc, lane, cap, reach * reach,
+                                    1e-5f * g.L + 1e-6f, cs, cell_base);
+    } else {
+        r = stencil_ranges<LD>(px, py, pz, g.L, g.invL, g.halfL, g.G, cs, cc, lane, cap,
+                               cell_base);
+    }
     float md = fmul(mdf, ri);
     float cx = 0.f, cy = 0.f, cz = 0.f;
     for (int base = 0; base < r.total; base += 32) {
@@ -386,9 +402,9 @@ __device__ __forceinline__ float maxov_term(float4 q, float4 me, float eps, cons
 // compute_local_max_overlaps (dynamics.py:304-352) for the particle at
 // sorted position kk (pairs i < j only); writes lmd[i] and returns the depth's
 // float bits (non-negative floats order as their bits).  All 32 lanes.
-// rmax > 0 (fixed-capacity rows, cell_base 0, G >= 5; rmax the largest
-// radius): only the cells that can hold a particle within ri + rmax, the
-// only ones with a positive depth, are visited (stencil_ranges_near).
+// rmax > 0 (G >= 5; rmax the largest radius): only the cells that can hold a
+// particle within ri + rmax, the only ones with a positive depth, are visited
+// (stencil_ranges_near).
 template <class LD>
 __device__ __forceinline__ unsigned int maxov_warp(int kk, int lane, const float4* sp,
                                                    const int32_t* ci, const GridGeom g,
@@ -401,7 +417,7 @@ __device__ __forceinline__ unsigned int maxov_warp(int kk, int lane, const float
     if (rmax > 0.f) {
         const float reach = (me.w + rmax) * 1.0001f;
         r = stencil_ranges_near<LD>(me.x, me.y, me.z, g, cell_w, cc, lane, cap, reach * reach,
-                                    1e-5f * g.L + 1e-6f);
+                                    1e-5f * g.L + 1e-6f, cs, cell_base);
     } else {
         r = stencil_ranges<LD>(me.x, me.y, me.z, g.L, g.invL, g.halfL, g.G, cs, cc, lane, cap,
                                cell_base);
