@@ -434,6 +434,7 @@ struct EnsArgs {
     float* delta_r;
     float* vol0;  // [n] r^P ping-pong of the pressure sweeps
     float* vol1;
+    int32_t* pnbr;  // [16 n] the frame's pressure neighbours (pressure_nbr_fill)
     float gap1, mdf, dmul, eps, contact_tol;
     double contact_tol_d;
     float alpha, max_step;
@@ -529,9 +530,17 @@ __global__ void __launch_bounds__(THREADS) k_ens_coop(EnsArgs a) {
     }
     if (!grid_barrier(a.ds, ep)) return;
     // (3) settle nudge of the foams whose settle counter is > 0; each final
-    // radius's power r^P seeds the pressure sweeps
+    // radius's power r^P seeds the pressure sweeps, and each particle's
+    // neighbours of the sweeps go to the table (its foam's hash offset)
+    const int frame = *((volatile int*)&a.ds->frame);
     for (int i = tid; i < a.n; i += T) {
         const int f = a.foam_of[i];
+        if (a.sweeps > 0) {
+            PressureArgs pa = a.pa;
+            pa.frame = frame;
+            pa.hoff = a.F[f].part_off;
+            pressure_nbr_fill<LdL2>(i, pa, a.pnbr);
+        }
         float r = __ldcg(&a.rad[i]);
         if (*((volatile int*)&a.W[f].settle) > 0) {
             const EnsFoamDev& d = a.F[f];
@@ -544,8 +553,8 @@ __global__ void __launch_bounds__(THREADS) k_ens_coop(EnsArgs a) {
         if (a.sweeps > 0) a.vol0[i] = pow_P(r, a.pa.P);
     }
     if (!grid_barrier(a.ds, ep)) return;
-    // (4) pressure sweeps with each foam's bounds and local hash index
-    const int frame = *((volatile int*)&a.ds->frame);
+    // (4) pressure sweeps with each foam's bounds, on the neighbour table; two
+    // rounds at a time, both groups' loads before either sum
     {
         const int groups_per_round = T / 8;
         const int p_rounds = (a.n + groups_per_round - 1) / groups_per_round;
@@ -554,18 +563,21 @@ __global__ void __launch_bounds__(THREADS) k_ens_coop(EnsArgs a) {
             float* rout = (w & 1) ? a.rad : a.rad_tmp;
             const float* vin = (w & 1) ? a.vol1 : a.vol0;
             float* vout = (w == a.sweeps - 1) ? nullptr : ((w & 1) ? a.vol0 : a.vol1);
-            for (int r = 0; r < p_rounds; ++r) {
-                int i = r * groups_per_round + tid / 8;
-                PressureArgs pa = a.pa;
-                pa.frame = frame;
-                if (i < a.n) {
-                    const EnsFoamDev& d = a.F[a.foam_of[i]];
-                    pa.rmin = d.r_min;
-                    pa.rmax = d.r_max;
-                    pa.hoff = d.part_off;
+            for (int r = 0; r < p_rounds; r += 2) {
+                const int i0 = r * groups_per_round + tid / 8, i1 = i0 + groups_per_round;
+                const PressureIn p0 = pressure_in8x2n<LdL2>(i0, lane, a.n, a.pnbr, rin, vin);
+                const PressureIn p1 = pressure_in8x2n<LdL2>(i1, lane, a.n, a.pnbr, rin, vin);
+                float2 b0 = make_float2(0.f, 0.f), b1 = make_float2(0.f, 0.f);
+                if (i0 < a.n) {
+                    const EnsFoamDev& d = a.F[a.foam_of[i0]];
+                    b0 = make_float2(d.r_min, d.r_max);
                 }
-                const PressureNbr nb = pressure_nbr8x2<LdL2>(i, lane, pa);
-                pressure_sweep8x2v<LdL2>(i, lane, pa, nb, rin, vin, rout, vout, a.delta_r);
+                if (i1 < a.n) {
+                    const EnsFoamDev& d = a.F[a.foam_of[i1]];
+                    b1 = make_float2(d.r_min, d.r_max);
+                }
+                pressure_out8x2n(i0, lane, a.n, a.pa, p0, b0.x, b0.y, rout, vout, a.delta_r);
+                pressure_out8x2n(i1, lane, a.n, a.pa, p1, b1.x, b1.y, rout, vout, a.delta_r);
             }
             if (!grid_barrier(a.ds, ep)) return;
         }
@@ -980,6 +992,7 @@ static int ens_coop_launch(FosEnsemble* e, int mode, cudaStream_t s) {
     a.delta_r = e->delta_r;
     a.vol0 = c->pvol;
     a.vol1 = c->pvol + c->max_n;
+    a.pnbr = c->pnbr;
     a.gap1 = c->gap1;
     a.mdf = c->mdf;
     a.dmul = c->dmul;

@@ -210,6 +210,7 @@ extern "C" int fos_ctx_create(const FosParams* p, int max_n, int max_res, int de
     ALLOC(c->rank, (size_t)max_n * 4);
     ALLOC(c->coop_slot, (size_t)max_n * 4);
     ALLOC(c->pvol, (size_t)max_n * 8);
+    ALLOC(c->pnbr, (size_t)max_n * 16 * 4);
     c->ptag_n = max_n < FOS_PTAG_MAX_N ? max_n : FOS_PTAG_MAX_N;
     ALLOC(c->ptag, (size_t)(FOS_PTAG_SWEEPS + 1) * c->ptag_n * 8);
     {
@@ -278,7 +279,7 @@ extern "C" int fos_ctx_destroy(FosCtx* c) {
                     c->fin_changed, c->sorted, c->ci_tmp, c->coop_bsum, c->coop_cnt,
                     c->coop_part, c->coop_cnt2, c->coop_cfix, c->coop_idsort, c->coop_spfix,
                     c->coop_spst,
-                    c->coop_slot, c->skip_part, c->pvol, c->ptag};
+                    c->coop_slot, c->skip_part, c->pvol, c->pnbr, c->ptag};
     for (void* q : ptrs)
         if (q) cudaFree(q);
     if (c->pinned) cudaFreeHost(c->pinned);

@@ -134,6 +134,7 @@ struct FosCtx {
     int coop_fixed = 0;               // the fixed-capacity rows are allocated
     int32_t* coop_slot = nullptr;     // [max_n] slot of each particle in the last rebuild
     float* pvol = nullptr;            // [2 * max_n] r^P ping-pong of the pressure sweeps
+    int32_t* pnbr = nullptr;          // [16 * max_n] a frame's pressure neighbours (sweeps with barriers)
     // tagged r^P words of the cooperative frame's barrier-free pressure sweeps:
     // [(FOS_PTAG_SWEEPS + 1) * ptag_n], zeroed at creation
     unsigned long long* ptag = nullptr;

@@ -43,6 +43,7 @@ struct CoopArgs {
     float* vol0;                // [n] r^P ping-pong of the pressure sweeps
     float* vol1;
     unsigned long long* ptag;   // non-NULL: barrier-free pressure sweeps on tagged words
+    int32_t* pnbr;              // [16 n] the frame's pressure neighbours (sweeps with barriers)
     int32_t* part;
     int32_t* bsum;
     float4* sp;
@@ -298,6 +299,16 @@ __global__ void __launch_bounds__(COOP_THREADS, COOP_BLOCKS_PER_SM) k_frame_coop
         if (!grid_barrier(a.ds, ep)) return;
         trace_mark(a, tk);
     } else {
+    // 8-lane groups, two neighbours per lane: every particle in one round
+    const int groups_per_round = T / 8;
+    const int p_rounds = (a.n + groups_per_round - 1) / groups_per_round;
+    // with one round (n <= T/8) each lane keeps its neighbours in registers
+    // for all sweeps, and the particles are spread over every block, so every
+    // SM issues the same share of the sweep
+    const bool keep_nbr = p_rounds == 1;
+    // with more rounds the nudge phase writes each particle's neighbours to a
+    // table (pressure_nbr_fill) and a sweep takes two rounds at a time
+    const bool table = a.pnbr != nullptr && !keep_nbr;
     // (3) nudge_radii_adaptive_ema while settle_frames_left > 0 (run.py:744-750);
     // each final radius's power r^P seeds the pressure sweeps
     {
@@ -309,18 +320,12 @@ __global__ void __launch_bounds__(COOP_THREADS, COOP_BLOCKS_PER_SM) k_frame_coop
                 a.rad[i] = r;
             }
             if (a.sweeps > 0) a.vol0[i] = pow_P(r, a.pa.P);
+            if (table && a.sweeps > 0) pressure_nbr_fill<LdL2>(i, pa, a.pnbr);
         }
     }
     if (!grid_barrier(a.ds, ep)) return;
     trace_mark(a, tk);
     // (4) pressure sweeps (run.py:755-771); the last sweep reports its stats
-    // 8-lane groups, two neighbours per lane: every particle in one round
-    const int groups_per_round = T / 8;
-    const int p_rounds = (a.n + groups_per_round - 1) / groups_per_round;
-    // with one round (n <= T/8) each lane keeps its neighbours in registers
-    // for all sweeps, and the particles are spread over every block, so every
-    // SM issues the same share of the sweep
-    const bool keep_nbr = p_rounds == 1;
     // four consecutive particles per warp (one sector of each per-particle
     // array), consecutive warps of particles on consecutive blocks
     const int i_one =
@@ -332,6 +337,34 @@ __global__ void __launch_bounds__(COOP_THREADS, COOP_BLOCKS_PER_SM) k_frame_coop
         const float* vin = (w & 1) ? a.vol1 : a.vol0;
         float* vout = (w & 1) ? a.vol0 : a.vol1;
         bool last = (w == a.sweeps - 1);
+        if (table) {
+            // two rounds at a time: both groups' loads before either sum
+            for (int r = 0; r < p_rounds; r += 2) {
+                const int i0 = r * groups_per_round + tid / 8, i1 = i0 + groups_per_round;
+                const PressureIn p0 = pressure_in8x2n<LdL2>(i0, lane, a.n, a.pnbr, rin, vin);
+                const PressureIn p1 = pressure_in8x2n<LdL2>(i1, lane, a.n, a.pnbr, rin, vin);
+                float* vo = last ? nullptr : vout;
+                const float d0 = pressure_out8x2n(i0, lane, a.n, pa, p0, pa.rmin, pa.rmax, rout,
+                                                  vo, a.delta_r);
+                const float d1 = pressure_out8x2n(i1, lane, a.n, pa, p1, pa.rmin, pa.rmax, rout,
+                                                  vo, a.delta_r);
+                if (last) {
+#pragma unroll
+                    for (int h = 0; h < 2; ++h) {
+                        const float ad = fabsf(h ? d1 : d0);
+                        const int ch = ((h ? i1 : i0) < a.n && (lane & 7) == 0) && ad > 1e-12f;
+                        const int cnt = __syncthreads_count(ch);
+                        const unsigned int bm =
+                            __reduce_max_sync(0xffffffffu, ch ? __float_as_uint(ad) : 0u);
+                        block_max_atomic(bm, &a.ds->maxabs_dr_bits);
+                        if (threadIdx.x == 0 && cnt) atomicAdd(&a.ds->changed, cnt);
+                    }
+                }
+            }
+            if (!grid_barrier(a.ds, ep)) return;
+            trace_mark(a, tk);
+            continue;
+        }
         for (int r = 0; r < p_rounds; ++r) {
             const int i = keep_nbr ? i_one : r * groups_per_round + tid / 8;
             const PressureNbr nb = keep_nbr ? nb0 : pressure_nbr8x2<LdL2>(i, lane, pa);
@@ -517,6 +550,8 @@ int fos_frame_coop_dynamics(FosCtx* c, const FosState* st, const FosFrameParams*
     if (c->ptag && n <= c->ptag_n && (long long)n * COOP_PLANES <= (long long)blocks * COOP_THREADS &&
         fp->pressure_iters >= 1 && fp->pressure_iters <= FOS_PTAG_SWEEPS)
         a.ptag = c->ptag;
+    else
+        a.pnbr = c->pnbr;
     a.part = c->coop_part;
     a.bsum = c->coop_bsum;
     a.sp = c->sorted;

@@ -753,6 +753,78 @@ __device__ __forceinline__ float pressure_sweep8x2v(int i, int lane, const Press
     return d;
 }
 
+// The budgeted neighbours of particle i for one frame's pressure sweeps, all
+// sixteen slots at once: nbr[16 i + t] = neighbour t of the hashed rotation
+// (pressure_nbr8x2's choice) or -1 where none takes part (past the budget,
+// invalid, or i itself).  The choice does not change within a frame, so the
+// sweeps then read one coalesced word per neighbour instead of fsc, the
+// rotation and face_ids.  st < fc and t < an <= fc, so (st + t) % fc is
+// st + t less fc once it reaches fc.  Needs max_nei <= 16.
+template <class LD>
+__device__ __forceinline__ void pressure_nbr_fill(int i, const PressureArgs& a, int32_t* nbr) {
+    const int fc = LD::ld(&a.fsc[i]);
+    const int an = fc > 0 ? (fc < a.max_nei ? fc : a.max_nei) : 0;
+    const int st = fc > 0 ? hash_func(i - a.hoff, a.frame) % fc : 0;
+    int v[16];
+#pragma unroll
+    for (int t = 0; t < 16; ++t) {
+        v[t] = -1;
+        if (t < an) {
+            const int ni = st + t >= fc ? st + t - fc : st + t;
+            const int j = LD::ld(&a.face_ids[(size_t)i * FOS_S + ni]);
+            if (!(j < 0 || j >= a.n || j == i)) v[t] = j;
+        }
+    }
+    int4* o = reinterpret_cast<int4*>(nbr + (size_t)i * 16);
+#pragma unroll
+    for (int q = 0; q < 4; ++q) o[q] = make_int4(v[4 * q], v[4 * q + 1], v[4 * q + 2], v[4 * q + 3]);
+}
+
+// One 8-lane group's inputs of a pressure sweep from the frame's neighbour
+// table (pressure_nbr_fill): lane t takes neighbours t and t + 8.  Loading
+// two groups' inputs before either sum keeps two dependent chains in flight.
+struct PressureIn {
+    PressureNbr nb;
+    float ri, Vi, vj0, vj1;
+};
+
+template <class LD>
+__device__ __forceinline__ PressureIn pressure_in8x2n(int i, int lane, int n, const int32_t* nbr,
+                                                      const float* rin, const float* vin) {
+    PressureIn p;
+    const int gl = lane & 7;
+    const bool live = i < n;
+    const int j0 = live ? LD::ld(&nbr[(size_t)i * 16 + gl]) : -1;
+    const int j1 = live ? LD::ld(&nbr[(size_t)i * 16 + gl + 8]) : -1;
+    p.ri = live ? LD::ld(&rin[i]) : 0.f;
+    p.Vi = live ? LD::ld(&vin[i]) : 0.f;
+    p.nb.fc = 1;
+    p.nb.j[0] = j0;
+    p.nb.j[1] = j1;
+    p.nb.ok[0] = j0 >= 0;
+    p.nb.ok[1] = j1 >= 0;
+    p.vj0 = j0 >= 0 ? LD::ld(&vin[j0]) : 0.f;
+    p.vj1 = j1 >= 0 ? LD::ld(&vin[j1]) : 0.f;
+    return p;
+}
+
+// pressure_sweep8x2v's result from PressureIn: a group with no neighbour
+// taking part sums nothing and gets +0, as when fsc[i] == 0.  Lane 0 of the
+// group writes delta_r[i], rout[i] (clamped to [rmin, rmax]) and, with vout,
+// the new power.  All 32 lanes.
+__device__ __forceinline__ float pressure_out8x2n(int i, int lane, int n, const PressureArgs& a,
+                                                  const PressureIn& p, float rmin, float rmax,
+                                                  float* rout, float* vout, float* delta_r) {
+    const float d = pressure_sum8x2(a, p.nb, lane, p.ri, p.Vi, p.vj0, p.vj1);
+    if (i < n && (lane & 7) == 0) {
+        delta_r[i] = d;
+        const float rn = fmaxf(rmin, fminf(rmax, fadd(p.ri, d)));
+        rout[i] = rn;
+        if (vout) vout[i] = pow_P(rn, a.P);
+    }
+    return d;
+}
+
 template <class LD>
 __device__ __forceinline__ float pressure_group8x2(int i, int lane, const PressureArgs a,
                                                    const float* rin, float* rout, float* delta_r) {
