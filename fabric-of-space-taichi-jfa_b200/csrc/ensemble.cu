@@ -388,6 +388,12 @@ __global__ void k_ens_targets(int ntot, const EnsFoamDev* __restrict__ F,
 }
 
 // ------------------------------------------------------------ dynamics
+// Rounds of 8-lane groups in flight in the pressure sweeps: their loads are
+// all issued before the first sum.
+#ifndef ENS_PRESS_ROUNDS
+#define ENS_PRESS_ROUNDS 2
+#endif
+
 struct EnsGeo {
     const EnsFoamDev* F;
     const int32_t* foam_of;
@@ -563,21 +569,25 @@ __global__ void __launch_bounds__(THREADS) k_ens_coop(EnsArgs a) {
             float* rout = (w & 1) ? a.rad : a.rad_tmp;
             const float* vin = (w & 1) ? a.vol1 : a.vol0;
             float* vout = (w == a.sweeps - 1) ? nullptr : ((w & 1) ? a.vol0 : a.vol1);
-            for (int r = 0; r < p_rounds; r += 2) {
-                const int i0 = r * groups_per_round + tid / 8, i1 = i0 + groups_per_round;
-                const PressureIn p0 = pressure_in8x2n<LdL2>(i0, lane, a.n, a.pnbr, rin, vin);
-                const PressureIn p1 = pressure_in8x2n<LdL2>(i1, lane, a.n, a.pnbr, rin, vin);
-                float2 b0 = make_float2(0.f, 0.f), b1 = make_float2(0.f, 0.f);
-                if (i0 < a.n) {
-                    const EnsFoamDev& d = a.F[a.foam_of[i0]];
-                    b0 = make_float2(d.r_min, d.r_max);
+            constexpr int NR = ENS_PRESS_ROUNDS;
+            for (int r = 0; r < p_rounds; r += NR) {
+                int ii[NR];
+                PressureIn pin[NR];
+                float2 bnd[NR];
+#pragma unroll
+                for (int h = 0; h < NR; ++h) {
+                    ii[h] = (r + h) * groups_per_round + tid / 8;
+                    pin[h] = pressure_in8x2n<LdL2>(ii[h], lane, a.n, a.pnbr, rin, vin);
+                    bnd[h] = make_float2(0.f, 0.f);
+                    if (ii[h] < a.n) {
+                        const EnsFoamDev& d = a.F[a.foam_of[ii[h]]];
+                        bnd[h] = make_float2(d.r_min, d.r_max);
+                    }
                 }
-                if (i1 < a.n) {
-                    const EnsFoamDev& d = a.F[a.foam_of[i1]];
-                    b1 = make_float2(d.r_min, d.r_max);
-                }
-                pressure_out8x2n(i0, lane, a.n, a.pa, p0, b0.x, b0.y, rout, vout, a.delta_r);
-                pressure_out8x2n(i1, lane, a.n, a.pa, p1, b1.x, b1.y, rout, vout, a.delta_r);
+#pragma unroll
+                for (int h = 0; h < NR; ++h)
+                    pressure_out8x2n(ii[h], lane, a.n, a.pa, pin[h], bnd[h].x, bnd[h].y, rout, vout,
+                                     a.delta_r);
             }
             if (!grid_barrier(a.ds, ep)) return;
         }

@@ -80,6 +80,11 @@ __device__ __forceinline__ unsigned long long ld_tagged(const unsigned long long
 #ifndef COOP_PLANES
 #define COOP_PLANES 8
 #endif
+// Rounds of 8-lane groups in flight in the pressure sweeps with grid barriers
+// (n > threads / 8): their loads are all issued before the first sum.
+#ifndef COOP_PRESS_ROUNDS
+#define COOP_PRESS_ROUNDS 2
+#endif
 // Pause between two polls of a word that is not ready yet, in ns (fewer L2
 // requests from waiting warps).
 #ifndef COOP_POLL_NS
@@ -338,21 +343,28 @@ __global__ void __launch_bounds__(COOP_THREADS, COOP_BLOCKS_PER_SM) k_frame_coop
         float* vout = (w & 1) ? a.vol0 : a.vol1;
         bool last = (w == a.sweeps - 1);
         if (table) {
-            // two rounds at a time: both groups' loads before either sum
-            for (int r = 0; r < p_rounds; r += 2) {
-                const int i0 = r * groups_per_round + tid / 8, i1 = i0 + groups_per_round;
-                const PressureIn p0 = pressure_in8x2n<LdL2>(i0, lane, a.n, a.pnbr, rin, vin);
-                const PressureIn p1 = pressure_in8x2n<LdL2>(i1, lane, a.n, a.pnbr, rin, vin);
+            // COOP_PRESS_ROUNDS rounds at a time: every group's loads before
+            // the first sum
+            constexpr int NR = COOP_PRESS_ROUNDS;
+            for (int r = 0; r < p_rounds; r += NR) {
+                int ii[NR];
+                PressureIn pin[NR];
+#pragma unroll
+                for (int h = 0; h < NR; ++h) {
+                    ii[h] = (r + h) * groups_per_round + tid / 8;
+                    pin[h] = pressure_in8x2n<LdL2>(ii[h], lane, a.n, a.pnbr, rin, vin);
+                }
                 float* vo = last ? nullptr : vout;
-                const float d0 = pressure_out8x2n(i0, lane, a.n, pa, p0, pa.rmin, pa.rmax, rout,
-                                                  vo, a.delta_r);
-                const float d1 = pressure_out8x2n(i1, lane, a.n, pa, p1, pa.rmin, pa.rmax, rout,
-                                                  vo, a.delta_r);
+                float dd[NR];
+#pragma unroll
+                for (int h = 0; h < NR; ++h)
+                    dd[h] = pressure_out8x2n(ii[h], lane, a.n, pa, pin[h], pa.rmin, pa.rmax, rout,
+                                             vo, a.delta_r);
                 if (last) {
 #pragma unroll
-                    for (int h = 0; h < 2; ++h) {
-                        const float ad = fabsf(h ? d1 : d0);
-                        const int ch = ((h ? i1 : i0) < a.n && (lane & 7) == 0) && ad > 1e-12f;
+                    for (int h = 0; h < NR; ++h) {
+                        const float ad = fabsf(dd[h]);
+                        const int ch = (ii[h] < a.n && (lane & 7) == 0) && ad > 1e-12f;
                         const int cnt = __syncthreads_count(ch);
                         const unsigned int bm =
                             __reduce_max_sync(0xffffffffu, ch ? __float_as_uint(ad) : 0u);
