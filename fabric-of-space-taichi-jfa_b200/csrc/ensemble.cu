@@ -288,7 +288,10 @@ __global__ void __launch_bounds__(256, 4)
         bd[m] = fminf(power_dist_unit2m(make_float2(vx[m], vy), vz, __ldg(&rin[l])), 1e10f);
         bl[m] = l;
     }
-    recx_scan<M>(rin, xp, ys, zs, vx, vy, vz, bd, bl);
+    if (M == 2 && 2 * step == R)  // block-uniform: a block covers one foam
+        recx_scan<M, true>(rin, xp, ys, zs, vx, vy, vz, bd, bl);
+    else
+        recx_scan<M>(rin, xp, ys, zs, vx, vy, vz, bd, bl);
 #pragma unroll
     for (int m = 0; m < M; ++m) {
         const int l = xp[m + 1] + ys[1] + zs[1];

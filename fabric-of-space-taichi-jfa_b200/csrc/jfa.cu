@@ -105,8 +105,9 @@ __global__ void __launch_bounds__(256, UNIT_L ? 6 : 4) k_jfa_pass_rec(const int3
 // coalesced 512-byte row.  Planes are visited in increasing x and rows in
 // (dy, dz) order, so each voxel sees its own record first and then the 26
 // others in the reference's (dx, dy, dz) order, with the same arithmetic as
-// jfa_rec_core.
-template <int M>
+// jfa_rec_core.  HALF: the step is R / 2, where only the offsets {-1, 0}^3
+// give distinct candidates (recx_scan).
+template <int M, bool HALF = false>
 __global__ void __launch_bounds__(256, 4)
     k_jfa_pass_recx(const int32_t* __restrict__ in, const float4* __restrict__ rin,
                     int32_t* __restrict__ out, float4* __restrict__ rout, int lgR, int lgS,
@@ -140,7 +141,7 @@ __global__ void __launch_bounds__(256, 4)
         bd[m] = fminf(power_dist_unit2m(make_float2(vx[m], vy), vz, __ldg(&rin[l])), 1e10f);
         bl[m] = l;
     }
-    recx_scan<M>(rin, xp, ys, zs, vx, vy, vz, bd, bl);
+    recx_scan<M, HALF>(rin, xp, ys, zs, vx, vy, vz, bd, bl);
 #pragma unroll
     for (int m = 0; m < M; ++m) {
         const int l = xp[m + 1] + ys[1] + zs[1];
@@ -790,6 +791,10 @@ static cudaError_t launch_pass_recx(FosCtx* c, int p, int step, int early_exit,
     float4* rout = (p & 1) ? c->recA : c->recB;
     if (M == 4)
         return cudaLaunchKernelEx(&cfg, k_jfa_pass_recx<4>, in, rin, out, rout, ilog2(R), lgS,
+                                  c->vs, c->halfL, c->ds, p, early_exit, c->p.min_jfa_passes,
+                                  c->p.th_pass_delta);
+    if (2 * step == R)  // the first pass: only 8 distinct candidates a voxel
+        return cudaLaunchKernelEx(&cfg, k_jfa_pass_recx<2, true>, in, rin, out, rout, ilog2(R), lgS,
                                   c->vs, c->halfL, c->ds, p, early_exit, c->p.min_jfa_passes,
                                   c->p.th_pass_delta);
     return cudaLaunchKernelEx(&cfg, k_jfa_pass_recx<2>, in, rin, out, rout, ilog2(R), lgS, c->vs,

@@ -297,7 +297,21 @@ __device__ __forceinline__ void jfa_pass_rec_body_any(const int32_t* __restrict_
 // the voxel itself) with power_dist_unit2m's floats (pdist_yz2m once per
 // row, pdist_x2m / pdist_x1m per voxel).  bd / bl hold each voxel's best
 // distance and voxel index, started from its own record.
-template <int M>
+//
+// HALF (the step is R / 2): on every axis the offsets -step and +step reach
+// the same voxel, and -1 comes first in the scan order, so a candidate with
+// any +1 offset repeats an earlier one: the same record, the same distance,
+// which a strict < never takes.  Only the offsets {-1, 0}^3 are scanned then
+// (7 candidates besides the voxel itself instead of 26); the result is the
+// full scan's.
+template <int M, bool HALF = false>
+__device__ __forceinline__ bool recx_serves(int p, int m, int k) {
+    const int dx = p - m;  // the candidate's x offset + 1
+    if (HALF) return dx >= 0 && dx <= 1 && k / 3 <= 1 && k % 3 <= 1 && !(dx == 1 && k == 4);
+    return dx >= 0 && dx <= 2 && !(dx == 1 && k == 4);
+}
+
+template <int M, bool HALF = false>
 __device__ __forceinline__ void recx_scan(const float4* __restrict__ rin, const int (&xp)[M + 2],
                                           const int (&ys)[3], const int (&zs)[3],
                                           const float (&vx)[M], float vy, float vz,
@@ -310,7 +324,7 @@ __device__ __forceinline__ void recx_scan(const float4* __restrict__ rin, const 
             bool used = false;
 #pragma unroll
             for (int m = 0; m < M; ++m)
-                if (p - m >= 0 && p - m <= 2 && !(p - m == 1 && k == 4)) used = true;
+                if (recx_serves<M, HALF>(p, m, k)) used = true;
             if (!used) continue;
             const int idx = xp[p] + ys[k / 3] + zs[k % 3];
             const float4 r = __ldg(&rin[idx]);
@@ -319,7 +333,7 @@ __device__ __forceinline__ void recx_scan(const float4* __restrict__ rin, const 
             int vm[3] = {0, 0, 0}, nv = 0;
 #pragma unroll
             for (int m = 0; m < M; ++m)
-                if (p - m >= 0 && p - m <= 2 && !(p - m == 1 && k == 4)) vm[nv++] = m;
+                if (recx_serves<M, HALF>(p, m, k)) vm[nv++] = m;
             const float2 qyz = pdist_yz2m(make_float2(vy, vz), r);
             float dv[3];
             if (nv >= 2) {
