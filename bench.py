@@ -481,8 +481,11 @@ def run_fos(args):
     achieved = alg_bytes / pass_s / 1e9
     # FP32 work: 27 candidates x ~20 FP32 operations per voxel and pass (the
     # nominal count of the scope table), none of them FMAs (-fmad=false), so
-    # the peak is the lane-operation rate 148 SMs x 128 lanes x 1.965 GHz
-    fp32_ops = 540.0 * V
+    # the peak is the lane-operation rate 148 SMs x 128 lanes x 1.965 GHz.
+    # The four-voxel form's first pass (step R/2) evaluates only the 8
+    # distinct candidates of a voxel, so that pass counts 8 / 27 of the work.
+    ops_per_voxel = 540.0 * ((passes - 1 + 8.0 / 27.0) / passes if multi else 1.0)
+    fp32_ops = ops_per_voxel * V
     fp32_lane_peak = 148 * 128 * 1.965e9
     fp32_frac = fp32_ops / pass_s / fp32_lane_peak
     # (c) face extraction (accumulate_face_area: k_faces_reset, k_faces,
@@ -557,7 +560,10 @@ def run_fos(args):
                               "fp32": {"achieved_T_ops_per_s": round(fp32_ops / pass_s / 1e12, 2),
                                        "peak_T_ops_per_s": round(fp32_lane_peak / 1e12, 2),
                                        "frac": round(fp32_frac, 4),
-                                       "ops_per_voxel": 540,
+                                       "ops_per_voxel": round(ops_per_voxel, 1),
+                                       "ops_note": "540 a voxel and pass (27 candidates x 20), "
+                                                   "the first pass 8 / 27 of it (its distinct "
+                                                   "candidates), averaged over the passes",
                                        "peak_note": "lane operations without FMA (148 x 128 x "
                                                     "1.965 GHz); 74.4 TFLOP/s counts an FMA "
                                                     "as two"},
