@@ -387,6 +387,19 @@ __global__ void __launch_bounds__(FACES_THREADS) k_faces(const int32_t* __restri
     faces_claims_flush(cb, claimed, ds);
 }
 
+// Face extraction over 4 x 8 x 8 voxel tiles with a per-block merge of the
+// pairs (faces_tile_body; R a multiple of 8).
+__global__ void __launch_bounds__(FACES_TILE_THREADS) k_faces_tile(
+    const int32_t* __restrict__ filt, int R, int n, unsigned long long* keys, unsigned int* hmin,
+    unsigned int* hcnt, unsigned int* claimed, FosDevState* ds, unsigned long long mask) {
+    __shared__ unsigned int s_slot[3 * FACES_TILE_THREADS];
+    __shared__ int s_n;
+    if (threadIdx.x == 0) s_n = 0;
+    const ClaimBuf cb{s_slot, &s_n, claimed};
+    faces_tile_body(filt, R, n, keys, hmin, hcnt, cb, ds, mask, blockIdx.x);
+    faces_claims_flush(cb, claimed, ds);
+}
+
 // Moves every claimed pair into its lower particle's candidate row and resets
 // the table slot for the next run.  Launched with 8 blocks of 256 per SM (the
 // full 2,048 threads at 32 registers): each pair is a chain of dependent
@@ -1019,7 +1032,15 @@ extern "C" int fos_jfa_accumulate_faces(FosCtx* c, int n, fos_stream_t s) {
     long long V = (long long)c->res * c->res * c->res;
     k_faces_reset<<<fos_blocks(n, 256), 256, 0, s>>>(c->ds, c->rowcnt, n);
     FOS_LAUNCHED(c);
-    k_faces<<<fos_blocks(V, FACES_THREADS), FACES_THREADS, 0, s>>>(c->filt, c->res, n, c->hkeys, c->hmin, c->hcnt,
+#ifndef FOS_FACES_TILE
+#define FOS_FACES_TILE 1
+#endif
+    if (FOS_FACES_TILE && c->res % 8 == 0)
+        k_faces_tile<<<(unsigned)(V / FACES_TILE_THREADS), FACES_TILE_THREADS, 0, s>>>(
+            c->filt, c->res, n, c->hkeys, c->hmin, c->hcnt, c->claimed, c->ds,
+            (unsigned long long)(c->H - 1));
+    else
+        k_faces<<<fos_blocks(V, FACES_THREADS), FACES_THREADS, 0, s>>>(c->filt, c->res, n, c->hkeys, c->hmin, c->hcnt,
                                                c->claimed, c->ds, (unsigned long long)(c->H - 1));
     FOS_LAUNCHED(c);
     k_compact<<<c->num_sms * 8, 256, 0, s>>>(c->hkeys, c->hmin, c->hcnt, c->claimed, c->ds,

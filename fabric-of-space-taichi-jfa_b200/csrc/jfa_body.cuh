@@ -554,6 +554,92 @@ __device__ __forceinline__ void faces_body(const int32_t* __restrict__ filt, int
                            mask);
 }
 
+// faces_body with a second merge per block (R a multiple of 8, 256 threads):
+// block blk takes a 4 (x) x 8 (y) x 8 (z) voxel tile made of eight 2 x 2 x 8
+// warp tiles.  Each warp merges its lanes' pairs as faces_body does; the
+// warps' merged groups then meet in a shared-memory table (count sum, minimum
+// first-touch key), and each distinct pair of the tile makes one update of
+// the global table, so a pair whose faces span several warps of the tile
+// probes the global table once instead of once per warp.  A group that finds
+// the shared table full goes to the global table directly.  Counts are sums
+// and keys minima, so the table ends as faces_body leaves it.  cb.n must be
+// zeroed before the call (the first barrier here publishes it).
+#define FACES_TILE_THREADS 256
+#define FACES_TILE_SLOTS 256  // shared-table slots (a power of two)
+__device__ __forceinline__ void faces_tile_body(const int32_t* __restrict__ filt, int R, int n,
+                                                unsigned long long* keys, unsigned int* hmin,
+                                                unsigned int* hcnt, const ClaimBuf& cb,
+                                                FosDevState* ds, unsigned long long mask,
+                                                int blk) {
+    __shared__ unsigned long long s_key[FACES_TILE_SLOTS];
+    __shared__ unsigned int s_min[FACES_TILE_SLOTS], s_cnt[FACES_TILE_SLOTS];
+    for (int t = threadIdx.x; t < FACES_TILE_SLOTS; t += blockDim.x) {
+        s_key[t] = EMPTY_KEY;
+        s_min[t] = 0xFFFFFFFFu;
+        s_cnt[t] = 0u;
+    }
+    __syncthreads();
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    const int nb = R >> 3;
+    const int bz = blk % nb, t1 = blk / nb, by = t1 % nb, bx = t1 / nb;
+    const int z = (bz << 3) + (lane & 7);
+    const int y = (by << 3) + ((w >> 1) << 1) + ((lane >> 3) & 1);
+    const int x = (bx << 2) + ((w & 1) << 1) + ((lane >> 4) & 1);
+    const int l = (x * R + y) * R + z;
+    int nlin[3], b[3];
+    nlin[0] = (wrap_small(x + 1, R) * R + y) * R + z;
+    nlin[1] = (x * R + wrap_small(y + 1, R)) * R + z;
+    nlin[2] = (x * R + y) * R + wrap_small(z + 1, R);
+    const int a = filt[l];
+#pragma unroll
+    for (int ax = 0; ax < 3; ++ax) b[ax] = filt[nlin[ax]];
+    const bool va = a >= 0 && a < n;
+#pragma unroll
+    for (int ax = 0; ax < 3; ++ax) {
+        const bool valid = va && b[ax] >= 0 && b[ax] < n && b[ax] != a;
+        unsigned long long pk = 0;
+        unsigned int fk = 0;
+        if (valid) {
+            const int lo = a < b[ax] ? a : b[ax], hi = a < b[ax] ? b[ax] : a;
+            pk = ((unsigned long long)(unsigned int)lo << 32) | (unsigned int)hi;
+            fk = (a < b[ax]) ? (unsigned int)l * 6u + (unsigned int)(ax * 2 + 1)
+                             : (unsigned int)nlin[ax] * 6u + (unsigned int)(ax * 2);
+        }
+        const unsigned int m = __ballot_sync(0xffffffffu, valid);
+        if (valid) {
+            const unsigned int grp = __match_any_sync(m, pk);
+            const unsigned int mn = __reduce_min_sync(grp, fk);
+            if (lane == __ffs(grp) - 1) {
+                const unsigned int c = __popc(grp);
+                unsigned int hs = (unsigned int)fmix64(pk) & (FACES_TILE_SLOTS - 1);
+                bool done = false;
+                for (int p = 0; p < FACES_TILE_SLOTS; ++p) {
+                    const unsigned long long prev = atomicCAS(&s_key[hs], EMPTY_KEY, pk);
+                    if (prev == EMPTY_KEY || prev == pk) {
+                        atomicMin(&s_min[hs], mn);
+                        atomicAdd(&s_cnt[hs], c);
+                        done = true;
+                        break;
+                    }
+                    hs = (hs + 1) & (FACES_TILE_SLOTS - 1);
+                }
+                if (!done) {
+                    const unsigned long long h = fmix64(pk) & mask;
+                    pair_insert_at(pk, mn, c, h, keys[h], keys, hmin, hcnt, cb, ds, mask);
+                }
+            }
+        }
+    }
+    __syncthreads();
+    for (int t = threadIdx.x; t < FACES_TILE_SLOTS; t += blockDim.x) {
+        const unsigned long long pk = s_key[t];
+        if (pk != EMPTY_KEY) {
+            const unsigned long long h = fmix64(pk) & mask;
+            pair_insert_at(pk, s_min[t], s_cnt[t], h, keys[h], keys, hmin, hcnt, cb, ds, mask);
+        }
+    }
+}
+
 // A faces kernel block's gathered claims: call with every thread of the block
 // after faces_body; cb.n was zeroed (and synchronised) before it.
 __device__ __forceinline__ void faces_claims_flush(const ClaimBuf& cb, unsigned int* claimed,
