@@ -346,6 +346,26 @@ __global__ void __launch_bounds__(512) k_ens_faces(const long long* __restrict__
     faces_claims_flush(cb, claimed, ds);
 }
 
+// The same over 4 x 8 x 8 voxel tiles with a per-block merge of the pairs
+// (faces_tile_body), every foam's R a multiple of 8: a block of 256 threads
+// takes one tile of its foam (foam offsets are multiples of 1024 voxels); a
+// block in the padding after a foam's voxels does nothing.
+__global__ void __launch_bounds__(FACES_TILE_THREADS) k_ens_faces_tile(
+    const long long* __restrict__ vo, int nf, const EnsFoamDev* __restrict__ F,
+    const int32_t* __restrict__ filt, int ntot, unsigned long long* keys, unsigned int* hmin,
+    unsigned int* hcnt, unsigned int* claimed, FosDevState* ds, unsigned long long mask) {
+    __shared__ unsigned int s_slot[3 * FACES_TILE_THREADS];
+    __shared__ int s_n;
+    const long long v0 = (long long)blockIdx.x * FACES_TILE_THREADS;
+    const EnsFoamDev d = F[ens_vox_foam(vo, nf, v0)];
+    const long long tile = (v0 - d.vox_off) / FACES_TILE_THREADS;
+    if (tile * FACES_TILE_THREADS >= (long long)d.R * d.R * d.R) return;  // block-uniform
+    if (threadIdx.x == 0) s_n = 0;
+    const ClaimBuf cb{s_slot, &s_n, claimed};
+    faces_tile_body(filt + d.vox_off, d.R, ntot, keys, hmin, hcnt, cb, ds, mask, (int)tile);
+    faces_claims_flush(cb, claimed, ds);
+}
+
 __global__ void k_ens_scores(int ntot, const EnsFoamDev* __restrict__ F,
                              const int32_t* __restrict__ foam_of,
                              const int32_t* __restrict__ face_ids,
@@ -1180,8 +1200,16 @@ static int ens_filter_faces(FosEnsemble* e, cudaStream_t s) {
     FOS_LAUNCHED(c);
     k_faces_reset<<<fos_blocks(n, 256), 256, 0, s>>>(c->ds, c->rowcnt, n);
     FOS_LAUNCHED(c);
-    k_ens_faces<<<vgrid, vb, 0, s>>>(e->dvo, e->nf, e->df, e->filt, n, c->hkeys, c->hmin, c->hcnt,
-                                     c->claimed, c->ds, (unsigned long long)(c->H - 1));
+    bool tiles = true;  // every foam's R a multiple of 8
+    for (const EnsFoamDev& d : e->hf) tiles = tiles && d.R % 8 == 0;
+    if (tiles && e->vtot % FACES_TILE_THREADS == 0)
+        k_ens_faces_tile<<<(unsigned)(e->vtot / FACES_TILE_THREADS), FACES_TILE_THREADS, 0, s>>>(
+            e->dvo, e->nf, e->df, e->filt, n, c->hkeys, c->hmin, c->hcnt, c->claimed, c->ds,
+            (unsigned long long)(c->H - 1));
+    else
+        k_ens_faces<<<vgrid, vb, 0, s>>>(e->dvo, e->nf, e->df, e->filt, n, c->hkeys, c->hmin,
+                                         c->hcnt, c->claimed, c->ds,
+                                         (unsigned long long)(c->H - 1));
     FOS_LAUNCHED(c);
     k_compact<<<c->num_sms * 8, 256, 0, s>>>(c->hkeys, c->hmin, c->hcnt, c->claimed, c->ds,
                                              c->rowcnt, c->rowbuf);
