@@ -346,9 +346,9 @@ __global__ void __launch_bounds__(512) k_ens_faces(const long long* __restrict__
     faces_claims_flush(cb, claimed, ds);
 }
 
-// The same over 4 x 8 x 8 voxel tiles with a per-block merge of the pairs
-// (faces_tile_body), every foam's R a multiple of 8: a block of 256 threads
-// takes one tile of its foam (foam offsets are multiples of 1024 voxels); a
+// The same over voxel tiles of FACES_TILE_THREADS voxels with a per-block merge of the pairs
+// (faces_tile_body), every foam's R a multiple of 8: a block of
+// FACES_TILE_THREADS threads takes one tile of its foam (foam offsets are multiples of 1024 voxels); a
 // block in the padding after a foam's voxels does nothing.
 __global__ void __launch_bounds__(FACES_TILE_THREADS) k_ens_faces_tile(
     const long long* __restrict__ vo, int nf, const EnsFoamDev* __restrict__ F,

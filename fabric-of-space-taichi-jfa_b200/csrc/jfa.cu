@@ -387,7 +387,7 @@ __global__ void __launch_bounds__(FACES_THREADS) k_faces(const int32_t* __restri
     faces_claims_flush(cb, claimed, ds);
 }
 
-// Face extraction over 4 x 8 x 8 voxel tiles with a per-block merge of the
+// Face extraction over voxel tiles of FACES_TILE_THREADS voxels with a per-block merge of the
 // pairs (faces_tile_body; R a multiple of 8).
 __global__ void __launch_bounds__(FACES_TILE_THREADS) k_faces_tile(
     const int32_t* __restrict__ filt, int R, int n, unsigned long long* keys, unsigned int* hmin,

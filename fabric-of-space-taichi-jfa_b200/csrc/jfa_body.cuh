@@ -554,9 +554,10 @@ __device__ __forceinline__ void faces_body(const int32_t* __restrict__ filt, int
                            mask);
 }
 
-// faces_body with a second merge per block (R a multiple of 8, 256 threads):
-// block blk takes a 4 (x) x 8 (y) x 8 (z) voxel tile made of eight 2 x 2 x 8
-// warp tiles.  Each warp merges its lanes' pairs as faces_body does; the
+// faces_body with a second merge per block (R a multiple of 8): block blk takes
+// a (2 FACES_TILE_WX) x (2 FACES_TILE_WY) x 8 voxel tile made of
+// FACES_TILE_WX x FACES_TILE_WY warp tiles of 2 x 2 x 8 (default 4 x 8 x 8,
+// eight warps).  Each warp merges its lanes' pairs as faces_body does; the
 // warps' merged groups then meet in a shared-memory table (count sum, minimum
 // first-touch key), and each distinct pair of the tile makes one update of
 // the global table, so a pair whose faces span several warps of the tile
@@ -564,8 +565,17 @@ __device__ __forceinline__ void faces_body(const int32_t* __restrict__ filt, int
 // the shared table full goes to the global table directly.  Counts are sums
 // and keys minima, so the table ends as faces_body leaves it.  cb.n must be
 // zeroed before the call (the first barrier here publishes it).
-#define FACES_TILE_THREADS 256
-#define FACES_TILE_SLOTS 256  // shared-table slots (a power of two)
+#ifndef FACES_TILE_WX
+#define FACES_TILE_WX 2  // warp tiles along x (2 voxels each)
+#endif
+#ifndef FACES_TILE_WY
+#define FACES_TILE_WY 4  // warp tiles along y (2 voxels each)
+#endif
+// R a multiple of 8 then tiles the grid: 2 WX and 2 WY divide 8
+static_assert(8 % (2 * FACES_TILE_WX) == 0 && 8 % (2 * FACES_TILE_WY) == 0,
+              "face tile sides must divide 8");
+#define FACES_TILE_THREADS (32 * FACES_TILE_WX * FACES_TILE_WY)
+#define FACES_TILE_SLOTS FACES_TILE_THREADS  // shared-table slots (a power of two)
 __device__ __forceinline__ void faces_tile_body(const int32_t* __restrict__ filt, int R, int n,
                                                 unsigned long long* keys, unsigned int* hmin,
                                                 unsigned int* hcnt, const ClaimBuf& cb,
@@ -580,11 +590,11 @@ __device__ __forceinline__ void faces_tile_body(const int32_t* __restrict__ filt
     }
     __syncthreads();
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
-    const int nb = R >> 3;
-    const int bz = blk % nb, t1 = blk / nb, by = t1 % nb, bx = t1 / nb;
+    const int nbz = R >> 3, nby = R / (2 * FACES_TILE_WY);
+    const int bz = blk % nbz, t1 = blk / nbz, by = t1 % nby, bx = t1 / nby;
     const int z = (bz << 3) + (lane & 7);
-    const int y = (by << 3) + ((w >> 1) << 1) + ((lane >> 3) & 1);
-    const int x = (bx << 2) + ((w & 1) << 1) + ((lane >> 4) & 1);
+    const int y = by * (2 * FACES_TILE_WY) + (w / FACES_TILE_WX) * 2 + ((lane >> 3) & 1);
+    const int x = bx * (2 * FACES_TILE_WX) + (w % FACES_TILE_WX) * 2 + ((lane >> 4) & 1);
     const int l = (x * R + y) * R + z;
     int nlin[3], b[3];
     nlin[0] = (wrap_small(x + 1, R) * R + y) * R + z;
