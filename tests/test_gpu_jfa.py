@@ -87,8 +87,10 @@ def test_hysteresis_history_over_several_runs():
         rad = (rad * rng.uniform(0.95, 1.05, rad.shape)).astype(np.float32)
 
 
-@pytest.mark.parametrize("R,L", [(48, 1.0), (40, 0.189)])
+@pytest.mark.parametrize("R,L", [(48, 1.0), (40, 0.189), (36, 1.0)])
 def test_non_power_of_two_and_reference_box(R, L):
+    """Non-power-of-two grids against the oracle; R = 36 (not a multiple of 8)
+    also takes the untiled face kernel."""
     rng = np.random.default_rng(11)
     n = 300
     pos = wrapped(rng.uniform(0, L, (n, 3)).astype(np.float32), L)
@@ -106,6 +108,33 @@ def test_non_power_of_two_and_reference_box(R, L):
     nl, used, fsc = O.finalize(rad, ids, cnt, prev, p)
     assert np.array_equal(ctx.fsc[:n].cpu().numpy(), fsc)
     assert np.array_equal(ctx.neighbor_list[:n].cpu().numpy(), nl)
+
+
+def test_face_tiles_with_crowded_pairs():
+    """3,000 seeds on a 16^3 grid: cells are about one voxel, so a 4 x 8 x 8
+    face tile meets more distinct pairs than its 256-slot shared table holds
+    and the overflow goes to the global table directly.  face_ids,
+    face_counts, fsc and the neighbour lists still equal the oracle's."""
+    rng = np.random.default_rng(5)
+    n, R, L = 3000, 16, 1.0
+    pos = wrapped(rng.uniform(0, L, (n, 3)).astype(np.float32), L)
+    rad = rng.uniform(0.002, 0.004, n).astype(np.float32)
+    p = O.OracleParams(n=n, R=R, L=L, r_max_cell=0.004)
+    lab, _, _ = O.jfa_labels(pos, rad, p)
+    cfg = FosConfig(DOMAIN_SIZE=L, CELL_SIZE=0.08, JFA_RES=R, JFA_RES_MIN=2, JFA_RES_MAX=R,
+                    JFA_EARLY_EXIT_ENABLED=False, MAX_PARTICLES=n)
+    ctx = Context(cfg, max_n=n, max_res=R)
+    ctx.jfa_run(_dev(pos), _dev(rad), n)
+    torch.cuda.synchronize()
+    assert np.array_equal(ctx.labels().cpu().numpy().reshape(-1), lab)
+    ids, cnt = O.accumulate_faces(O.majority_filter(lab, R), R, n)
+    assert np.array_equal(ctx.face_ids[:n].cpu().numpy(), ids)
+    assert np.array_equal(ctx.face_counts[:n].cpu().numpy(), cnt)
+    prev = np.zeros((n, 32), np.float32)
+    nl, used, fsc = O.finalize(rad, ids, cnt, prev, p)
+    assert np.array_equal(ctx.fsc[:n].cpu().numpy(), fsc)
+    assert np.array_equal(ctx.neighbor_list[:n].cpu().numpy(), nl)
+    assert ctx.device_error() == 0
 
 
 def test_early_exit_and_tie_rule_flags():
