@@ -154,6 +154,59 @@ __global__ void __launch_bounds__(256, 4)
     }
 }
 
+// The same for any R (unit L, R / s >= M and R a multiple of M s): coordinates
+// by division, wraps by compare-and-add, a tail of threads past R^3 / M.
+template <int M, bool HALF = false>
+__global__ void __launch_bounds__(256, 4)
+    k_jfa_pass_recx_any(const int32_t* __restrict__ in, const float4* __restrict__ rin,
+                        int32_t* __restrict__ out, float4* __restrict__ rout, int R, int step,
+                        float vs, float halfL, FosDevState* ds, int pass, int early_exit,
+                        int min_passes, double th) {
+    asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
+    asm volatile("griddepcontrol.wait;" ::: "memory");
+    const long long V = (long long)R * R * R;
+    if (early_exit && jfa_exited_before(ds, pass, (double)V, min_passes, th)) return;
+    const long long tl = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    const bool live = tl < V / M;
+    const int tt = live ? (int)tl : 0;
+    const int z = tt % R, yz = tt / R, y = yz % R, xi = yz / R;
+    const int g = xi / step;
+    const int xb = g * M * step + (xi - g * step);
+    int ys[3], zs[3], xp[M + 2];
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+        const int o = (k - 1) * step;
+        ys[k] = wrap_small(y + o, R) * R;
+        zs[k] = wrap_small(z + o, R);
+    }
+#pragma unroll
+    for (int p = 0; p < M + 2; ++p) xp[p] = wrap_small(xb + (p - 1) * step, R) * R * R;
+    const float vy = voxel_centre(y, vs, halfL), vz = voxel_centre(z, vs, halfL);
+    float vx[M], bd[M];
+    int bl[M], own[M];
+#pragma unroll
+    for (int m = 0; m < M; ++m) {
+        const int l = xp[m + 1] + ys[1] + zs[1];
+        vx[m] = voxel_centre(xb + m * step, vs, halfL);
+        own[m] = in[l];
+        bd[m] = fminf(power_dist_unit2m(make_float2(vx[m], vy), vz, __ldg(&rin[l])), 1e10f);
+        bl[m] = l;
+    }
+    recx_scan<M, HALF>(rin, xp, ys, zs, vx, vy, vz, bd, bl);
+#pragma unroll
+    for (int m = 0; m < M; ++m) {
+        const int l = xp[m + 1] + ys[1] + zs[1];
+        int best = own[m];
+        if (bl[m] != l) best = in[bl[m]];
+        if (live) {
+            out[l] = best;
+            rout[l] = __ldg(&rin[bl[m]]);
+        }
+        const int cnt = __syncthreads_count(live && best != own[m]);
+        if (threadIdx.x == 0 && cnt) atomicAdd(&ds->changes[pass], (unsigned long long)cnt);
+    }
+}
+
 // ------------------------------------------------ pass with staged record rows
 // The same pass with the records a block needs staged in shared memory by
 // the tensor memory accelerator (cp.async.bulk.tensor, no multicast), for
@@ -815,6 +868,44 @@ static cudaError_t launch_pass_recx(FosCtx* c, int p, int step, int early_exit,
                               c->p.th_pass_delta);
 }
 
+// Voxels a thread of the multi-voxel pass at any R and step s: 4 where R is a
+// multiple of 4 s, 2 where it is a multiple of 2 s (the first pass, s = R/2,
+// then scans its 8 distinct candidates), else 0 (the one-voxel pass runs).
+static int recx_any_m(int R, int step) {
+    return R % (4 * step) == 0 ? 4 : (R % (2 * step) == 0 ? 2 : 0);
+}
+
+static cudaError_t launch_pass_recx_any(FosCtx* c, int p, int step, int early_exit,
+                                        cudaStream_t s) {
+    const int R = c->res;
+    const int M = recx_any_m(R, step);
+    const long long V = (long long)R * R * R;
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3((unsigned)fos_blocks(V / M, 256));
+    cfg.blockDim = dim3(256);
+    cfg.stream = s;
+    cudaLaunchAttribute at[1];
+    at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    at[0].val.programmaticStreamSerializationAllowed = 1;
+    cfg.attrs = at;
+    cfg.numAttrs = p > 0 ? 1 : 0;
+    const int32_t* in = (p & 1) ? c->labB : c->labA;
+    int32_t* out = (p & 1) ? c->labA : c->labB;
+    const float4* rin = (p & 1) ? c->recB : c->recA;
+    float4* rout = (p & 1) ? c->recA : c->recB;
+    if (M == 4)
+        return cudaLaunchKernelEx(&cfg, k_jfa_pass_recx_any<4>, in, rin, out, rout, R, step, c->vs,
+                                  c->halfL, c->ds, p, early_exit, c->p.min_jfa_passes,
+                                  c->p.th_pass_delta);
+    if (2 * step == R)
+        return cudaLaunchKernelEx(&cfg, k_jfa_pass_recx_any<2, true>, in, rin, out, rout, R, step,
+                                  c->vs, c->halfL, c->ds, p, early_exit, c->p.min_jfa_passes,
+                                  c->p.th_pass_delta);
+    return cudaLaunchKernelEx(&cfg, k_jfa_pass_recx_any<2>, in, rin, out, rout, R, step, c->vs,
+                              c->halfL, c->ds, p, early_exit, c->p.min_jfa_passes,
+                              c->p.th_pass_delta);
+}
+
 // cuTensorMapEncodeTiled through the runtime's driver entry point (no link
 // against libcuda).
 typedef CUresult (*EncodeTiledFn)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*,
@@ -917,13 +1008,17 @@ static int run_passes(FosCtx* c, int first_step, int npass, int early_exit, cuda
         const bool tma = tma_applies(c) && tma_maps(c);
         // several voxels a thread where the grid still fills the GPU (at 64^3,
         // 65k threads: 0.084 against 0.077 ms for 7 passes), or when forced
-        const bool recx = ul && p2 && R >= 16 &&
-                          (c->use_recx == 2 ||
-                           (c->use_recx == 1 && V / 4 >= (long long)c->num_sms * 1024));
+        const bool multi = ul && R >= 16 &&
+                           (c->use_recx == 2 ||
+                            (c->use_recx == 1 && V / 4 >= (long long)c->num_sms * 1024));
+        const bool recx = multi && p2;
+        const bool recx_any = multi && !p2;
         for (int p = 0; p < npass; ++p) {
             if (step < 1) step = 1;
             cudaError_t le;
-            if (tma) le = launch_pass_tma(c, p, step, early_exit, s);
+            if (recx_any && recx_any_m(R, step) > 0)
+                le = launch_pass_recx_any(c, p, step, early_exit, s);
+            else if (tma) le = launch_pass_tma(c, p, step, early_exit, s);
             else if (recx) le = launch_pass_recx(c, p, step, early_exit, s);
             else if (ul && p2) le = launch_pass_rec<true, true>(c, p, step, early_exit, s);
             else if (ul) le = launch_pass_rec<true, false>(c, p, step, early_exit, s);

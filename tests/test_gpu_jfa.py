@@ -268,13 +268,15 @@ def test_unwrapped_seed_positions(shift):
     assert np.array_equal(ctx.labels().cpu().numpy().reshape(-1), lab)
 
 
-@pytest.mark.parametrize("R", [16, 32, 64, 128, 256])
+@pytest.mark.parametrize("R", [16, 32, 36, 48, 64, 96, 128, 256])
 def test_pass_forms_agree(R):
     """The record pass with four voxels a thread along x (forced at every R),
     the one-voxel-a-thread pass and (R >= 32) the pass with TMA-staged rows
     give the same labels and per-pass change counts, with and without early
-    exit; at R = 16 and 32 the four-voxel pass is also checked against the
-    oracle."""
+    exit; at R <= 48 the four-voxel pass is also checked against the oracle.
+    R = 36, 48 and 96 take the multi-voxel pass for any R (two voxels a thread
+    at the first step, four where R is a multiple of 4 steps, one voxel a
+    thread at R = 36's step 4)."""
     rng = np.random.default_rng(R + 1)
     n = 40 + R * 4
     pos = wrapped(rng.random((n, 3), dtype=np.float32))
@@ -297,7 +299,7 @@ def test_pass_forms_agree(R):
             ctx.close()
         for o in out[1:]:
             assert np.array_equal(out[0][0], o[0]) and out[0][1] == o[1] and out[0][2] == o[2]
-        if R <= 32:
+        if R <= 48:
             p = O.OracleParams(n=n, R=R, early_exit=early, r_max_cell=0.05)
             lab, ch, done = O.jfa_labels(pos, rad, p)
             assert np.array_equal(out[0][0], lab) and done == out[0][2]
