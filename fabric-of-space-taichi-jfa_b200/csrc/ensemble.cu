@@ -47,6 +47,8 @@ struct EnsWords {  // per-foam device words
     int zero_fsc;
     unsigned int omax_bits;
     unsigned int rmax_bits;      // the foam's largest radius after the pressure sweeps
+    unsigned int rmax0_bits;     // the foam's largest radius at the frame's first rebuild
+    int pad;
     unsigned long long rad_sum;  // OU jitter: the foam's radii, 2^-40 fixed point (exact)
     unsigned long long changes[FOS_MAX_PASSES];
 };
@@ -509,8 +511,97 @@ __device__ __forceinline__ void ens_pbd(const EnsArgs& a, const EnsGeo& geo, con
     if (p1) d1.flush(a, geo, a.pos, coop_p1_par(a, par), ou);
 }
 
+// A frame's rebuilds on arrival-order rows, as the single-foam frame kernel
+// runs them: rebuild r (0 before max overlap, 1..pbd_iters before each PBD
+// sweep, pbd_iters + 1 the final CSR one) drops its particles into count
+// buffer r % 3 (a.cnt holds three of a.G3 cells), row set r & 1 and overflow
+// bit r % 3 of ds->grid_ovf; its P1 runs in the phase that produced the
+// positions.  No phase sorts the rows: max overlap does not depend on the
+// order, and the PBD sweeps add their hits in (stencil cell, particle index)
+// order themselves (pbd_warp_rows).
+__device__ __forceinline__ P1Dst ens_p1_dst(const EnsArgs& a, int r) {
+    return P1Dst{a.cnt + (size_t)(r % 3) * a.G3, a.cfix ? ((r & 1) ? a.idsort : a.cfix) : nullptr,
+                 (r & 1) ? a.spfix : a.spst, a.slot_of, (unsigned int*)&a.ds->grid_ovf,
+                 1u << (r % 3)};
+}
+
+// Layout of rebuild r for the phase that reads it (its P1 is behind a grid
+// barrier): the rows when none overflowed, else the CSR form, whose phases
+// run first.  Also clears count buffer and overflow bit (r + 2) % 3 for
+// rebuild r + 2, whose P1 comes one phase later (their last reader, of
+// rebuild r - 1, is done).
+__device__ __forceinline__ bool ens_layout(const EnsArgs& a, const EnsGeo& geo, int r, int& tk,
+                                           unsigned int& ep, CoopLayout& lay, bool& rows) {
+    const int T = gridDim.x * blockDim.x;
+    const int tid = blockIdx.x * blockDim.x + threadIdx.x;
+    int32_t* zc = a.cnt + (size_t)((r + 2) % 3) * a.G3;
+    for (int c = tid; c < a.G3; c += T) zc[c] = 0;
+    const bool ovf = ((*((volatile int*)&a.ds->grid_ovf)) >> (r % 3)) & 1;
+    if (tid == 0) atomicAnd(&a.ds->grid_ovf, ~(1 << ((r + 2) % 3)));
+    const int32_t* cnt = a.cnt + (size_t)(r % 3) * a.G3;
+    rows = a.cfix != nullptr && !ovf;
+    if (rows) {
+        lay = CoopLayout{(r & 1) ? a.idsort : a.cfix, (r & 1) ? a.spfix : a.spst, nullptr, cnt,
+                         COOP_CAP};
+        return true;
+    }
+    lay = CoopLayout{a.ci, a.sp, a.cs, a.cc, 0};
+    return coop_csr(a, geo, cnt, a.pos, a.rad, false, tk, ep);
+}
+
+// One PBD sweep over every particle of every foam on layout `lay` (rows or
+// CSR), into pos_tmp; each new position also enters rebuild `next` (P1).
+__device__ __forceinline__ void ens_pbd_frame(const EnsArgs& a, const EnsGeo& geo,
+                                              const CoopLayout& lay, bool rows, int wid, int W_,
+                                              int lane, const P1Dst& next,
+                                              const OuStep* ou = nullptr) {
+    const int rounds = (a.n + W_ - 1) / W_;
+    P1Defer d1;
+    int kk_next = wid < a.n ? __ldcg(&a.slot_of[wid]) : 0;
+    for (int r = 0; r < rounds; ++r) {
+        const int i = r * W_ + wid;
+        const int kk = kk_next;
+        kk_next = i + W_ < a.n ? __ldcg(&a.slot_of[i + W_]) : 0;
+        if (i < a.n) {  // warp-uniform
+            const int f = a.foam_of[i];
+            const EnsFoamDev& d = a.F[f];
+            const GridGeom g{d.G, a.L, a.invL, a.halfL};
+            // the stencil skips the cells beyond reach of the foam's largest
+            // radius (set in the Brownian phase; radii are fixed during PBD)
+            const float rmax = d.G >= 5 ? __uint_as_float(__ldcg(&a.W[f].rmax_bits)) : 0.f;
+            const float cw = a.L / (float)d.G;
+            float4 nv = make_float4(0.f, 0.f, 0.f, 0.f);
+            const int pi =
+                rows ? pbd_warp_rows<LdL2>(kk, lane, lay.sp, lay.ci, a.pos_tmp, g,
+                                           lay.cc + d.cell_off, COOP_CAP, a.gap1, a.mdf, a.dmul,
+                                           &nv, rmax, cw, d.cell_off)
+                     : pbd_warp<LdL2>(kk, lane, lay.sp, lay.ci, a.pos_tmp, g, lay.cs + d.cell_off,
+                                      lay.cc + d.cell_off, a.gap1, a.mdf, a.dmul, &nv, 0,
+                                      d.cell_off, rmax, cw);
+            d1.put(a, geo, lane, pi, nv, a.pos, next, ou);
+        }
+    }
+    d1.flush(a, geo, a.pos, next, ou);
+}
+
+// The largest radius of each foam into *bits (w: the foam's word): one
+// atomic per warp when the warp's particles share a foam (foams are
+// contiguous index ranges), else one per particle.  Positive floats order as
+// their bits.  Called by every active lane of the warp.
+__device__ __forceinline__ void ens_foam_max(unsigned int* bits, int f, float r_i, int lane) {
+    const unsigned int am = __activemask();
+    const unsigned int rb = __float_as_uint(r_i);
+    const int f0 = __shfl_sync(am, f, __ffs(am) - 1);
+    if (__all_sync(am, f == f0)) {
+        const unsigned int wm = __reduce_max_sync(am, rb);
+        if (lane == __ffs(am) - 1 && wm > __ldcg(bits)) atomicMax(bits, wm);
+    } else {
+        atomicMax(bits, rb);
+    }
+}
+
 template <int THREADS>
-__global__ void __launch_bounds__(THREADS) k_ens_coop(EnsArgs a) {
+__global__ void __launch_bounds__(THREADS, 1024 / THREADS) k_ens_coop(EnsArgs a) {
     const int T = gridDim.x * blockDim.x;
     const int tid = blockIdx.x * blockDim.x + threadIdx.x;
     const int lane = threadIdx.x & 31;
@@ -519,6 +610,8 @@ __global__ void __launch_bounds__(THREADS) k_ens_coop(EnsArgs a) {
     const EnsGeo geo{a.F, a.foam_of, a.L, a.invL, a.halfL};
     int tk = 0;
     unsigned int ep = 0;
+    if (a.trace && threadIdx.x == 0) atomicMax(&a.trace[a.trace_cap - 2], ~global_ns());
+    trace_mark(a, tk);
     CoopLayout lay;
     int gk = 0;  // rebuild gk uses count buffer gk & 1
     if (a.mode == 1) {
@@ -534,10 +627,25 @@ __global__ void __launch_bounds__(THREADS) k_ens_coop(EnsArgs a) {
         }
         return;
     }
-    // (1) rebuild_grid
-    if (!coop_grid(a, geo, a.pos, a.pos, a.rad, false, tk, ep, false, gk & 1, false, &lay)) return;
-    ++gk;
-    // (2) compute_max_overlap: per-foam maxima
+    // (1) rebuild_grid: rebuild 0's P1, with each foam's largest radius for
+    // the max-overlap stencils
+    {
+        const P1Dst t = ens_p1_dst(a, 0);
+        for (int i = spread_tid(); i < a.n; i += T) {
+            const float r_i = __ldcg(&a.rad[i]);
+            ens_foam_max(&a.W[a.foam_of[i]].rmax0_bits, a.foam_of[i], r_i, lane);
+            coop_p1_val(a, geo, i,
+                        make_float3(__ldcg(&a.pos[3 * i + 0]), __ldcg(&a.pos[3 * i + 1]),
+                                    __ldcg(&a.pos[3 * i + 2])),
+                        r_i, a.pos, t);
+        }
+    }
+    if (!grid_barrier(a.ds, ep)) return;
+    trace_mark(a, tk);
+    // (2) compute_max_overlap: per-foam maxima; the stencils visit only the
+    // cells that can hold a positive depth
+    bool rows = false;
+    if (!ens_layout(a, geo, 0, tk, ep, lay, rows)) return;
     {
         const int rounds = (a.n + W_ - 1) / W_;
         int kk_next = wid < a.n ? __ldcg(&a.slot_of[wid]) : 0;
@@ -549,15 +657,18 @@ __global__ void __launch_bounds__(THREADS) k_ens_coop(EnsArgs a) {
                 const int f = a.foam_of[i];
                 const EnsFoamDev& d = a.F[f];
                 const GridGeom g{d.G, a.L, a.invL, a.halfL};
+                const float rmax0 =
+                    d.G >= 5 ? __uint_as_float(__ldcg(&a.W[f].rmax0_bits)) : 0.f;
                 unsigned int b = maxov_warp<LdL2>(kk, lane, lay.sp, lay.ci, g,
                                                   lay.cs ? lay.cs + d.cell_off : nullptr,
                                                   lay.cc + d.cell_off, a.eps, a.lmd, lay.cap,
-                                                  d.cell_off);
+                                                  d.cell_off, rmax0, a.L / (float)d.G);
                 if (lane == 0 && b > __ldcg(&a.W[f].omax_bits)) atomicMax(&a.W[f].omax_bits, b);
             }
         }
     }
     if (!grid_barrier(a.ds, ep)) return;
+    trace_mark(a, tk);
     // (3) settle nudge of the foams whose settle counter is > 0; each final
     // radius's power r^P seeds the pressure sweeps, and each particle's
     // neighbours of the sweeps go to the table (its foam's hash offset)
@@ -582,6 +693,7 @@ __global__ void __launch_bounds__(THREADS) k_ens_coop(EnsArgs a) {
         if (a.sweeps > 0) a.vol0[i] = pow_P(r, a.pa.P);
     }
     if (!grid_barrier(a.ds, ep)) return;
+    trace_mark(a, tk);
     // (4) pressure sweeps with each foam's bounds, on the neighbour table; two
     // rounds at a time, both groups' loads before either sum
     {
@@ -613,6 +725,7 @@ __global__ void __launch_bounds__(THREADS) k_ens_coop(EnsArgs a) {
                                      a.delta_r);
             }
             if (!grid_barrier(a.ds, ep)) return;
+            trace_mark(a, tk);
         }
     }
     // (5) Brownian jitter with each foam's key and local counter; settle -= 1.
@@ -624,28 +737,15 @@ __global__ void __launch_bounds__(THREADS) k_ens_coop(EnsArgs a) {
         const EnsFoamDev& d = a.F[f];
         const float r_i = __ldcg(&a.rad[i]);
         if (a.ou) atomicAdd(&a.W[f].rad_sum, (unsigned long long)rad_fixed(r_i));
-        // the foam's largest radius (positive floats order as their bits):
-        // one atomic per warp when its particles share a foam (foams are
-        // contiguous index ranges), else one per particle
-        {
-            const unsigned int am = __activemask();
-            const unsigned int rb = __float_as_uint(r_i);
-            const int f0 = __shfl_sync(am, f, __ffs(am) - 1);
-            if (__all_sync(am, f == f0)) {
-                const unsigned int wm = __reduce_max_sync(am, rb);
-                if (lane == __ffs(am) - 1 && wm > __ldcg(&a.W[f].rmax_bits))
-                    atomicMax(&a.W[f].rmax_bits, wm);
-            } else {
-                atomicMax(&a.W[f].rmax_bits, rb);
-            }
-        }
+        ens_foam_max(&a.W[f].rmax_bits, f, r_i, lane);  // for the PBD stencils
         brownian_one<LdL2>(i, (unsigned int)(i - d.part_off), a.pos, a.strength, a.domain, a.halfL,
                            d.k0, d.k1, (unsigned int)frame);
-        coop_p1_one(a, geo, i, a.pos, a.rad, a.pos, coop_p1_par(a, gk & 1));
+        coop_p1_one(a, geo, i, a.pos, a.rad, a.pos, ens_p1_dst(a, 1));
     }
     for (int f = tid; f < a.nf; f += T)
         if (a.W[f].settle > 0) a.W[f].settle -= 1;
     if (!grid_barrier(a.ds, ep)) return;
+    trace_mark(a, tk);
     // (6) PBD sweeps, each on a fresh grid; (7) final rebuild.  The OU jitter
     // (run.py:855-867) runs inside the last sweep's P1 with each foam's kick
     // (from its mean radius, written here, read after the layout phase's
@@ -657,16 +757,18 @@ __global__ void __launch_bounds__(THREADS) k_ens_coop(EnsArgs a) {
                                                 a.F[f].n));
     OuStep ous{a.vjit, a.rad, a.ou_p, 0.f, (unsigned int)frame, 0,
                a.foam_of, a.ou_kick, a.ou_key, a.ou_base};
-    const float* src = a.pos;
     for (int k = 0; k < a.pbd_iters; ++k) {
-        if (!coop_grid(a, geo, src, a.pos, a.rad, false, tk, ep, true, gk & 1, false, &lay)) return;
-        ++gk;
-        ens_pbd(a, geo, lay, wid, W_, lane, true, gk & 1,
-                a.ou && k == a.pbd_iters - 1 ? &ous : nullptr);
+        if (!ens_layout(a, geo, k + 1, tk, ep, lay, rows)) return;
+        ens_pbd_frame(a, geo, lay, rows, wid, W_, lane, ens_p1_dst(a, k + 2),
+                      a.ou && k == a.pbd_iters - 1 ? &ous : nullptr);
         if (!grid_barrier(a.ds, ep)) return;
-        src = a.pos_tmp;
+        trace_mark(a, tk);
     }
-    coop_grid(a, geo, src, a.pos, nullptr, true, tk, ep, true, gk & 1, true, nullptr);
+    coop_csr(a, geo, a.cnt + (size_t)((a.pbd_iters + 1) % 3) * a.G3, a.pos, nullptr, true, tk, ep);
+    if (a.trace) {
+        __syncthreads();
+        if (threadIdx.x == 0) atomicMax(&a.trace[a.trace_cap - 1], global_ns());
+    }
 }
 
 __global__ void k_ens_coop_prep(FosDevState* ds, EnsWords* W, int nf) {
@@ -674,6 +776,7 @@ __global__ void k_ens_coop_prep(FosDevState* ds, EnsWords* W, int nf) {
     if (f < nf) {
         W[f].omax_bits = 0u;
         W[f].rmax_bits = 0u;
+        W[f].rmax0_bits = 0u;
         W[f].rad_sum = 0ull;
     }
     if (f == 0) {
@@ -974,7 +1077,8 @@ static int ens_coop_blocks(FosEnsemble* e, int threads, int per_sm_want) {
     return blocks > 1024 ? 1024 : blocks;
 }
 
-static int ens_coop_launch(FosEnsemble* e, int mode, cudaStream_t s) {
+static int ens_coop_launch(FosEnsemble* e, int mode, cudaStream_t s,
+                           unsigned long long* trace = nullptr, int trace_cap = 0) {
     FosCtx* c = e->c;
     int threads = e->tune.coop_threads;
     int blocks = ens_coop_blocks(e, threads, e->tune.coop_blocks_per_sm);
@@ -1049,9 +1153,13 @@ static int ens_coop_launch(FosEnsemble* e, int mode, cudaStream_t s) {
     a.ou_base = e->ou_base;
     a.ou_p = ou_params(fp->jitter_rms, fp->jitter_tau, fp->max_drift_fraction, c->p.gap_fraction,
                        (float)fp->dt, c->L, c->invL, 0);
+    a.trace = trace;
+    a.trace_cap = trace_cap;
     k_ens_coop_prep<<<fos_blocks(e->nf > 0 ? e->nf : 1, 256), 256, 0, s>>>(c->ds, e->dw, e->nf);
     FOS_LAUNCHED(c);
-    FOS_CUDA(cudaMemsetAsync(c->coop_cnt, 0, (size_t)e->g3tot * sizeof(int32_t), s));
+    // count buffers 0 and 1 of the frame's rebuilds (the kernel clears buffer 2
+    // itself; the warm-up form uses buffer 0 and coop_cnt2)
+    FOS_CUDA(cudaMemsetAsync(c->coop_cnt, 0, 2 * (size_t)e->g3tot * sizeof(int32_t), s));
     cudaLaunchConfig_t cfg = {};
     cfg.gridDim = dim3(blocks);
     cfg.blockDim = dim3(threads);
@@ -1278,6 +1386,29 @@ static int ens_jfa(FosEnsemble* e, cudaStream_t s) {
     rc = ens_filter_faces(e, s);
     if (rc) return rc;
     return ens_finalize_targets(e, s);
+}
+
+extern "C" int fos_ensemble_trace(FosEnsemble* e, long long* ns_host, int cap, int* count,
+                                  fos_stream_t s_) {
+    FOS_REQUIRE(e && ns_host && count && cap >= 3, FOS_E_ARG, "NULL argument or cap < 3");
+    cudaStream_t s = (cudaStream_t)s_;
+    int rc = ens_kernel_attributes();
+    if (rc) return rc;
+    unsigned long long* d = nullptr;
+    FOS_CUDA(cudaMalloc(&d, (size_t)cap * 8));
+    cudaError_t e0 = cudaMemsetAsync(d, 0, (size_t)cap * 8, s);
+    rc = e0 == cudaSuccess ? ens_coop_launch(e, 0, s, d, cap)
+                           : fos_cuda_fail(e0, "cudaMemsetAsync", __FILE__, __LINE__);
+    if (rc == FOS_OK) {
+        cudaError_t e1 = cudaMemcpyAsync(ns_host, d, (size_t)cap * 8, cudaMemcpyDeviceToHost, s);
+        if (e1 == cudaSuccess) e1 = cudaStreamSynchronize(s);
+        if (e1 != cudaSuccess) rc = fos_cuda_fail(e1, "trace readback", __FILE__, __LINE__);
+    }
+    cudaFree(d);
+    int k = 0;
+    while (rc == FOS_OK && k < cap - 2 && ns_host[k] != 0) ++k;
+    *count = k;
+    return rc;
 }
 
 extern "C" int fos_ensemble_frame(FosEnsemble* e, int jfa_frame, fos_stream_t s_) {

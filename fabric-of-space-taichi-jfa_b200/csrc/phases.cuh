@@ -341,20 +341,23 @@ __device__ __forceinline__ int pbd_warp(int kk, int lane, const float4* sp, cons
 // rmax > 0 (the largest radius of any particle; G >= 5): the stencil keeps only
 // the cells that can hold a particle within (ri + rmax) * gap1 of p
 // (stencil_ranges_near), which is every cell that can hold an overlap.
+// cell_base as in stencil_ranges (cc then indexed from the grid's first cell).
 template <class LD>
 __device__ __forceinline__ int pbd_warp_rows(int kk, int lane, const float4* sp, const int32_t* ci,
                                              float* pout, const GridGeom g, const int32_t* cc,
                                              int cap, float gap1, float mdf, float dmul,
-                                             float4* np, float rmax = 0.f, float cs = 0.f) {
+                                             float4* np, float rmax = 0.f, float cs = 0.f,
+                                             int cell_base = 0) {
     float4 me = LD::ld(&sp[kk]);
     float px = me.x, py = me.y, pz = me.z, ri = me.w;
     Stencil r;
     if (rmax > 0.f) {
         const float reach = (ri + rmax) * gap1 * 1.0001f;
         r = stencil_ranges_near<LD>(px, py, pz, g, cs, cc, lane, cap, reach * reach,
-                                    1e-5f * g.L + 1e-6f);
+                                    1e-5f * g.L + 1e-6f, nullptr, cell_base);
     } else {
-        r = stencil_ranges<LD>(px, py, pz, g.L, g.invL, g.halfL, g.G, nullptr, cc, lane, cap, 0);
+        r = stencil_ranges<LD>(px, py, pz, g.L, g.invL, g.halfL, g.G, nullptr, cc, lane, cap,
+                               cell_base);
     }
     float md = fmul(mdf, ri);
     float cx = 0.f, cy = 0.f, cz = 0.f;

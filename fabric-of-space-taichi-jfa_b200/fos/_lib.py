@@ -216,6 +216,7 @@ SIGNATURES = {
     "fos_ensemble_frame_graph": [_P, _I, _P],
     "fos_ensemble_set_tuning": [_P, C.POINTER(FosEnsembleTuning)],
     "fos_ensemble_set_multi_voxel": [_P, _I],
+    "fos_ensemble_trace": [_P, C.POINTER(C.c_longlong), _I, C.POINTER(C.c_int), _P],
     "fos_ensemble_frame_surrogate": [_P, _P, _I, _P],
     "fos_ensemble_surrogate_mode": [_P, _I],
     "fos_ensemble_surrogate_stats": [_P, C.POINTER(FosSurrogateStats), _P],

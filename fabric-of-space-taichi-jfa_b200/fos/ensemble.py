@@ -240,6 +240,15 @@ class Ensemble:
         are the same."""
         call("fos_ensemble_set_multi_voxel", self.h, int(bool(on)))
 
+    def trace_dynamics(self, cap: int = 512) -> list:
+        """ns between the phases of one dynamics kernel over every foam (block
+        0's view; positions and radii advance, the frame index does not)."""
+        buf = (C.c_longlong * cap)()
+        cnt = C.c_int()
+        call("fos_ensemble_trace", self.h, buf, cap, C.byref(cnt), stream())
+        t = [buf[i] for i in range(cnt.value)]
+        return [t[i + 1] - t[i] for i in range(len(t) - 1)]
+
     def signature(self) -> str:
         """Device name + shape of the ensemble (counts, JFA res, hash res)."""
         shape = [(f.n, c.JFA_RES, c.grid_res()) for f, c in zip(self.foams, self.cfgs)]

@@ -658,6 +658,14 @@ int fos_ensemble_autotune(FosEnsemble* e, int reps, FosEnsembleTuning* best, flo
                           int report_cap, fos_stream_t s);
 /* Frame index (synchronises). */
 int fos_ensemble_frame_index(FosEnsemble* e, int* frame, fos_stream_t s);
+/* Tracing (no reference counterpart): the dynamics kernel of one plain frame
+ * of every foam with a %globaltimer stamp, in ns, at kernel entry and after
+ * every grid barrier (block 0's view), as fos_frame_trace.  Advances the
+ * positions and radii as that kernel does, not the frame index; allocates a
+ * scratch buffer and synchronises.  *count gets the number of stamps (<= cap
+ * - 2); ns_host[cap - 2] holds the bitwise NOT of the earliest block's start
+ * and ns_host[cap - 1] the latest block's end (cap >= 3). */
+int fos_ensemble_trace(FosEnsemble* e, long long* ns_host, int cap, int* count, fos_stream_t s);
 long long fos_ensemble_launch_count(FosEnsemble* e);
 
 /* Number of this library's kernel launches issued so far on ctx (host count). */

@@ -74,6 +74,33 @@ def test_ensemble_equals_single_foams(use_graph):
     ens.close()
 
 
+def test_ensemble_with_crowded_cells_equals_single_foams():
+    """A foam that starts with 300 of its 2,000 particles in a 0.02 cube
+    (hash cells 0.04 wide): its cells overflow the 32-slot rows, so those
+    rebuilds of the ensemble's frame take the CSR form, and every foam still
+    equals the same foam run alone."""
+    from fos.inputs import Foam
+    rng = np.random.default_rng(9)
+    n = 2000
+    pos = rng.random((n, 3), dtype=np.float32)
+    pos[:300] = (0.3 + 0.02 * rng.random((300, 3))).astype(np.float32)
+    rad = rng.uniform(0.01, 0.02, n).astype(np.float32)
+    crowd = Foam("crowd-2k-64", pos, rad, 64, 0.01, 0.02, 10, 14, 8, 20, 20, 5, 500, 9)
+    foams = [inputs.ensemble_member(700, 11, 10), crowd]
+    ens = Ensemble(foams, **OVER)
+    sims = _singles(foams)
+    ens.initialize()
+    for f in range(4):
+        jfa = ens.step()
+        for s in sims:
+            assert s.step() == jfa
+        torch.cuda.synchronize()
+        _assert_same(ens, sims, f"frame {f}")
+    for s in sims:
+        s.ctx.close()
+    ens.close()
+
+
 def test_ensemble_with_ou_jitter_equals_single_foams():
     """The OU jitter (dynamics.py:607-660, run.py:855-867) inside the
     ensemble's dynamics kernel: each foam's mean radius from its own exact
