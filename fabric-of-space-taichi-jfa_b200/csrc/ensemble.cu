@@ -413,6 +413,12 @@ __global__ void k_ens_targets(int ntot, const EnsFoamDev* __restrict__ F,
 }
 
 // ------------------------------------------------------------ dynamics
+// Loads of the PBD and max-overlap sweeps: L1-allocating (LdL1) or L2 only
+// (LdL2).  Every phase reads what earlier phases wrote behind a grid barrier,
+// whose acquire makes those writes visible to the block's plain loads.
+#ifndef ENS_SWEEP_LD
+#define ENS_SWEEP_LD LdL1
+#endif
 // Rounds of 8-lane groups in flight in the pressure sweeps: their loads are
 // all issued before the first sum.
 #ifndef ENS_PRESS_ROUNDS
@@ -572,10 +578,10 @@ __device__ __forceinline__ void ens_pbd_frame(const EnsArgs& a, const EnsGeo& ge
             const float cw = a.L / (float)d.G;
             float4 nv = make_float4(0.f, 0.f, 0.f, 0.f);
             const int pi =
-                rows ? pbd_warp_rows<LdL2>(kk, lane, lay.sp, lay.ci, a.pos_tmp, g,
+                rows ? pbd_warp_rows<ENS_SWEEP_LD>(kk, lane, lay.sp, lay.ci, a.pos_tmp, g,
                                            lay.cc + d.cell_off, COOP_CAP, a.gap1, a.mdf, a.dmul,
                                            &nv, rmax, cw, d.cell_off)
-                     : pbd_warp<LdL2>(kk, lane, lay.sp, lay.ci, a.pos_tmp, g, lay.cs + d.cell_off,
+                     : pbd_warp<ENS_SWEEP_LD>(kk, lane, lay.sp, lay.ci, a.pos_tmp, g, lay.cs + d.cell_off,
                                       lay.cc + d.cell_off, a.gap1, a.mdf, a.dmul, &nv, 0,
                                       d.cell_off, rmax, cw);
             d1.put(a, geo, lane, pi, nv, a.pos, next, ou);
@@ -659,7 +665,7 @@ __global__ void __launch_bounds__(THREADS, 1024 / THREADS) k_ens_coop(EnsArgs a)
                 const GridGeom g{d.G, a.L, a.invL, a.halfL};
                 const float rmax0 =
                     d.G >= 5 ? __uint_as_float(__ldcg(&a.W[f].rmax0_bits)) : 0.f;
-                unsigned int b = maxov_warp<LdL2>(kk, lane, lay.sp, lay.ci, g,
+                unsigned int b = maxov_warp<ENS_SWEEP_LD>(kk, lane, lay.sp, lay.ci, g,
                                                   lay.cs ? lay.cs + d.cell_off : nullptr,
                                                   lay.cc + d.cell_off, a.eps, a.lmd, lay.cap,
                                                   d.cell_off, rmax0, a.L / (float)d.G);
