@@ -718,7 +718,7 @@ __global__ void __launch_bounds__(THREADS, 1024 / THREADS) k_ens_coop(EnsArgs a)
 #pragma unroll
                 for (int h = 0; h < NR; ++h) {
                     ii[h] = (r + h) * groups_per_round + tid / 8;
-                    pin[h] = pressure_in8x2n<LdL2>(ii[h], lane, a.n, a.pnbr, rin, vin);
+                    pin[h] = pressure_in8x2n<PRESS_LD>(ii[h], lane, a.n, a.pnbr, rin, vin);
                     bnd[h] = make_float2(0.f, 0.f);
                     if (ii[h] < a.n) {
                         const EnsFoamDev& d = a.F[a.foam_of[ii[h]]];

@@ -352,7 +352,7 @@ __global__ void __launch_bounds__(COOP_THREADS, COOP_BLOCKS_PER_SM) k_frame_coop
 #pragma unroll
                 for (int h = 0; h < NR; ++h) {
                     ii[h] = (r + h) * groups_per_round + tid / 8;
-                    pin[h] = pressure_in8x2n<LdL2>(ii[h], lane, a.n, a.pnbr, rin, vin);
+                    pin[h] = pressure_in8x2n<PRESS_LD>(ii[h], lane, a.n, a.pnbr, rin, vin);
                 }
                 float* vo = last ? nullptr : vout;
                 float dd[NR];

@@ -811,6 +811,13 @@ __device__ __forceinline__ PressureIn pressure_in8x2n(int i, int lane, int n, co
     return p;
 }
 
+// Loads of the table-driven pressure sweeps (pressure_in8x2n): L1-allocating
+// (LdL1) or L2 only (LdL2).  The sweeps read what the sweep before wrote,
+// behind a grid barrier whose acquire makes it visible to plain loads.
+#ifndef PRESS_LD
+#define PRESS_LD LdL1
+#endif
+
 // pressure_sweep8x2v's result from PressureIn: a group with no neighbour
 // taking part sums nothing and gets +0, as when fsc[i] == 0.  Lane 0 of the
 // group writes delta_r[i], rout[i] (clamped to [rmin, rmax]) and, with vout,
