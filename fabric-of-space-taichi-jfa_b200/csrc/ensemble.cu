@@ -563,18 +563,21 @@ __device__ __forceinline__ void ens_pbd_frame(const EnsArgs& a, const EnsGeo& ge
                                               const OuStep* ou = nullptr) {
     const int rounds = (a.n + W_ - 1) / W_;
     P1Defer d1;
+    // the next round's slot and foam are loaded one round ahead
     int kk_next = wid < a.n ? __ldcg(&a.slot_of[wid]) : 0;
+    int f_next = wid < a.n ? a.foam_of[wid] : 0;
     for (int r = 0; r < rounds; ++r) {
         const int i = r * W_ + wid;
         const int kk = kk_next;
+        const int f = f_next;
         kk_next = i + W_ < a.n ? __ldcg(&a.slot_of[i + W_]) : 0;
+        f_next = i + W_ < a.n ? a.foam_of[i + W_] : 0;
         if (i < a.n) {  // warp-uniform
-            const int f = a.foam_of[i];
             const EnsFoamDev& d = a.F[f];
             const GridGeom g{d.G, a.L, a.invL, a.halfL};
             // the stencil skips the cells beyond reach of the foam's largest
             // radius (set in the Brownian phase; radii are fixed during PBD)
-            const float rmax = d.G >= 5 ? __uint_as_float(__ldcg(&a.W[f].rmax_bits)) : 0.f;
+            const float rmax = d.G >= 5 ? __uint_as_float(a.W[f].rmax_bits) : 0.f;
             const float cw = a.L / (float)d.G;
             float4 nv = make_float4(0.f, 0.f, 0.f, 0.f);
             const int pi =
@@ -655,16 +658,17 @@ __global__ void __launch_bounds__(THREADS, 1024 / THREADS) k_ens_coop(EnsArgs a)
     {
         const int rounds = (a.n + W_ - 1) / W_;
         int kk_next = wid < a.n ? __ldcg(&a.slot_of[wid]) : 0;
+        int f_next = wid < a.n ? a.foam_of[wid] : 0;
         for (int r = 0; r < rounds; ++r) {
             const int i = r * W_ + wid;
             const int kk = kk_next;
+            const int f = f_next;
             kk_next = i + W_ < a.n ? __ldcg(&a.slot_of[i + W_]) : 0;
+            f_next = i + W_ < a.n ? a.foam_of[i + W_] : 0;
             if (i < a.n) {
-                const int f = a.foam_of[i];
                 const EnsFoamDev& d = a.F[f];
                 const GridGeom g{d.G, a.L, a.invL, a.halfL};
-                const float rmax0 =
-                    d.G >= 5 ? __uint_as_float(__ldcg(&a.W[f].rmax0_bits)) : 0.f;
+                const float rmax0 = d.G >= 5 ? __uint_as_float(a.W[f].rmax0_bits) : 0.f;
                 unsigned int b = maxov_warp<ENS_SWEEP_LD>(kk, lane, lay.sp, lay.ci, g,
                                                   lay.cs ? lay.cs + d.cell_off : nullptr,
                                                   lay.cc + d.cell_off, a.eps, a.lmd, lay.cap,
