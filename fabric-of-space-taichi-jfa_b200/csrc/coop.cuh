@@ -79,10 +79,12 @@ __device__ __forceinline__ int spread_tid() {
     return (int)((((threadIdx.x >> 5) * gridDim.x + blockIdx.x) << 5) + (threadIdx.x & 31));
 }
 
-// One rebuild's grid as its consumers (max overlap, PBD) see it.  Both forms
-// hold each cell's particles in ascending index order, so a stencil walk
-// visits candidates in the reference's order either way; slot_of[i] (an
-// argument array) is particle i's slot in whichever form was built.
+// One rebuild's grid as its consumers (max overlap, PBD) see it.  The CSR
+// form and the sorted fixed-capacity rows (coop_grid) hold each cell's
+// particles in ascending index order, so a stencil walk visits candidates in
+// the reference's order; the frames' arrival-order rows do not, and their PBD
+// sweeps order the hits themselves (pbd_warp_rows).  slot_of[i] (an argument
+// array) is particle i's slot in whichever form was built.
 struct CoopLayout {
     const int32_t* ci;  // particle at slot k
     const float4* sp;   // (pos, rad) at slot k

@@ -15,8 +15,8 @@
 //   particle stages foam_of[i] gives the foam's descriptor (hash grid, cell
 //                  offset, band, radius bounds, Brownian key, offsets).
 // The dynamics of a frame are one persistent cooperative kernel (the same
-// phases as k_frame_coop) whose grid rebuild fills one packed cell table with
-// each foam's cells at its offset.  Each foam's arithmetic is exactly the
+// phases as k_frame_coop, on arrival-order cell rows) whose grid rebuilds fill
+// one packed cell table with each foam's cells at its offset.  Each foam's arithmetic is exactly the
 // single-foam path's, with its own local index where the reference uses one
 // (the pressure rotation hash, the Brownian counter), so each foam's result
 // is bit-identical to running it alone.
