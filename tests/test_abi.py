@@ -42,6 +42,27 @@ def test_ctypes_binding_covers_header(lib_path):
         assert s in _lib.SIGNATURES, f"{s} has no ctypes signature"
 
 
+def declared_arities():
+    """Parameter count of every function declared in include/fos.h."""
+    src = open(os.path.join(ROOT, "include", "fos.h")).read()
+    src = re.sub(r"/\*.*?\*/", "", src, flags=re.S)
+    out = {}
+    for name, params in re.findall(r"\b(fos_[a-z0-9_]+)\s*\(([^;{}]*?)\)\s*;", src, flags=re.S):
+        params = " ".join(params.split())
+        out[name] = 0 if params in ("", "void") else params.count(",") + 1
+    return out
+
+
+def test_ctypes_argument_counts_match_header():
+    """Every ctypes signature takes as many arguments as its declaration."""
+    from fos import _lib
+    ar = declared_arities()
+    assert len(ar) >= 40
+    bad = {k: (n, len(_lib.SIGNATURES[k])) for k, n in ar.items()
+           if k in _lib.SIGNATURES and len(_lib.SIGNATURES[k]) != n}
+    assert not bad, bad
+
+
 def test_status_strings_without_gpu(lib_path):
     from fos import _lib
     lib = _lib.load()
