@@ -520,6 +520,17 @@ def run_fos(args):
         return 0
 
     topo = run_topology(sim, foam, not args.no_cpu_baseline) if headline_arms else None
+    # where the dynamics kernel's time goes: %globaltimer after every grid
+    # barrier of one plain-frame dynamics kernel (block 0), taken after every
+    # timed region (it advances the foam by one frame's dynamics)
+    try:
+        tr = sim.trace_dynamics()
+        dyn_trace = {"phases_us": [round(x / 1000.0, 2) for x in tr],
+                     "kernel_us": round(sum(tr) / 1000.0, 2), "phases": len(tr),
+                     "source": "%globaltimer at kernel entry and after every grid barrier "
+                               "(block 0), one plain frame after the timed steps"}
+    except Exception as e:  # a diagnostic only: never fails the line
+        dyn_trace = {"error": str(e)[:120]}
     cpu = None
     if not args.no_cpu_baseline:
         fps, dt, cores, first = time_cpu(foam, args.cpu_sample_steps, args.warmup)
@@ -586,13 +597,15 @@ def run_fos(args):
                         "finalize_iterations": st.finalize_iterations,
                         "face_pairs": st.face_pairs, "mean_fsc": round(st.mean_fsc, 3),
                         "voxel_passes_per_s": round(V * passes * value / FRAMES_PER_STEP, 1),
+                        "dynamics_trace": dyn_trace,
 
                         "topology": topo},
     }
     faces_achieved = faces_bytes / faces_s / 1e9
     line["roofline_faces"] = {
-        "bound": "hbm", "kernel": f"face extraction ({foam.res}^3: k_faces_reset, k_faces, "
-                                  f"k_compact, k_rows)",
+        "bound": "hbm", "kernel": f"face extraction ({foam.res}^3: k_faces_reset, k_faces_tile "
+                                  f"(k_faces where R is not a multiple of 8), k_compact, "
+                                  f"k_rows)",
         "achieved": round(faces_achieved, 2), "peak": peak, "unit": "GB/s",
         "frac": round(faces_achieved / peak, 4), "alg_bytes_per_launch": faces_bytes,
         "face_pairs": int(st.face_pairs), "us": round(faces_s * 1e6, 2),
