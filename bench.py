@@ -1079,6 +1079,12 @@ def run_profile(args):
         torch.cuda.cudart().cudaProfilerStop()
         out["ms_per_frame"] = round(a.elapsed_time(b) / 5, 4)
         out["workload"] = "ensemble-64"
+        # one plain frame's dynamics kernel over all foams, phase by phase
+        # (%globaltimer after every grid barrier, block 0), outside the
+        # profiled range
+        tr = ens.trace_dynamics()
+        out["dynamics_phase_us"] = [round(x / 1000.0, 1) for x in tr]
+        out["dynamics_total_us"] = round(sum(tr) / 1000.0, 1)
         ens.close()
     elif args.profile == "inference":
         # surrogate inference alone on the candidate pairs of the headline foam
