@@ -75,3 +75,32 @@ def test_status_strings_without_gpu(lib_path):
     # argument validation needs no device
     assert lib.fos_ctx_create(None, 10, 64, 0, C.byref(C.c_void_p())) == 1
     assert lib.fos_set_resolution(None, 64) == 1
+
+
+def test_ctypes_structures_match_header_layout(tmp_path):
+    """Every ctypes structure of the binding has the size and field offsets of
+    its C declaration in include/fos.h (a C probe compiled with gcc prints
+    them), so no field is silently shifted across the boundary."""
+    import ctypes as C
+    from fos import _lib
+    structs = {name: cls for name, cls in vars(_lib).items()
+               if isinstance(cls, type) and issubclass(cls, C.Structure) and name.startswith("Fos")}
+    assert len(structs) >= 10
+    lines = ['#include <stdio.h>', '#include <stddef.h>', '#include "fos.h"', "int main(void) {"]
+    for name, cls in sorted(structs.items()):
+        lines.append(f'  printf("{name} %zu\\n", sizeof({name}));')
+        for fname, _ in cls._fields_:
+            lines.append(f'  printf("{name}.{fname} %zu\\n", offsetof({name}, {fname}));')
+    lines += ["  return 0;", "}"]
+    src = tmp_path / "layout.c"
+    src.write_text("\n".join(lines) + "\n")
+    exe = tmp_path / "layout"
+    subprocess.run(["gcc", "-std=c11", "-I", os.path.join(ROOT, "include"), str(src), "-o",
+                    str(exe)], check=True, capture_output=True)
+    got = dict(l.split() for l in subprocess.run([str(exe)], capture_output=True, text=True,
+                                                   check=True).stdout.splitlines())
+    for name, cls in structs.items():
+        assert int(got[name]) == C.sizeof(cls), name
+        for fname, _ in cls._fields_:
+            assert int(got[f"{name}.{fname}"]) == getattr(cls, fname).offset, f"{name}.{fname}"
+
