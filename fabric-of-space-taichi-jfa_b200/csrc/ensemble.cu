@@ -622,7 +622,7 @@ __global__ void __launch_bounds__(THREADS, 1024 / THREADS) k_ens_coop(EnsArgs a)
     if (a.trace && threadIdx.x == 0) atomicMax(&a.trace[a.trace_cap - 2], ~global_ns());
     trace_mark(a, tk);
     CoopLayout lay;
-    int gk = 0;  // rebuild gk uses count buffer gk & 1
+    int gk = 0;  // the warm-up form's rebuild gk uses count buffer gk & 1 (coop_grid)
     if (a.mode == 1) {
         // warmup_pbd of initialize_simulation (run.py:293-318): grid + PBD + copy-back
         for (int k = 0; k < a.warmup; ++k) {
