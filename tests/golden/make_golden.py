@@ -276,6 +276,22 @@ def case_jfa_r24_overflow(ref_dir):
     return out, meta
 
 
+def case_jfa_r36_crowded(ref_dir):
+    """R = 36: not a power of two and not a multiple of 8 (7 passes: steps 18,
+    9, 4, 2, 1, 1, 1), with 150 small cells of about 300 voxels each, so that
+    many distinct face pairs meet in every region of the grid."""
+    ref = load_reference(ref_dir, DOMAIN_SIZE=1.0, JFA_EARLY_EXIT_ENABLED=False, JFA_RES_MAX=64)
+    ref.jfa.set_resolution(36)
+    assert ref.jfa.JFA_RES == 36  # not clamped by set_resolution
+    rng = np.random.default_rng(3606)
+    n = 150
+    pos = (rng.random((n, 3), dtype=np.float32) - np.float32(0.5)).astype(np.float32)
+    rad = rng.uniform(0.02, 0.05, n).astype(np.float32)
+    out = _jfa_runs(ref, pos, rad, 2, rng, 0.01, 0.10)
+    meta = dict(L=1.0, R=36, n=n, runs=2, early_exit=False, calls="jfa.run_jfa x2")
+    return out, meta
+
+
 def _edge_positions(G: int, L: float, rng, n: int) -> np.ndarray:
     f = np.float32
     pos = (rng.random((n, 3), dtype=np.float32) - f(0.5)).astype(np.float32)
@@ -556,6 +572,7 @@ CASES = {
     "jfa_r24_ties_early_exit": case_jfa_r24_ties_early_exit,
     "jfa_r16_domain0189": case_jfa_r16_domain0189,
     "jfa_r24_overflow": case_jfa_r24_overflow,
+    "jfa_r36_crowded": case_jfa_r36_crowded,
     "grid_g3": case_grid_g3,
     "grid_g5": case_grid_g5,
     "pbd_g4": case_pbd_g4,
