@@ -292,6 +292,22 @@ def case_jfa_r36_crowded(ref_dir):
     return out, meta
 
 
+def case_jfa_r16_crowded(ref_dir):
+    """R = 16 with 400 seeds (about ten voxels a cell; 19 seeds own no
+    voxel), so that most voxel faces separate two cells and a face row holds
+    up to 26 partners."""
+    ref = load_reference(ref_dir, DOMAIN_SIZE=1.0, JFA_EARLY_EXIT_ENABLED=False)
+    ref.jfa.set_resolution(16)
+    assert ref.jfa.JFA_RES == 16
+    rng = np.random.default_rng(1616)
+    n = 400
+    pos = (rng.random((n, 3), dtype=np.float32) - np.float32(0.5)).astype(np.float32)
+    rad = rng.uniform(0.01, 0.03, n).astype(np.float32)
+    out = _jfa_runs(ref, pos, rad, 2, rng, 0.01, 0.10)
+    meta = dict(L=1.0, R=16, n=n, runs=2, early_exit=False, calls="jfa.run_jfa x2")
+    return out, meta
+
+
 def _edge_positions(G: int, L: float, rng, n: int) -> np.ndarray:
     f = np.float32
     pos = (rng.random((n, 3), dtype=np.float32) - f(0.5)).astype(np.float32)
@@ -573,6 +589,7 @@ CASES = {
     "jfa_r16_domain0189": case_jfa_r16_domain0189,
     "jfa_r24_overflow": case_jfa_r24_overflow,
     "jfa_r36_crowded": case_jfa_r36_crowded,
+    "jfa_r16_crowded": case_jfa_r16_crowded,
     "grid_g3": case_grid_g3,
     "grid_g5": case_grid_g5,
     "pbd_g4": case_pbd_g4,

@@ -45,7 +45,7 @@ def test_every_fixture_is_checked():
 
 
 JFA_CASES = ["jfa_r16_hysteresis", "jfa_r24_ties_early_exit", "jfa_r16_domain0189",
-             "jfa_r24_overflow", "jfa_r36_crowded"]
+             "jfa_r24_overflow", "jfa_r36_crowded", "jfa_r16_crowded"]
 
 
 @pytest.mark.parametrize("case", JFA_CASES)
