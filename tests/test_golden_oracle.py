@@ -58,6 +58,8 @@ def test_jfa_runs_match_reference(case):
     prev = np.zeros((n, 32), np.float32)
     ema = np.zeros(n, np.float32)
     for k in range(m["runs"]):
+        # the reference ran at the recorded resolution (set_resolution clamps)
+        assert f[f"run{k}_labels"].size == R ** 3
         pos, rad = f[f"run{k}_pos"], f[f"run{k}_rad"]
         lab, changes, passes = O.jfa_labels(pos, rad, p)
         assert passes == f[f"run{k}_stat_num_passes"]
